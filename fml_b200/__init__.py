@@ -1,0 +1,29 @@
+"""fml_b200 — B200 (sm_100a) implementation of andersx/fml's KRR hot path.
+
+Drop-in names (same signatures and error behaviour as the reference):
+
+* ``Molecule`` with ``read_xyz``, ``generate_coulomb_matrix``,
+  ``generate_arad_descriptor`` (fml/fml.py)
+* ``gaussian_kernel``, ``laplacian_kernel``, ``get_atomic_kernels_arad``,
+  ``get_atomic_symmetric_kernels_arad`` (fml/kernels/kernels.py)
+* ``cho_solve`` (fml/math/cho_solve.py)
+
+Batched forms: ``generate_coulomb_matrices``, ``generate_arad_descriptors``.
+
+All compute runs in libfmlb.so (hand-written CUDA for sm_100a) through its C
+ABI; torch is used for device buffers and streams only. There is no CPU
+fallback: without the built library or a CUDA device the calls raise.
+"""
+
+from .cho_solve import CholeskyWarning, cho_solve
+from .data import NUCLEAR_CHARGE, PTP
+from .descriptors import generate_arad_descriptors, generate_coulomb_matrices
+from .kernels import (gaussian_kernel, get_atomic_kernels_arad,
+                      get_atomic_symmetric_kernels_arad, laplacian_kernel)
+from .molecule import Molecule
+
+__all__ = [
+    "Molecule", "gaussian_kernel", "laplacian_kernel", "get_atomic_kernels_arad",
+    "get_atomic_symmetric_kernels_arad", "cho_solve", "CholeskyWarning",
+    "generate_coulomb_matrices", "generate_arad_descriptors", "NUCLEAR_CHARGE", "PTP",
+]

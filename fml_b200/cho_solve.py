@@ -1,0 +1,72 @@
+"""``cho_solve``: drop-in for fml/math/cho_solve.py:33-58.
+
+Solves ``A x = y`` by a Cholesky factorisation on the GPU (hand-written
+blocked FP64 factor + triangular solves, the replacement for the LAPACK
+``dpotrf('U')`` / ``dpotrs('U')`` calls of fcho_solve.f90:35-42).
+
+Behaviour kept from the reference: ``ValueError`` on shape mismatch
+(cho_solve.py:47-51); a non-positive pivot emits a warning and the call
+returns (fcho_solve.f90:36-38 prints a WARNING and continues); only the
+upper triangle of ``A`` (numpy indices ``i <= j``) is read, as dpotrf('U')
+reads it. Difference: ``A`` is never modified (with a Fortran-ordered float64
+``A`` the reference overwrites its upper triangle with the factor as an f2py
+side effect). ``strict=True`` raises ``numpy.linalg.LinAlgError`` instead of
+warning.
+"""
+
+import warnings
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._tensors import device, is_torch, to_device, to_output, workspace
+
+
+class CholeskyWarning(RuntimeWarning):
+    pass
+
+
+def _upper_as_rowmajor_lower(A):
+    """Device copy whose row-major lower triangle is A's upper triangle."""
+    if is_torch(A):
+        t = A.to(device=device(), dtype=torch.float64)
+        return t.t().contiguous(), False
+    a = np.asarray(A, dtype=np.float64)
+    t, _ = to_device(np.ascontiguousarray(a.T), torch.float64)
+    return t, True
+
+
+def potrf(Ad, n):
+    """In-place FP64 factorisation of a device (n, n) tensor; returns (work, info)."""
+    work = workspace(_lib.load().fmlb_potrf_workspace_bytes(n))
+    info = torch.zeros(1, dtype=torch.int32, device=Ad.device)
+    _lib.call("fmlb_potrf_f64", _lib.ptr(Ad), Ad.stride(0), n, _lib.ptr(work), _lib.ptr(info),
+              _lib.stream_handle())
+    return work, info
+
+
+def potrs(Ad, n, work, x):
+    _lib.call("fmlb_potrs_f64", _lib.ptr(Ad), Ad.stride(0), n, _lib.ptr(work), _lib.ptr(x),
+              _lib.stream_handle())
+
+
+def cho_solve(A, y, strict=False):
+    """Solve A x = y for symmetric positive-definite A."""
+    if len(A.shape) != 2 or A.shape[0] != A.shape[1]:
+        raise ValueError('expected square matrix')
+    if len(y.shape) != 1 or y.shape[0] != A.shape[1]:
+        raise ValueError('expected matrix and vector of same stride size')
+    n = A.shape[0]
+    Ad, as_np = _upper_as_rowmajor_lower(A)
+    x, _ = to_device(y, torch.float64)
+    x = x.clone()
+    work, info = potrf(Ad, n)
+    code = int(info.item())
+    if code > 0:
+        msg = "WARNING: Cholesky decomposition DPOTRF() exited with error code: %d" % code
+        if strict:
+            raise np.linalg.LinAlgError(msg)
+        warnings.warn(msg, CholeskyWarning, stacklevel=2)
+    potrs(Ad, n, work, x)
+    return to_output(x, as_np or not is_torch(y))

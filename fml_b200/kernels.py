@@ -1,0 +1,148 @@
+"""Kernel matrices: drop-ins for fml/kernels/kernels.py.
+
+* ``gaussian_kernel(A, B, sigma)``  -> fgaussian_kernel (fkernels.f90:317-349)
+* ``laplacian_kernel(A, B, sigma)`` -> flaplacian_kernel (fkernels.f90:351-377)
+* ``get_atomic_kernels_arad`` / ``get_atomic_symmetric_kernels_arad``
+  -> fget_kernels_arad / fget_symmetric_kernels_arad (farad_kernels.f90:439-755)
+
+Signatures follow the reference: ``A`` is (d, na) and ``B`` is (d, nb) with
+descriptors as columns; the result is (na, nb). Extension: ``sigma`` may be a
+sequence, giving (nsigma, na, nb) from one pass. ``A is B`` selects the
+symmetric build (lower tiles computed, mirrored; bit-identical to the full
+build).
+
+Differences from the reference, by design: results are C-ordered (the
+reference returns Fortran order; values are the same), and
+``get_atomic_symmetric_kernels_arad`` works (the reference wrapper calls
+``fget_symmetric_kernels_arad`` without importing it, kernels.py:36-39 vs
+:348, and raises NameError).
+"""
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._tensors import device, is_torch, to_device, to_output, workspace
+from .data import ptp_of
+
+PRECISIONS = {"fp64": 0, "fp32": 1}
+
+
+def _sigma_list(sigma):
+    if np.ndim(sigma) == 0:
+        return [float(sigma)], True
+    s = [float(v) for v in np.asarray(sigma).ravel()]
+    if not s:
+        raise ValueError("need at least one sigma")
+    return s, False
+
+
+def _descriptor_rows(A):
+    """(d, n) reference layout -> (n, d) rows on the device (float64)."""
+    if is_torch(A):
+        t = A.to(device=device(), dtype=torch.float64)
+        return t.t().contiguous(), False
+    a = np.asarray(A, dtype=np.float64)
+    if a.ndim != 2:
+        raise ValueError("expected a 2-D descriptor matrix (d, n)")
+    rows, _ = to_device(np.ascontiguousarray(a.T), torch.float64)
+    return rows, True
+
+
+def _pairwise(A, B, sigma, fn):
+    sig, scalar = _sigma_list(sigma)
+    symmetric = A is B
+    a, as_np = _descriptor_rows(A)
+    b = a if symmetric else _descriptor_rows(B)[0]
+    if a.shape[1] != b.shape[1]:
+        raise ValueError("A and B must hold descriptors of the same length")
+    na, d = a.shape
+    nb = b.shape[0]
+    K = torch.empty((len(sig), na, nb), dtype=torch.float64, device=device())
+    sp, keep = _lib.host_doubles(sig)
+    if na and nb:
+        _lib.call(fn, _lib.ptr(a), na, d, _lib.ptr(b), nb, d, d, sp, len(sig), _lib.ptr(K), nb,
+                  na * nb, 1 if symmetric else 0, _lib.stream_handle())
+    del keep
+    out = K[0] if scalar else K
+    return to_output(out, as_np)
+
+
+def gaussian_kernel(A, B, sigma):
+    """K_ij = exp(-0.5 / sigma**2 * ||A_i - B_j||_2**2), FP64 direct differences."""
+    return _pairwise(A, B, sigma, "fmlb_gaussian_kernel_f64")
+
+
+def laplacian_kernel(A, B, sigma):
+    """K_ij = exp(-1 / sigma * ||A_i - B_j||_1), FP64 direct differences."""
+    return _pairwise(A, B, sigma, "fmlb_laplacian_kernel_f64")
+
+
+# ---------------------------------------------------------------------------
+# ARAD
+# ---------------------------------------------------------------------------
+def _ptp_arrays(Z, amax):
+    """kernels.py:261-292: PTP (nm, amax, 2) float64 and atom counts N (nm,) int32."""
+    nm = len(Z)
+    N = np.array([len(z) for z in Z], dtype=np.int32)
+    if nm and N.max() > amax:
+        raise ValueError("a molecule has more atoms (%d) than the descriptor size %d"
+                         % (int(N.max()), amax))
+    Zp = np.zeros((nm, amax, 2))
+    for i, z in enumerate(Z):
+        if len(z):
+            Zp[i, :len(z)] = ptp_of(z)
+    return Zp, N
+
+
+def _arad(X1, X2, Z1, Z2, sigmas, width, cut_distance, r_width, c_width, symmetric, precision):
+    prec = PRECISIONS[precision]
+    sig, _ = _sigma_list(sigmas)
+    amax = X1.shape[1]
+    nm1 = len(Z1)
+    nm2 = nm1 if symmetric else len(Z2)
+    x1, as_np = to_device(X1, torch.float64)
+    z1p, n1 = _ptp_arrays(Z1, amax)
+    z1, _ = to_device(z1p, torch.float64)
+    n1d, _ = to_device(n1, torch.int32)
+    if symmetric:
+        x2 = z2 = n2d = None
+    else:
+        x2, _ = to_device(X2, torch.float64)
+        z2p, n2 = _ptp_arrays(Z2, amax)
+        z2, _ = to_device(z2p, torch.float64)
+        n2d, _ = to_device(n2, torch.int32)
+    K = torch.empty((len(sig), nm1, nm2), dtype=torch.float64, device=device())
+    nbytes = _lib.load().fmlb_arad_workspace_bytes(nm1, nm2, amax, 1 if symmetric else 0)
+    ws = workspace(nbytes)
+    sp, keep = _lib.host_doubles(sig)
+    _lib.call("fmlb_arad_kernels", _lib.ptr(x1), _lib.ptr(z1), _lib.ptr(n1d), nm1,
+              _lib.ptr(x2), _lib.ptr(z2), _lib.ptr(n2d), nm2, amax, sp, len(sig),
+              float(width), float(cut_distance), float(r_width), float(c_width),
+              1 if symmetric else 0, prec, _lib.ptr(K), _lib.ptr(ws), ws.numel(),
+              _lib.stream_handle())
+    del keep
+    return to_output(K, as_np)
+
+
+def get_atomic_kernels_arad(X1, X2, Z1, Z2, sigmas, width=0.2, cut_distance=6.0, r_width=1.0,
+                            c_width=0.5, precision="fp64"):
+    """Kernels (nsigma, nm1, nm2) between two sets of ARAD descriptors."""
+    amax = X1.shape[1]
+    # the reference's argument checks, kernels.py:251-259
+    assert X1.shape[3] == amax, "ERROR: Check ARAD decriptor sizes! code = 1"
+    assert X2.shape[1] == amax, "ERROR: Check ARAD decriptor sizes! code = 2"
+    assert X2.shape[3] == amax, "ERROR: Check ARAD decriptor sizes! code = 3"
+    assert X1.shape[0] == len(Z1), "ERROR: Check ARAD decriptor sizes! code = 4"
+    assert X2.shape[0] == len(Z2), "ERROR: Check ARAD decriptor sizes! code = 5"
+    return _arad(X1, X2, Z1, Z2, sigmas, width, cut_distance, r_width, c_width, False, precision)
+
+
+def get_atomic_symmetric_kernels_arad(X1, Z1, sigmas, width=0.2, cut_distance=6.0, r_width=1.0,
+                                      c_width=0.5, precision="fp64"):
+    """Kernels (nsigma, nm1, nm1) of one set with itself (i <= j computed, mirrored)."""
+    amax = X1.shape[1]
+    assert X1.shape[3] == amax, "ERROR: Check ARAD decriptor sizes! code = 1"
+    assert X1.shape[0] == len(Z1), "ERROR: Check ARAD decriptor sizes! code = 4"
+    return _arad(X1, None, Z1, None, sigmas, width, cut_distance, r_width, c_width, True,
+                 precision)

@@ -1,0 +1,152 @@
+/*
+ * fmlb.h — C ABI of libfmlb.so, the B200 (sm_100a) implementation of the
+ * andersx/fml kernel-ridge-regression hot path.
+ *
+ * Conventions
+ *   - Every pointer argument is DEVICE memory unless stated otherwise; the
+ *     caller owns all buffers. Arrays are C-order (row-major).
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream). Calls are asynchronous on that stream unless stated.
+ *   - Return value: FMLB_OK (0) or a negative error code; the message of the
+ *     last error on the calling thread is in fmlb_last_error_string().
+ *   - Descriptors are rows: a descriptor matrix of n descriptors of length d
+ *     is an (n, d) array with leading dimension ld >= d. The reference's
+ *     Python wrappers take the transpose, (d, n), and hand f2py Fortran-order
+ *     arrays whose columns are descriptors; the memory layout is the same.
+ *
+ * Each entry point names the reference routine it replaces (file:line in the
+ * andersx/fml tree).
+ */
+#ifndef FMLB_H
+#define FMLB_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FMLB_OK 0
+#define FMLB_EINVAL (-22)    /* invalid argument (shape, size, pointer) */
+#define FMLB_ENOMEM (-12)    /* workspace too small */
+#define FMLB_ECUDA (-5)      /* CUDA launch / runtime error */
+#define FMLB_ENOTSUP (-95)   /* size outside what the kernels support */
+#define FMLB_ETIMEDOUT (-110)/* a bounded device-side wait gave up */
+
+/* Message describing the last error returned on this thread ("" if none). */
+const char *fmlb_last_error_string(void);
+
+/* ABI version of this library. */
+int fmlb_version(void);
+
+/* ------------------------------------------------------------------------
+ * Sorted Coulomb matrices for a packed ragged batch of molecules.
+ * Replaces fgenerate_coulomb_matrix, fml/representations/frepresentations.f90:23-110
+ * (called per molecule by Molecule.generate_coulomb_matrix, fml/fml.py:64-66).
+ *
+ *   charges  (total_atoms,)    nuclear charges
+ *   coords   (total_atoms, 3)  Cartesian coordinates
+ *   offsets  (nmol + 1,) int   molecule m owns atoms [offsets[m], offsets[m+1])
+ *   nmax     padded size; each output row holds nmax*(nmax+1)/2 values
+ *   cm       (nmol, ldcm) float64 output, ldcm >= nmax*(nmax+1)/2 (may be NULL)
+ *   cm32     (nmol, ldcm32) float32 copy of the same values (may be NULL);
+ *            columns beyond nmax*(nmax+1)/2 are zeroed up to ldcm32
+ *   order    (nmol, nmax) int: original atom index at each sorted position,
+ *            -1 past the molecule's atom count (may be NULL)
+ * Row-norm order: descending, ties -> higher original index first
+ * (the reference's repeated minloc filled from the end, :86-91).
+ *   status   device int (may be NULL): set to 1 when a molecule has more than
+ *            nmax atoms (the reference writes out of bounds there); that
+ *            molecule's row is written as zeros.
+ * Errors: FMLB_EINVAL if nmax is outside 1..255 or a leading dimension is short.
+ * ---------------------------------------------------------------------- */
+int fmlb_coulomb_matrices(const double *charges, const double *coords, const int *offsets,
+                          int nmol, int nmax, double *cm, int ldcm, float *cm32, int ldcm32,
+                          int *order, int *status, void *stream);
+
+/* ------------------------------------------------------------------------
+ * ARAD descriptors for a packed ragged batch of molecules.
+ * Replaces ARAD.describe, fml/arad.py:70-145 (non-periodic path), as called
+ * by Molecule.generate_arad_descriptor, fml/fml.py:80-86.
+ *
+ *   out  (nmol, size, 5, size) float64: channel 0 sorted neighbour distances
+ *        (padding 1e100), 1/2 PTP row/column, 3/4 damped mean cos/sin.
+ *   cut  neighbour cut-off (Angstrom).
+ *   status device int (may be NULL): 1 if a molecule has more than `size`
+ *        atoms (its rows are padding only), 2 if a charge has no
+ *        periodic-table position (its channels 1/2 hold -1).
+ * Errors: FMLB_EINVAL if size is outside 1..128.
+ * ---------------------------------------------------------------------- */
+int fmlb_arad_descriptors(const double *charges, const double *coords, const int *offsets,
+                          int nmol, int size, double cut, double *out, int *status, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Gaussian and Laplacian kernel matrices, plain FP64 (direct differences).
+ * Replace fgaussian_kernel / flaplacian_kernel, fml/kernels/fkernels.f90:317-377
+ * (wrappers gaussian_kernel / laplacian_kernel, fml/kernels/kernels.py:136-196).
+ *
+ *   A (na, lda), B (nb, ldb): descriptor rows of length d
+ *   K: nsigma matrices (na, nb), matrix s at K + s*sigma_stride, row stride ldk
+ *      gaussian:  K_s[j,i] = exp(-0.5/sigma_s^2 * sum_k (A[j,k]-B[i,k])^2)
+ *      laplacian: K_s[j,i] = exp(-1/sigma_s   * sum_k |A[j,k]-B[i,k]|)
+ *   symmetric != 0: A == B (same pointer, na == nb); only tiles on or below
+ *      the diagonal are computed and mirrored (results are bit-identical to
+ *      the full computation, which is exactly symmetric).
+ * ---------------------------------------------------------------------- */
+int fmlb_gaussian_kernel_f64(const double *A, int na, int lda, const double *B, int nb, int ldb,
+                             int d, const double *sigmas_host, int nsigma, double *K,
+                             long long ldk, long long sigma_stride, int symmetric, void *stream);
+int fmlb_laplacian_kernel_f64(const double *A, int na, int lda, const double *B, int nb, int ldb,
+                              int d, const double *sigmas_host, int nsigma, double *K,
+                              long long ldk, long long sigma_stride, int symmetric, void *stream);
+
+/* ------------------------------------------------------------------------
+ * ARAD molecular kernels.
+ * Replace fget_kernels_arad (fml/kernels/farad_kernels.f90:439-616) and
+ * fget_symmetric_kernels_arad (:619-755), core atomic_distl2 (:29-90);
+ * wrappers get_atomic_kernels_arad / get_atomic_symmetric_kernels_arad,
+ * fml/kernels/kernels.py:229-349.
+ *
+ *   X1 (nm1, amax, 5, amax), X2 (nm2, amax, 5, amax) float64 ARAD descriptors
+ *   Z1 (nm1, amax, 2), Z2 (nm2, amax, 2) float64 PTP (row, column) per atom
+ *   N1 (nm1,), N2 (nm2,) int atom counts (<= amax)
+ *   sigmas_host (nsigma,) HOST array; K (nsigma, nm1, nm2) float64 output
+ *   symmetric != 0: set 2 is set 1 (X2/Z2/N2 ignored), only i <= j computed
+ *      and mirrored, with the symmetric routine's sine table (:689-698).
+ *   precision: 0 = FP64 (parity path), 1 = FP32 arithmetic, FP64 output.
+ *   workspace: device scratch of fmlb_arad_workspace_bytes(...) bytes.
+ * Errors: FMLB_ENOTSUP if amax > 64; FMLB_ENOMEM if ws_bytes is too small.
+ * ---------------------------------------------------------------------- */
+size_t fmlb_arad_workspace_bytes(int nm1, int nm2, int amax, int symmetric);
+int fmlb_arad_kernels(const double *X1, const double *Z1, const int *N1, int nm1,
+                      const double *X2, const double *Z2, const int *N2, int nm2, int amax,
+                      const double *sigmas_host, int nsigma, double width, double cut_distance,
+                      double r_width, double c_width, int symmetric, int precision, double *K,
+                      void *workspace, size_t ws_bytes, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Cholesky factorisation and solve, FP64.
+ * Replace LAPACK dpotrf('U') / dpotrs('U') as called by fcho_solve,
+ * fml/math/fcho_solve.f90:23-47 (wrapper cho_solve, fml/math/cho_solve.py:33-58).
+ *
+ * A is an (n, n) row-major matrix with row stride lda. The factorisation
+ * reads the triangle i >= j of the row-major array and overwrites it with L,
+ * A = L L^T. For the reference's C-order numpy argument this is the upper
+ * triangle of the Fortran view, A = U^T U with U = L^T, i.e. dpotrf('U').
+ *
+ *   work     device scratch of fmlb_potrf_workspace_bytes(n) bytes; keeps the
+ *            inverted diagonal blocks that fmlb_potrs_f64 reuses.
+ *   info     device int: 0, or the 1-based column of the first non-positive
+ *            pivot (LAPACK convention); work after a failed pivot is skipped.
+ * fmlb_potrs_f64 solves A x = b in place in x (n,) given the factor and work.
+ * ---------------------------------------------------------------------- */
+size_t fmlb_potrf_workspace_bytes(int n);
+int fmlb_potrf_f64(double *A, long long lda, int n, void *work, int *info, void *stream);
+int fmlb_potrs_f64(const double *L, long long lda, int n, const void *work, double *x,
+                   void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FMLB_H */

@@ -1,0 +1,194 @@
+"""CPU ORACLE — test infrastructure, not product code.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline /
+reference arm use this package, as the checker; the product package
+``fml_b200`` never imports it.
+
+* ``oracle.c`` (built into ``liboracle.so`` by ``oracle/Makefile``) restates the
+  reference's Fortran routines on the hot path in plain C, FP64, with the
+  reference's OpenMP outer loops.
+* ``arad_describe.py`` restates ``ARAD.describe`` (fml/arad.py:70-145).
+* ``cho_solve`` calls LAPACK ``dpotrf``/``dpotrs`` through scipy (OpenBLAS),
+  the same LAPACK routines fml/math/fcho_solve.f90:35-42 calls; the reference
+  pins no LAPACK version (Makefile:14 links the system ``-llapack``).
+
+The functions below keep the reference's Python signatures
+(fml/kernels/kernels.py, fml/math/cho_solve.py) so parity tests read like
+the reference's own usage.
+"""
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from .arad_describe import describe as arad_describe  # noqa: F401
+from .ptp import ptp_of
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def build():
+    """Compile liboracle.so (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        lib = ctypes.CDLL(path)
+        lib.orc_cm_sorted.restype = ctypes.c_int
+        lib.orc_cm_sorted_batch.restype = ctypes.c_int
+        lib.orc_potrf_upper.restype = ctypes.c_int
+        lib.orc_num_threads.restype = ctypes.c_int
+        _LIB = lib
+    return _LIB
+
+
+def _p(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+def num_threads():
+    return _lib().orc_num_threads()
+
+
+# --------------------------------------------------------------------------
+# descriptors
+# --------------------------------------------------------------------------
+def generate_coulomb_matrix(charges, coords, size=23, return_order=False):
+    """frepresentations.f90:23-110 for one molecule."""
+    z = np.ascontiguousarray(charges, dtype=np.float64)
+    r = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1, 3)
+    if len(z) != len(r):
+        raise ValueError("coordinates / nuclear_charges size mismatch")
+    if len(z) > size:
+        raise ValueError("molecule has more atoms than size")
+    cm = np.zeros(size * (size + 1) // 2)
+    order = np.zeros(max(len(z), 1), dtype=np.int32)
+    _lib().orc_cm_sorted(len(z), _p(z), _p(r), size, _p(cm), _p(order, _ip))
+    return (cm, order[: len(z)]) if return_order else cm
+
+
+def coulomb_matrices(charges, coords, offsets, size=23, return_order=False):
+    """Batch of sorted CMs over a packed ragged molecule buffer."""
+    z = np.ascontiguousarray(charges, dtype=np.float64)
+    r = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1, 3)
+    off = np.ascontiguousarray(offsets, dtype=np.int32)
+    nmol = len(off) - 1
+    cm = np.zeros((nmol, size * (size + 1) // 2))
+    order = np.full((nmol, size), -1, dtype=np.int32)
+    rc = _lib().orc_cm_sorted_batch(nmol, _p(off, _ip), _p(z), _p(r), size, _p(cm),
+                                    _p(order, _ip))
+    if rc:
+        raise ValueError("molecule has more atoms than size")
+    return (cm, order) if return_order else cm
+
+
+def arad_descriptors(charges, coords, offsets, size=23, cut=5.0):
+    off = np.asarray(offsets)
+    out = np.zeros((len(off) - 1, size, 5, size))
+    for m in range(len(off) - 1):
+        out[m] = arad_describe(coords[off[m]:off[m + 1]], charges[off[m]:off[m + 1]], size, cut)
+    return out
+
+
+# --------------------------------------------------------------------------
+# kernels (reference signatures: A is (d, na), B is (d, nb))
+# --------------------------------------------------------------------------
+def _rows(A):
+    # the reference's A(:, j) is descriptor j; store descriptors as C rows
+    return np.ascontiguousarray(np.asarray(A, dtype=np.float64).T)
+
+
+def gaussian_kernel(A, B, sigma):
+    """fkernels.f90:317-349 via kernels.py:167-196."""
+    a, b = _rows(A), _rows(B)
+    na, nb, d = a.shape[0], b.shape[0], a.shape[1]
+    K = np.empty((na, nb))
+    _lib().orc_gaussian_kernel(_p(a), na, _p(b), nb, d, ctypes.c_double(sigma), _p(K))
+    return K
+
+
+def laplacian_kernel(A, B, sigma):
+    """fkernels.f90:351-377 via kernels.py:136-164."""
+    a, b = _rows(A), _rows(B)
+    na, nb, d = a.shape[0], b.shape[0], a.shape[1]
+    K = np.empty((na, nb))
+    _lib().orc_laplacian_kernel(_p(a), na, _p(b), nb, d, ctypes.c_double(sigma), _p(K))
+    return K
+
+
+def _ptp_pad(Z, amax):
+    out = np.zeros((len(Z), amax, 2))
+    for i, z in enumerate(Z):
+        if len(z):
+            out[i, : len(z)] = ptp_of(z)
+    return out
+
+
+def get_atomic_kernels_arad(X1, X2, Z1, Z2, sigmas, width=0.2, cut_distance=6.0,
+                            r_width=1.0, c_width=0.5):
+    """farad_kernels.f90:439-616 via kernels.py:229-297."""
+    X1 = np.ascontiguousarray(X1, dtype=np.float64)
+    X2 = np.ascontiguousarray(X2, dtype=np.float64)
+    amax = X1.shape[1]
+    n1 = np.array([len(z) for z in Z1], dtype=np.int32)
+    n2 = np.array([len(z) for z in Z2], dtype=np.int32)
+    z1, z2 = _ptp_pad(Z1, amax), _ptp_pad(Z2, amax)
+    s = np.ascontiguousarray(sigmas, dtype=np.float64)
+    K = np.zeros((len(s), len(Z1), len(Z2)))
+    _lib().orc_arad_kernels(_p(X1), _p(X2), _p(z1), _p(z2), _p(n1, _ip), _p(n2, _ip), _p(s),
+                            len(Z1), len(Z2), len(s), amax, ctypes.c_double(width),
+                            ctypes.c_double(cut_distance), ctypes.c_double(r_width),
+                            ctypes.c_double(c_width), _p(K))
+    return K
+
+
+def get_atomic_symmetric_kernels_arad(X1, Z1, sigmas, width=0.2, cut_distance=6.0,
+                                      r_width=1.0, c_width=0.5):
+    """farad_kernels.f90:619-755 via kernels.py:300-349."""
+    X1 = np.ascontiguousarray(X1, dtype=np.float64)
+    amax = X1.shape[1]
+    n1 = np.array([len(z) for z in Z1], dtype=np.int32)
+    z1 = _ptp_pad(Z1, amax)
+    s = np.ascontiguousarray(sigmas, dtype=np.float64)
+    K = np.zeros((len(s), len(Z1), len(Z1)))
+    _lib().orc_arad_symmetric_kernels(_p(X1), _p(z1), _p(n1, _ip), _p(s), len(Z1), len(s), amax,
+                                      ctypes.c_double(width), ctypes.c_double(cut_distance),
+                                      ctypes.c_double(r_width), ctypes.c_double(c_width), _p(K))
+    return K
+
+
+# --------------------------------------------------------------------------
+# solve
+# --------------------------------------------------------------------------
+def cho_solve(A, y):
+    """fcho_solve.f90:23-47: LAPACK dpotrf('U') then dpotrs('U') (scipy/OpenBLAS).
+
+    Returns (x, info_potrf)."""
+    from scipy.linalg import lapack
+
+    A = np.asarray(A, dtype=np.float64)
+    c, info = lapack.dpotrf(np.asfortranarray(A), lower=0, clean=0, overwrite_a=0)
+    x, info2 = lapack.dpotrs(c, np.asarray(y, dtype=np.float64), lower=0)
+    return x, int(info)
+
+
+def cho_solve_restated(A, y):
+    """Plain-C unblocked restatement of dpotrf('U') + dpotrs('U'). (x, info)."""
+    U = np.array(A, dtype=np.float64, order="C", copy=True)
+    n = U.shape[0]
+    info = _lib().orc_potrf_upper(n, _p(U))
+    x = np.array(y, dtype=np.float64, copy=True)
+    if info == 0:
+        _lib().orc_potrs_upper(n, _p(U), _p(x))
+    return x, int(info)

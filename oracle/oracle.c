@@ -1,0 +1,378 @@
+/*
+ * CPU ORACLE — test infrastructure, not product code.
+ *
+ * Plain-C FP64 restatement of the reference's Fortran routines on the KRR hot
+ * path. Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline /
+ * reference arm may load this library; the product (fml_b200) never does.
+ *
+ * Every routine cites the reference file:line it restates (paths are relative
+ * to the andersx/fml tree). Arithmetic is written in the same order as the
+ * Fortran source and is compiled with -ffp-contract=off so that no FMA is
+ * introduced. Parallelism follows the reference: one OpenMP loop over the
+ * outermost molecule / column index.
+ *
+ * Layout convention (C order, matching the numpy arrays the reference's
+ * Python wrappers hand to f2py):
+ *   descriptors  X   (n, d)              row = one descriptor
+ *   kernel       K   (na, nb)            K[j*nb + i] = k(A_j, B_i)
+ *   ARAD         Q   (nm, amax, 5, amax) Q[((m*amax + a)*5 + ch)*amax + k]
+ *   PTP          Z   (nm, amax, 2)
+ *   ARAD kernel  K   (nsigma, nm1, nm2)
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <float.h>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Sorted Coulomb matrix: frepresentations.f90:23-110                         */
+/* ------------------------------------------------------------------------ */
+/*
+ * charges[n], coords[n*3] (row-major), output cm[nmax*(nmax+1)/2].
+ * order_out (optional, n ints): order_out[p] = original 0-based atom index
+ * placed at sorted position p.
+ * Returns 0, or -1 when n > nmax (the Fortran writes out of bounds there).
+ */
+int orc_cm_sorted(int n, const double *charges, const double *coords, int nmax,
+                  double *cm, int *order_out)
+{
+    if (n > nmax || n < 0) return -1;
+    const int len = nmax * (nmax + 1) / 2;
+    for (int t = 0; t < len; ++t) cm[t] = 0.0;
+    if (n == 0) return 0;
+
+    double *pair = (double *)malloc(sizeof(double) * (size_t)n * n);
+    double *row_norms = (double *)malloc(sizeof(double) * n);
+    int *sorted_atoms = (int *)malloc(sizeof(int) * n);
+
+    /* :62-70 diagonal 0.5 * Z**2.4 seeds the row norms */
+    for (int i = 0; i < n; ++i) {
+        double pn = 0.5 * pow(charges[i], 2.4);
+        row_norms[i] = 0.0 + pn;
+        pair[i * n + i] = pn;
+    }
+    /* :72-84 off-diagonal Z_i Z_j / |R_j - R_i|, accumulated in loop order */
+    for (int i = 0; i < n; ++i) {
+        for (int j = i + 1; j < n; ++j) {
+            double dx = coords[j * 3 + 0] - coords[i * 3 + 0];
+            double dy = coords[j * 3 + 1] - coords[i * 3 + 1];
+            double dz = coords[j * 3 + 2] - coords[i * 3 + 2];
+            double s = dx * dx;
+            s = s + dy * dy;
+            s = s + dz * dz;
+            double pn = charges[i] * charges[j] / sqrt(s);
+            row_norms[j] = row_norms[j] + pn;
+            row_norms[i] = row_norms[i] + pn;
+            pair[i * n + j] = pn;
+            pair[j * n + i] = pn;
+        }
+    }
+    /* :86-91 repeated minloc (first index of the minimum), filled from the end */
+    for (int it = 0; it < n; ++it) {
+        int jmin = 0;
+        for (int j = 1; j < n; ++j)
+            if (row_norms[j] < row_norms[jmin]) jmin = j;
+        sorted_atoms[n - it - 1] = jmin;
+        row_norms[jmin] = DBL_MAX;
+    }
+    /* :93-104 packed lower triangle of the sorted matrix, row by row */
+    for (int m = 0; m < n; ++m) {
+        int i = sorted_atoms[m];
+        int idx = m * (m + 1) / 2;
+        for (int q = 0; q <= m; ++q) cm[idx + q] = pair[i * n + sorted_atoms[q]];
+    }
+    if (order_out)
+        for (int m = 0; m < n; ++m) order_out[m] = sorted_atoms[m];
+    free(pair);
+    free(row_norms);
+    free(sorted_atoms);
+    return 0;
+}
+
+/* Batch form: offsets[nmol+1] into the packed atom arrays; cm (nmol, len). */
+int orc_cm_sorted_batch(int nmol, const int *offsets, const double *charges,
+                        const double *coords, int nmax, double *cm, int *order_out)
+{
+    const int len = nmax * (nmax + 1) / 2;
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(| : bad)
+    for (int m = 0; m < nmol; ++m) {
+        int a0 = offsets[m], n = offsets[m + 1] - offsets[m];
+        int rc = orc_cm_sorted(n, charges + a0, coords + 3 * (size_t)a0, nmax,
+                               cm + (size_t)m * len,
+                               order_out ? order_out + (size_t)m * nmax : NULL);
+        if (rc) bad |= 1;
+    }
+    return bad ? -1 : 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Gaussian kernel: fkernels.f90:317-349                                      */
+/* ------------------------------------------------------------------------ */
+void orc_gaussian_kernel(const double *A, int na, const double *B, int nb, int d,
+                         double sigma, double *K)
+{
+    const double inv_sigma = -0.5 / (sigma * sigma); /* :334 */
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < nb; ++i) {                 /* :338-339 OMP over columns of B */
+        const double *b = B + (size_t)i * d;
+        for (int j = 0; j < na; ++j) {
+            const double *a = A + (size_t)j * d;
+            double s = 0.0;
+            for (int k = 0; k < d; ++k) {          /* :341-342 sum(temp*temp) */
+                double t = a[k] - b[k];
+                s = s + t * t;
+            }
+            K[(size_t)j * nb + i] = exp(inv_sigma * s);
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Laplacian kernel: fkernels.f90:351-377                                     */
+/* ------------------------------------------------------------------------ */
+void orc_laplacian_kernel(const double *A, int na, const double *B, int nb, int d,
+                          double sigma, double *K)
+{
+    const double inv_sigma = -1.0 / sigma; /* :367 */
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < nb; ++i) {
+        const double *b = B + (size_t)i * d;
+        for (int j = 0; j < na; ++j) {
+            const double *a = A + (size_t)j * d;
+            double s = 0.0;
+            for (int k = 0; k < d; ++k) s = s + fabs(a[k] - b[k]); /* :372 */
+            K[(size_t)j * nb + i] = exp(inv_sigma * s);
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* ARAD atom-pair distance: farad_kernels.f90:29-90 (atomic_distl2)           */
+/* ------------------------------------------------------------------------ */
+/* x1, x2: one atom's descriptor (5, amax) row-major; s1, s2: sine factors.   */
+static double orc_atomic_distl2(const double *x1, const double *x2, int n1, int n2,
+                                const double *s1, const double *s2, int amax,
+                                double width, double cut, double r_width, double c_width)
+{
+    const double inv_width = -1.0 / (4.0 * width * width); /* :58 */
+    const double maxgausdist2 = (8.0 * width) * (8.0 * width); /* :60 */
+    const double rw2 = r_width * r_width, cw2 = c_width * c_width;
+    const double *r1 = x1, *p1 = x1 + amax, *g1 = x1 + 2 * amax, *c1 = x1 + 3 * amax,
+                 *z1 = x1 + 4 * amax;
+    const double *r2 = x2, *p2 = x2 + amax, *g2 = x2 + 2 * amax, *c2 = x2 + 3 * amax,
+                 *z2 = x2 + 4 * amax;
+    double aadist = 0.0;
+    for (int m1 = 0; m1 < n1; ++m1) {
+        if (r1[m1] > cut) break;                        /* :68 */
+        for (int m2 = 0; m2 < n2; ++m2) {
+            if (r2[m2] > cut) break;                    /* :72 */
+            double dr = r2[m2] - r1[m1];
+            double r2v = dr * dr;                       /* :74 */
+            if (r2v < maxgausdist2) {                   /* :76 */
+                double d = exp(r2v * inv_width) * s1[m1] * s2[m2]; /* :78 */
+                double dp = p1[m1] - p2[m2], dg = g1[m1] - g2[m2];
+                d = d * (rw2 / (rw2 + dp * dp) * cw2 / (cw2 + dg * dg)); /* :80-81 */
+                aadist = aadist + d * (1.0 + c1[m1] * c2[m2] + z1[m1] * z2[m2]); /* :83 */
+            }
+        }
+    }
+    return aadist;
+}
+
+/* sin factor tables, farad_kernels.f90:521-545 (non-symmetric: only r < cut)
+ * and :689-698 (symmetric: unconditional). sin[(m*amax + a)*amax + k]. */
+static double *orc_arad_sines(const double *Q, const int *N, int nm, int amax, double cut,
+                              int conditional)
+{
+    const double pi = 4.0 * atan(1.0);
+    const double inv_cut = pi / (2.0 * cut); /* :510 */
+    double *s = (double *)calloc((size_t)nm * amax * amax, sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int m = 0; m < nm; ++m) {
+        int ni = N[m];
+        for (int k = 0; k < ni; ++k)
+            for (int a = 0; a < ni; ++a) {
+                double r = Q[(((size_t)m * amax + a) * 5 + 0) * amax + k];
+                if (!conditional || r < cut)
+                    s[((size_t)m * amax + a) * amax + k] = 1.0 - sin(r * inv_cut);
+            }
+    }
+    return s;
+}
+
+/* self terms selfl2, farad_kernels.f90:550-568 */
+static double *orc_arad_self(const double *Q, const int *N, const double *S, int nm, int amax,
+                             double width, double cut, double rw, double cw)
+{
+    double *self = (double *)calloc((size_t)nm * amax, sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int m = 0; m < nm; ++m) {
+        int ni = N[m];
+        for (int a = 0; a < ni; ++a) {
+            const double *x = Q + ((size_t)m * amax + a) * 5 * amax;
+            const double *s = S + ((size_t)m * amax + a) * amax;
+            self[(size_t)m * amax + a] =
+                orc_atomic_distl2(x, x, ni, ni, s, s, amax, width, cut, rw, cw);
+        }
+    }
+    return self;
+}
+
+static double orc_arad_pair(const double *Q1, const double *Z1, const int *N1, const double *S1,
+                            const double *self1, int i, const double *Q2, const double *Z2,
+                            const int *N2, const double *S2, const double *self2, int j,
+                            int amax, double width, double cut, double rw, double cw,
+                            const double *inv_sigma2, int nsig, double *ad, double *out)
+{
+    const double eps = 5.0e-12f; /* :505 a single-precision literal in the source */
+    const double rw2 = rw * rw, cw2 = cw * cw;
+    int ni = N1[i], nj = N2[j];
+    for (int j1 = 0; j1 < nj; ++j1) {
+        for (int i1 = 0; i1 < ni; ++i1) {
+            const double *x1 = Q1 + ((size_t)i * amax + i1) * 5 * amax;
+            const double *x2 = Q2 + ((size_t)j * amax + j1) * 5 * amax;
+            double l2 = orc_atomic_distl2(x1, x2, ni, nj, S1 + ((size_t)i * amax + i1) * amax,
+                                          S2 + ((size_t)j * amax + j1) * amax, amax, width, cut,
+                                          rw, cw);
+            double dz1 = Z1[((size_t)i * amax + i1) * 2 + 0] - Z2[((size_t)j * amax + j1) * 2 + 0];
+            double dz2 = Z1[((size_t)i * amax + i1) * 2 + 1] - Z2[((size_t)j * amax + j1) * 2 + 1];
+            /* :590-592 */
+            l2 = self1[(size_t)i * amax + i1] + self2[(size_t)j * amax + j1] -
+                 2.0 * l2 * (rw2 / (rw2 + dz1 * dz1) * cw2 / (cw2 + dz2 * dz2));
+            if (fabs(l2) < eps) l2 = 0.0; /* :594 */
+            ad[(size_t)j1 * ni + i1] = l2; /* column-major like atomic_distance(:ni,:nj) */
+        }
+    }
+    /* :602-604 sum(exp(atomic_distance(:ni,:nj) * inv_sigma2(k))), column-major order */
+    for (int k = 0; k < nsig; ++k) {
+        double s = 0.0;
+        for (int t = 0; t < ni * nj; ++t) s = s + exp(ad[t] * inv_sigma2[k]);
+        out[k] = s;
+    }
+    return 0.0;
+}
+
+/* fget_kernels_arad: farad_kernels.f90:439-616. K (nsig, nm1, nm2). */
+void orc_arad_kernels(const double *Q1, const double *Q2, const double *Z1, const double *Z2,
+                      const int *N1, const int *N2, const double *sigmas, int nm1, int nm2,
+                      int nsig, int amax, double width, double cut, double rw, double cw,
+                      double *K)
+{
+    double *inv_sigma2 = (double *)malloc(sizeof(double) * (nsig > 0 ? nsig : 1));
+    for (int k = 0; k < nsig; ++k) inv_sigma2[k] = -1.0 / (sigmas[k] * sigmas[k]); /* :511 */
+    double *S1 = orc_arad_sines(Q1, N1, nm1, amax, cut, 1);
+    double *S2 = orc_arad_sines(Q2, N2, nm2, amax, cut, 1);
+    double *self1 = orc_arad_self(Q1, N1, S1, nm1, amax, width, cut, rw, cw);
+    double *self2 = orc_arad_self(Q2, N2, S2, nm2, amax, width, cut, rw, cw);
+#pragma omp parallel
+    {
+        double *ad = (double *)malloc(sizeof(double) * (size_t)amax * amax);
+        double *out = (double *)malloc(sizeof(double) * (nsig > 0 ? nsig : 1));
+#pragma omp for schedule(dynamic, 1)
+        for (int j = 0; j < nm2; ++j) { /* :576-577 OMP over molecules of set 2 */
+            for (int i = 0; i < nm1; ++i) {
+                orc_arad_pair(Q1, Z1, N1, S1, self1, i, Q2, Z2, N2, S2, self2, j, amax, width,
+                              cut, rw, cw, inv_sigma2, nsig, ad, out);
+                for (int k = 0; k < nsig; ++k)
+                    K[((size_t)k * nm1 + i) * nm2 + j] = out[k];
+            }
+        }
+        free(ad);
+        free(out);
+    }
+    free(inv_sigma2);
+    free(S1);
+    free(S2);
+    free(self1);
+    free(self2);
+}
+
+/* fget_symmetric_kernels_arad: farad_kernels.f90:619-755. K (nsig, nm, nm). */
+void orc_arad_symmetric_kernels(const double *Q1, const double *Z1, const int *N1,
+                                const double *sigmas, int nm1, int nsig, int amax, double width,
+                                double cut, double rw, double cw, double *K)
+{
+    double *inv_sigma2 = (double *)malloc(sizeof(double) * (nsig > 0 ? nsig : 1));
+    for (int k = 0; k < nsig; ++k) inv_sigma2[k] = -1.0 / (sigmas[k] * sigmas[k]); /* :685 */
+    double *S1 = orc_arad_sines(Q1, N1, nm1, amax, cut, 0);
+    double *self1 = orc_arad_self(Q1, N1, S1, nm1, amax, width, cut, rw, cw);
+#pragma omp parallel
+    {
+        double *ad = (double *)malloc(sizeof(double) * (size_t)amax * amax);
+        double *out = (double *)malloc(sizeof(double) * (nsig > 0 ? nsig : 1));
+#pragma omp for schedule(dynamic, 1)
+        for (int j = 0; j < nm1; ++j) {      /* :717-718 */
+            for (int i = 0; i <= j; ++i) {   /* :720 only i <= j */
+                orc_arad_pair(Q1, Z1, N1, S1, self1, i, Q1, Z1, N1, S1, self1, j, amax, width,
+                              cut, rw, cw, inv_sigma2, nsig, ad, out);
+                for (int k = 0; k < nsig; ++k) {
+                    K[((size_t)k * nm1 + i) * nm1 + j] = out[k];
+                    K[((size_t)k * nm1 + j) * nm1 + i] = out[k]; /* :744 mirror */
+                }
+            }
+        }
+        free(ad);
+        free(out);
+    }
+    free(inv_sigma2);
+    free(S1);
+    free(self1);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Cholesky: restatement of LAPACK dpotrf('U') / dpotrs('U') as called by     */
+/* fcho_solve.f90:35-42 (unblocked "dpotf2" column order, Golub & Van Loan    */
+/* Algorithm 4.2.1). A is the numpy (n, n) array in C order; its upper        */
+/* triangle A[i][j], i <= j, is the Fortran A(i,j) upper triangle.            */
+/* On exit the upper triangle holds U with A = U^T U. Returns LAPACK info:    */
+/* 0, or the 1-based column of the first non-positive pivot.                  */
+/* ------------------------------------------------------------------------ */
+int orc_potrf_upper(int n, double *A)
+{
+    for (int j = 0; j < n; ++j) {
+        double ajj = A[(size_t)j * n + j];
+        for (int k = 0; k < j; ++k) ajj -= A[(size_t)k * n + j] * A[(size_t)k * n + j];
+        if (!(ajj > 0.0)) {
+            A[(size_t)j * n + j] = ajj;
+            return j + 1;
+        }
+        ajj = sqrt(ajj);
+        A[(size_t)j * n + j] = ajj;
+#pragma omp parallel for schedule(static)
+        for (int c = j + 1; c < n; ++c) {
+            double s = A[(size_t)j * n + c];
+            for (int k = 0; k < j; ++k) s -= A[(size_t)k * n + j] * A[(size_t)k * n + c];
+            A[(size_t)j * n + c] = s / ajj;
+        }
+    }
+    return 0;
+}
+
+/* dpotrs('U', nrhs=1): solve U^T z = b, then U x = z, in place in x. */
+void orc_potrs_upper(int n, const double *U, double *x)
+{
+    for (int i = 0; i < n; ++i) {
+        double s = x[i];
+        for (int k = 0; k < i; ++k) s -= U[(size_t)k * n + i] * x[k];
+        x[i] = s / U[(size_t)i * n + i];
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        double s = x[i];
+        for (int k = i + 1; k < n; ++k) s -= U[(size_t)i * n + k] * x[k];
+        x[i] = s / U[(size_t)i * n + i];
+    }
+}
+
+int orc_num_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

@@ -1,0 +1,71 @@
+"""Host-side logic that needs no GPU: tables, marshalling, generators, errors."""
+
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import fml_b200
+from fml_b200 import data, synthetic
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_ptp_of_matches_table():
+    z = np.array([1, 6, 7, 8, 16, 101, 102])
+    np.testing.assert_array_equal(data.ptp_of(z), [[1, 1], [2, 4], [2, 5], [2, 6], [3, 6],
+                                                   [7, 32], [7, 14]])
+    with pytest.raises(KeyError):
+        data.ptp_of([0])
+    with pytest.raises(KeyError):
+        data.ptp_of([119])
+
+
+def test_synthetic_generator_is_seeded_and_valid():
+    a = synthetic.generate(50, nmax=23, seed=7)
+    b = synthetic.generate(50, nmax=23, seed=7)
+    np.testing.assert_array_equal(a.coords, b.coords)
+    np.testing.assert_array_equal(a.energies, b.energies)
+    n = a.natoms
+    assert n.min() >= 4 and n.max() <= 23
+    assert set(np.unique(a.charges)) <= {1.0, 6.0, 7.0, 8.0, 16.0}
+    for i in range(a.nmol):
+        z, r = a.molecule(i)
+        d = np.sqrt(((r[:, None] - r[None]) ** 2).sum(-1))
+        assert (d[np.triu_indices(len(z), 1)] >= synthetic.MIN_PAIR_DIST).all()
+        assert (np.linalg.norm(r, axis=1) <= 1.5 * len(z) ** (1 / 3) + 1e-12).all()
+    sub = a.subset([3, 1])
+    assert sub.nmol == 2 and sub.natoms[0] == a.natoms[3]
+
+
+def test_read_xyz(tmp_path):
+    p = tmp_path / "m.xyz"
+    p.write_text("3\ncomment\n O 0.0 0.0 0.1\n H 0.7 0.0 -0.4\n H -0.7 0.0 -0.4\n")
+    m = fml_b200.Molecule()
+    m.read_xyz(str(p))
+    assert m.natoms == 3
+    assert m.nuclear_charges == [8, 1, 1]
+    assert m.coordinates.shape == (3, 3)
+
+
+def test_no_cpu_fallback_without_gpu():
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        fml_b200.gaussian_kernel(np.ones((4, 3)), np.ones((4, 2)), 1.0)
+
+
+def test_cho_solve_shape_errors():
+    with pytest.raises(ValueError, match="expected square matrix"):
+        fml_b200.cho_solve(np.ones((3, 4)), np.ones(3))
+    with pytest.raises(ValueError, match="same stride size"):
+        fml_b200.cho_solve(np.eye(3), np.ones(4))
+
+
+def test_arad_size_asserts():
+    X = np.zeros((2, 5, 5, 5))
+    with pytest.raises(AssertionError, match="code = 2"):
+        fml_b200.get_atomic_kernels_arad(X, np.zeros((2, 4, 5, 4)), [[1], [1]], [[1], [1]], [1.0])
+    with pytest.raises(AssertionError, match="code = 4"):
+        fml_b200.get_atomic_symmetric_kernels_arad(X, [[1]], [1.0])

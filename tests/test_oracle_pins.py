@@ -1,0 +1,111 @@
+"""Pins the CPU oracle against the reference's own outputs (tests/golden/).
+
+The fixtures were produced by tests/golden/make_golden.py from the
+reference's Python-3-runnable code: ARAD.describe (fml/arad.py), the
+pure-Python sorted Coulomb matrix (fml/representations/representations.py:63-113)
+and the ARAD distance/kernel restatement of tests/test_arad.py:172-310,
+evaluated as tests/test_arad.py:319-400 does.
+"""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from fml_b200.data import NUCLEAR_CHARGE, PTP
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _mols(g, prefix):
+    off = g[prefix + "offsets"]
+    return [(g[prefix + "charges"][off[i]:off[i + 1]], g[prefix + "coords"][off[i]:off[i + 1]])
+            for i in range(len(off) - 1)]
+
+
+def test_tables_match_reference():
+    t = json.load(open(os.path.join(HERE, "golden", "reference_tables.json")))
+    assert {int(k): v for k, v in t["PTP"].items()} == PTP
+    assert t["NUCLEAR_CHARGE"] == NUCLEAR_CHARGE
+
+
+@pytest.mark.parametrize("size", [23, 30])
+def test_cm_oracle_matches_reference_python(golden, oracle_mod, size):
+    g = golden
+    cm = oracle_mod.coulomb_matrices(g["xyz_charges"], g["xyz_coords"], g["xyz_offsets"], size)
+    ref = g["cm_xyz_s%d" % size]
+    np.testing.assert_allclose(cm, ref, rtol=1e-14, atol=1e-13)
+
+
+def test_cm_oracle_matches_reference_python_synthetic(golden, oracle_mod):
+    g = golden
+    cm = oracle_mod.coulomb_matrices(g["syn12_charges"], g["syn12_coords"], g["syn12_offsets"], 23)
+    np.testing.assert_allclose(cm, g["cm_syn_s23"], rtol=1e-14, atol=1e-13)
+
+
+@pytest.mark.parametrize("key,size,cut", [("xyz_s30_c5", 30, 5.0), ("xyz_s20_c5", 20, 5.0),
+                                          ("xyz_s23_c1e+06", 23, 1e6), ("xyz_s23_c5", 23, 5.0)])
+def test_arad_describe_oracle_matches_reference(golden, oracle_mod, key, size, cut):
+    g = golden
+    d = oracle_mod.arad_descriptors(g["xyz_charges"], g["xyz_coords"], g["xyz_offsets"], size, cut)
+    np.testing.assert_allclose(d, g["arad_" + key], rtol=1e-13, atol=1e-14)
+
+
+@pytest.mark.parametrize("cut", [5.0, 1e6])
+def test_arad_describe_oracle_matches_reference_synthetic(golden, oracle_mod, cut):
+    g = golden
+    d = oracle_mod.arad_descriptors(g["syn11_charges"], g["syn11_coords"], g["syn11_offsets"],
+                                    23, cut)
+    np.testing.assert_allclose(d, g["arad_syn_s23_c%g" % cut], rtol=1e-13, atol=1e-14)
+
+
+def test_arad_kernel_oracle_matches_reference_test_restatement(golden, oracle_mod):
+    """tests/test_arad.py:358-399: 5 vs 5 fixture molecules, sigmas {0.1, 1, 10, 100}."""
+    g = golden
+    x = g["arad_xyz_s30_c5"]
+    Z = [z for z, _ in _mols(g, "xyz_")]
+    K = oracle_mod.get_atomic_kernels_arad(x[:5], x[5:], Z[:5], Z[5:], g["testarad_sigmas"])
+    np.testing.assert_allclose(K, g["testarad_K_5v5"], rtol=1e-11)
+
+
+def test_arad_symmetric_kernel_oracle_matches_reference_test_restatement(golden, oracle_mod):
+    # the test restatement has no |l2| < 5e-12 clamp (farad_kernels.f90:735); on the
+    # diagonal (identical atoms, l2 ~ 1e-15) that changes exp(-l2/0.1**2) by ~1e-10
+    g = golden
+    x = g["arad_xyz_s30_c5"]
+    Z = [z for z, _ in _mols(g, "xyz_")]
+    K = oracle_mod.get_atomic_symmetric_kernels_arad(x, Z, g["testarad_sigmas"])
+    np.testing.assert_allclose(K, g["testarad_K_10v10"], rtol=1e-9)
+
+
+def test_arad_kernel_oracle_synthetic_far_cut(golden, oracle_mod):
+    """Descriptor cut 1e6 (neighbours beyond the kernel cut of 6.0 are dropped)."""
+    g = golden
+    x = g["arad_syn_s23_c1e+06"][:12]
+    Z = [z for z, _ in _mols(g, "syn11_")][:12]
+    K = oracle_mod.get_atomic_kernels_arad(x[:6], x[6:], Z[:6], Z[6:], g["testarad_syn_sigmas"])
+    np.testing.assert_allclose(K, g["testarad_syn_K_6v6"], rtol=1e-11)
+
+
+def test_oracle_cho_solve_restatement_matches_lapack(oracle_mod):
+    rng = np.random.default_rng(3)
+    M = rng.standard_normal((120, 120))
+    A = M @ M.T + 120 * np.eye(120)
+    y = rng.standard_normal(120)
+    x1, i1 = oracle_mod.cho_solve(A, y)
+    x2, i2 = oracle_mod.cho_solve_restated(A, y)
+    assert i1 == i2 == 0
+    np.testing.assert_allclose(x1, x2, rtol=1e-12)
+    B = A.copy()
+    B[37, 37] = -1.0
+    assert oracle_mod.cho_solve(B, y)[1] == oracle_mod.cho_solve_restated(B, y)[1] == 38
+
+
+def test_oracle_symmetric_equals_general(golden, oracle_mod):
+    g = golden
+    x = g["arad_xyz_s23_c5"]
+    Z = [z for z, _ in _mols(g, "xyz_")]
+    s = [0.5, 2.0]
+    np.testing.assert_allclose(oracle_mod.get_atomic_symmetric_kernels_arad(x, Z, s),
+                               oracle_mod.get_atomic_kernels_arad(x, x, Z, Z, s), rtol=1e-13)

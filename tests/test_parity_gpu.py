@@ -1,0 +1,256 @@
+"""GPU parity: every hot-path entry point against the CPU oracle and the
+reference's golden fixtures, through the C ABI (libfmlb.so).
+
+Tolerances (stated per test):
+* Coulomb matrices: sort order bit-exact; values to 1e-14 relative.
+* ARAD descriptors: 1e-12 relative / 1e-13 absolute (padding 1e100 exact).
+* Gaussian / Laplacian FP64: 1e-12 relative.
+* ARAD kernels FP64: 1e-12 relative against the oracle.
+* cho_solve FP64: 1e-10 relative on well-conditioned systems; LAPACK info equal.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import fml_b200
+from fml_b200 import synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def _mols(g, prefix):
+    off = g[prefix + "offsets"]
+    return [(g[prefix + "charges"][off[i]:off[i + 1]], g[prefix + "coords"][off[i]:off[i + 1]])
+            for i in range(len(off) - 1)]
+
+
+# ---------------------------------------------------------------------------
+# descriptors
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("nmax,seed,nmol", [(23, 0, 700), (29, 2, 500), (5, 3, 64), (40, 4, 64)])
+def test_coulomb_matrices_vs_oracle(oracle_mod, nmax, seed, nmol):
+    b = synthetic.generate(nmol, nmax=nmax, seed=seed, nmin=1 if nmax < 6 else 4)
+    cm, order = fml_b200.generate_coulomb_matrices(b.charges, b.coords, b.offsets, size=nmax,
+                                                   return_order=True)
+    ref, ref_order = oracle_mod.coulomb_matrices(b.charges, b.coords, b.offsets, nmax,
+                                                 return_order=True)
+    np.testing.assert_array_equal(order, ref_order)          # bit-exact permutation
+    np.testing.assert_allclose(cm, ref, rtol=1e-14, atol=0)
+
+
+def test_coulomb_matrix_ties_go_to_higher_index(oracle_mod):
+    # two identical H atoms mirrored through the C: equal row norms
+    z = np.array([6.0, 1.0, 1.0])
+    r = np.array([[0.0, 0.0, 0.0], [1.1, 0.0, 0.0], [-1.1, 0.0, 0.0]])
+    cm, order = fml_b200.generate_coulomb_matrices(z, r, [0, 3], size=4, return_order=True)
+    _, ref_order = oracle_mod.generate_coulomb_matrix(z, r, 4, return_order=True)
+    assert list(order[0, :3]) == list(ref_order) == [0, 2, 1]
+
+
+@pytest.mark.parametrize("size", [23, 30])
+def test_coulomb_matrices_vs_reference_python(golden, size):
+    g = golden
+    cm = fml_b200.generate_coulomb_matrices(g["xyz_charges"], g["xyz_coords"], g["xyz_offsets"],
+                                            size=size)
+    np.testing.assert_allclose(cm, g["cm_xyz_s%d" % size], rtol=1e-14, atol=1e-13)
+
+
+def test_molecule_dropin(golden):
+    g = golden
+    for i, (z, r) in enumerate(_mols(g, "xyz_")):
+        m = fml_b200.Molecule()
+        m.nuclear_charges = list(z)
+        m.coordinates = r
+        m.natoms = len(z)
+        m.generate_coulomb_matrix(size=23)
+        np.testing.assert_allclose(m.coulomb_matrix, g["cm_xyz_s23"][i], rtol=1e-14, atol=1e-13)
+        m.generate_arad_descriptor(size=30)
+        np.testing.assert_allclose(m.arad_descriptor, g["arad_xyz_s30_c5"][i], rtol=1e-12,
+                                   atol=1e-13)
+
+
+def test_coulomb_oversize_raises():
+    with pytest.raises(ValueError):
+        fml_b200.generate_coulomb_matrices(np.ones(5), np.random.rand(5, 3), [0, 5], size=4)
+
+
+@pytest.mark.parametrize("key,size,cut", [("xyz_s30_c5", 30, 5.0), ("xyz_s20_c5", 20, 5.0),
+                                          ("xyz_s23_c1e+06", 23, 1e6)])
+def test_arad_descriptors_vs_reference(golden, key, size, cut):
+    g = golden
+    d = fml_b200.generate_arad_descriptors(g["xyz_charges"], g["xyz_coords"], g["xyz_offsets"],
+                                           size=size, cut=cut)
+    np.testing.assert_allclose(d, g["arad_" + key], rtol=1e-12, atol=1e-13)
+
+
+@pytest.mark.parametrize("cut,nmax", [(5.0, 23), (1e6, 23), (5.0, 29), (3.0, 64)])
+def test_arad_descriptors_vs_oracle(oracle_mod, cut, nmax):
+    b = synthetic.generate(150, nmax=nmax, seed=21)
+    d = fml_b200.generate_arad_descriptors(b.charges, b.coords, b.offsets, size=nmax, cut=cut)
+    ref = oracle_mod.arad_descriptors(b.charges, b.coords, b.offsets, nmax, cut)
+    np.testing.assert_allclose(d, ref, rtol=1e-12, atol=1e-13)
+
+
+def test_arad_unknown_element_raises():
+    with pytest.raises(KeyError):
+        fml_b200.generate_arad_descriptors(np.array([1.0, 0.0]), np.random.rand(2, 3), [0, 2])
+
+
+# ---------------------------------------------------------------------------
+# Gaussian / Laplacian
+# ---------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def cm_small(oracle_mod):
+    b = synthetic.generate(523, nmax=23, seed=5)
+    return oracle_mod.coulomb_matrices(b.charges, b.coords, b.offsets, 23)
+
+
+@pytest.mark.parametrize("fn", ["gaussian_kernel", "laplacian_kernel"])
+@pytest.mark.parametrize("sigma", [724.0, 50.0])
+def test_pairwise_kernel_vs_oracle(oracle_mod, cm_small, fn, sigma):
+    A = cm_small[:317].T  # reference layout (d, na)
+    B = cm_small[317:].T
+    K = getattr(fml_b200, fn)(A, B, sigma)
+    ref = getattr(oracle_mod, fn)(A, B, sigma)
+    assert K.shape == (317, 206)
+    np.testing.assert_allclose(K, ref, rtol=1e-12, atol=1e-300)
+
+
+@pytest.mark.parametrize("fn", ["gaussian_kernel", "laplacian_kernel"])
+def test_pairwise_kernel_symmetric_and_multi_sigma(oracle_mod, cm_small, fn):
+    A = cm_small[:263].T
+    sig = [100.0, 400.0, 1600.0]
+    Ks = getattr(fml_b200, fn)(A, A, sig)              # A is A -> symmetric build
+    Kf = getattr(fml_b200, fn)(A, A.copy(), sig)       # full build
+    assert Ks.shape == (3, 263, 263)
+    np.testing.assert_array_equal(Ks, Kf)
+    for k, s in enumerate(sig):
+        np.testing.assert_array_equal(Ks[k], Ks[k].T)
+        np.testing.assert_allclose(Ks[k], getattr(oracle_mod, fn)(A, A, s), rtol=1e-12)
+
+
+def test_pairwise_kernel_torch_in_torch_out(oracle_mod, cm_small):
+    A = torch.from_numpy(cm_small[:64].T.copy()).cuda()
+    K = fml_b200.gaussian_kernel(A, A, 300.0)
+    assert isinstance(K, torch.Tensor) and K.is_cuda
+    np.testing.assert_allclose(K.cpu().numpy(),
+                               oracle_mod.gaussian_kernel(cm_small[:64].T, cm_small[:64].T, 300.0),
+                               rtol=1e-12)
+
+
+def test_pairwise_kernel_edge_sizes(oracle_mod):
+    rng = np.random.default_rng(0)
+    for na, nb, d in [(1, 1, 1), (1, 70, 3), (65, 1, 17), (129, 130, 33)]:
+        A = rng.standard_normal((d, na))
+        B = rng.standard_normal((d, nb))
+        np.testing.assert_allclose(fml_b200.gaussian_kernel(A, B, 2.0),
+                                   oracle_mod.gaussian_kernel(A, B, 2.0), rtol=1e-12)
+        np.testing.assert_allclose(fml_b200.laplacian_kernel(A, B, 2.0),
+                                   oracle_mod.laplacian_kernel(A, B, 2.0), rtol=1e-12)
+
+
+# ---------------------------------------------------------------------------
+# ARAD kernels
+# ---------------------------------------------------------------------------
+def test_arad_kernels_vs_reference_test(golden):
+    """tests/test_arad.py:358-399 fixture comparison, now with an assertion."""
+    g = golden
+    x = g["arad_xyz_s30_c5"]
+    Z = [list(z) for z, _ in _mols(g, "xyz_")]
+    K = fml_b200.get_atomic_kernels_arad(x[:5], x[5:], Z[:5], Z[5:], list(g["testarad_sigmas"]))
+    np.testing.assert_allclose(K, g["testarad_K_5v5"], rtol=1e-11)
+
+
+@pytest.mark.parametrize("cut_desc", [5.0, 1e6])
+def test_arad_kernels_vs_oracle(oracle_mod, cut_desc):
+    b = synthetic.generate(40, nmax=23, seed=31)
+    X = oracle_mod.arad_descriptors(b.charges, b.coords, b.offsets, 23, cut_desc)
+    Z = [b.molecule(i)[0] for i in range(b.nmol)]
+    sig = [0.1, 0.5, 1.0, 2.0, 5.0]
+    K = fml_b200.get_atomic_kernels_arad(X[:25], X[25:], Z[:25], Z[25:], sig)
+    ref = oracle_mod.get_atomic_kernels_arad(X[:25], X[25:], Z[:25], Z[25:], sig)
+    np.testing.assert_allclose(K, ref, rtol=1e-12, atol=1e-300)
+    Ks = fml_b200.get_atomic_symmetric_kernels_arad(X, Z, sig)
+    refs = oracle_mod.get_atomic_symmetric_kernels_arad(X, Z, sig)
+    np.testing.assert_allclose(Ks, refs, rtol=1e-12, atol=1e-300)
+
+
+def test_arad_kernels_fp32_error_bound(oracle_mod):
+    b = synthetic.generate(40, nmax=23, seed=32)
+    X = oracle_mod.arad_descriptors(b.charges, b.coords, b.offsets, 23, 1e6)
+    Z = [b.molecule(i)[0] for i in range(b.nmol)]
+    sig = [0.5, 1.0, 2.0, 5.0]
+    K32 = fml_b200.get_atomic_symmetric_kernels_arad(X, Z, sig, precision="fp32")
+    K64 = oracle_mod.get_atomic_symmetric_kernels_arad(X, Z, sig)
+    rel = np.abs(K32 - K64) / np.maximum(np.abs(K64), 1e-300)
+    assert rel.max() < 2e-3, rel.max()
+
+
+# ---------------------------------------------------------------------------
+# Cholesky
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("n", [1, 63, 64, 65, 200, 700])
+def test_cho_solve_vs_lapack(oracle_mod, cm_small, n):
+    rng = np.random.default_rng(n)
+    M = rng.standard_normal((n, n))
+    A = M @ M.T / n + np.eye(n)
+    y = rng.standard_normal(n)
+    x = fml_b200.cho_solve(A, y)
+    ref, info = oracle_mod.cho_solve(A, y)
+    assert info == 0
+    np.testing.assert_allclose(x, ref, rtol=1e-10, atol=1e-12)
+
+
+def test_cho_solve_kernel_matrix(oracle_mod, cm_small):
+    X = cm_small[:500]
+    K = oracle_mod.gaussian_kernel(X.T, X.T, 724.0) + 1e-2 * np.eye(500)
+    y = np.random.default_rng(1).standard_normal(500)
+    x = fml_b200.cho_solve(K, y)
+    ref, _ = oracle_mod.cho_solve(K, y)
+    np.testing.assert_allclose(x, ref, rtol=1e-9, atol=1e-9 * np.abs(ref).max())
+
+
+def test_cho_solve_reads_upper_triangle_only(oracle_mod):
+    rng = np.random.default_rng(2)
+    M = rng.standard_normal((90, 90))
+    A = M @ M.T + 90 * np.eye(90)
+    y = rng.standard_normal(90)
+    B = A.copy()
+    B[np.tril_indices(90, -1)] = 1e6  # garbage below the diagonal
+    np.testing.assert_allclose(fml_b200.cho_solve(B, y), oracle_mod.cho_solve(A, y)[0],
+                               rtol=1e-10)
+
+
+def test_cho_solve_not_positive_definite_warns(oracle_mod):
+    A = np.eye(150) * 2.0
+    A[100, 100] = -1.0
+    y = np.ones(150)
+    with pytest.warns(fml_b200.CholeskyWarning, match="error code: 101"):
+        fml_b200.cho_solve(A, y)
+    assert oracle_mod.cho_solve(A, y)[1] == 101
+    with pytest.raises(np.linalg.LinAlgError):
+        fml_b200.cho_solve(A, y, strict=True)
+
+
+# ---------------------------------------------------------------------------
+# end to end: plain FP64 KRR on sorted Coulomb matrices (2000 molecules)
+# ---------------------------------------------------------------------------
+def test_krr_plain_fp64_end_to_end(oracle_mod):
+    b = synthetic.generate(2000, nmax=23, seed=0)
+    X = fml_b200.generate_coulomb_matrices(b.charges, b.coords, b.offsets, size=23)
+    Xr = oracle_mod.coulomb_matrices(b.charges, b.coords, b.offsets, 23)
+    np.testing.assert_allclose(X, Xr, rtol=1e-14)
+    tr, te = slice(0, 1000), slice(1000, 2000)
+    sigma, lam = 724.0, 1e-8
+    K = fml_b200.gaussian_kernel(X[tr].T, X[tr].T, sigma)
+    K[np.diag_indices_from(K)] += lam
+    alpha = fml_b200.cho_solve(K, b.energies[tr])
+    Ks = fml_b200.gaussian_kernel(X[te].T, X[tr].T, sigma)
+    mae = np.abs(Ks @ alpha - b.energies[te]).mean()
+    Kr = oracle_mod.gaussian_kernel(Xr[tr].T, Xr[tr].T, sigma)
+    Kr[np.diag_indices_from(Kr)] += lam
+    ar, _ = oracle_mod.cho_solve(Kr, b.energies[tr])
+    mae_r = np.abs(oracle_mod.gaussian_kernel(Xr[te].T, Xr[tr].T, sigma) @ ar
+                   - b.energies[te]).mean()
+    assert abs(mae - mae_r) <= 1e-6 * mae_r, (mae, mae_r)
