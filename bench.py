@@ -1,0 +1,367 @@
+"""Benchmark of the KRR hot path on B200.
+
+Workload (default): large-N Gaussian KRR on sorted Coulomb matrices —
+N_train = 32768, N_test = 8192 synthetic molecules with 4..29 atoms
+(descriptor length 435), sigma in {100, 400, 1600}, lambda = 1e-8, FP64.
+One step = one full pass of the hot path over the batch: sorted Coulomb
+matrices from coordinates, the symmetric training kernel for all sigmas,
+K + lambda I, Cholesky factorisation and solve per sigma, and the fused
+prediction of all test molecules for every sigma.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU runs are independent replicas (one problem per GPU, no data-path
+collective; the KRR problem does not shard), so scaling is weak.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# the CPU baseline's OpenMP / OpenBLAS thread counts must be set before those
+# libraries initialise
+_CORES = len(os.sched_getaffinity(0))
+os.environ.setdefault("OMP_NUM_THREADS", str(_CORES))
+os.environ.setdefault("OPENBLAS_NUM_THREADS", str(_CORES))
+
+import numpy as np  # noqa: E402
+
+METRIC = "kernel entries/s & KRR solves/s at stated MAE vs FP64 oracle; p50/p99 latency"
+UNIT = "kernel entries/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--ntrain", type=int, default=32768)
+    p.add_argument("--ntest", type=int, default=8192)
+    p.add_argument("--nmax", type=int, default=29)
+    p.add_argument("--sigmas", default="100,400,1600")
+    p.add_argument("--lam", type=float, default=1e-8)
+    p.add_argument("--seed", type=int, default=2)
+    p.add_argument("--cpu-ntrain", type=int, default=4096)
+    p.add_argument("--cpu-ntest", type=int, default=1024)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def entries_per_step(ntrain, ntest, nsig):
+    return (ntrain * ntrain + ntest * ntrain) * nsig
+
+
+def workload_name(a, nsig):
+    return ("gaussian KRR on sorted Coulomb matrices: N_train=%d, N_test=%d, nmax=%d (d=%d), "
+            "sigma=%s, lambda=%g, FP64" % (a.ntrain, a.ntest, a.nmax, a.nmax * (a.nmax + 1) // 2,
+                                          a.sigmas, a.lam))
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if r[5 + i].lower().startswith("active")})
+        loaded = [v for v in sm if v > 0.5 * smax] or sm
+        return {"sm_mhz": float(np.median(loaded)), "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle port (C/OpenMP restatement + LAPACK via scipy)
+# ---------------------------------------------------------------------------
+def cpu_krr_sample(a, sigmas, seed):
+    import oracle
+    from fml_b200 import synthetic
+    oracle.build()
+    b = synthetic.generate(a.cpu_ntrain + a.cpu_ntest, nmax=a.nmax, seed=seed)
+
+    def one():
+        X = oracle.coulomb_matrices(b.charges, b.coords, b.offsets, a.nmax)
+        tr, te = X[:a.cpu_ntrain], X[a.cpu_ntrain:]
+        preds = []
+        for s in sigmas:  # the reference builds one sigma per call
+            K = oracle.gaussian_kernel(tr.T, tr.T, s)
+            K[np.diag_indices_from(K)] += a.lam
+            alpha, _ = oracle.cho_solve(K, b.energies[:a.cpu_ntrain])
+            preds.append(oracle.gaussian_kernel(te.T, tr.T, s) @ alpha)
+        return np.array(preds)
+
+    return one, b
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sigmas = [float(s) for s in a.sigmas.split(",")]
+    one, _ = cpu_krr_sample(a, sigmas, a.seed)
+    for _ in range(a.warmup):
+        one()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        one()
+    dt = (time.perf_counter() - t0) / a.steps
+    v = entries_per_step(a.cpu_ntrain, a.cpu_ntest, len(sigmas)) / dt
+    sample = ("N_train=%d, N_test=%d per step (bounded sample of the workload; same descriptors, "
+              "sigmas and lambda)" % (a.cpu_ntrain, a.cpu_ntest))
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(a, len(sigmas)), "sample": sample},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": _CORES, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def measure_syrk(pipe, torch, lib_call, ptr, stream):
+    """Per-launch timing of the dominant kernel (FP64 trailing update) over the
+    exact launch sequence of one factorisation, on the pipeline's K buffer."""
+    from fml_b200.krr import PANEL
+    n = pipe.n_train
+    K = pipe.K[0]
+    evs = []
+    flops = 0.0
+    for k0 in range(0, n, PANEL):
+        kn = min(PANEL, n - k0)
+        base = k0 + kn
+        m = n - base
+        if m <= 0:
+            break
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        Cv = K[base:, base:]
+        Pv = K[base:, k0:k0 + kn]
+        lib_call("fmlb_syrk_lower_f64", ptr(Cv), n, m, ptr(Pv), n, kn, None, stream)
+        e1.record()
+        evs.append((e0, e1))
+        flops += float(m) * (m + 1) * kn
+    torch.cuda.synchronize()
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
+    return flops, ms, len(evs)
+
+
+def measure_dgemm_peak(torch):
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    best = 1e30
+    for _ in range(4):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def run_ours(a):
+    import torch
+    import torch.distributed as dist
+
+    import fml_b200
+    from fml_b200 import _lib, krr, synthetic
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    sigmas = [float(s) for s in a.sigmas.split(",")]
+    nsig = len(sigmas)
+    n_mol = a.ntrain + a.ntest
+    b = synthetic.generate(n_mol, nmax=a.nmax, seed=a.seed + 1000 * rank)
+    dev = torch.device("cuda", local)
+    z = torch.from_numpy(b.charges).to(dev)
+    r = torch.from_numpy(b.coords).to(dev)
+    o = torch.from_numpy(b.offsets).to(dev)
+    y = torch.from_numpy(np.ascontiguousarray(b.energies[:a.ntrain])).to(dev)
+    pipe = krr.KRRPipeline(n_mol, a.ntrain, a.nmax, sigmas, a.lam)
+    stream = torch.cuda.current_stream()
+
+    for _ in range(a.warmup):
+        pipe.run(z, r, o, y)
+    torch.cuda.synchronize()
+    info = pipe.info.cpu().numpy()
+    pred = pipe.pred[:, :a.ntest].cpu().numpy()
+    yt = b.energies[a.ntrain:]
+    mae = {str(s): float(np.abs(pred[k] - yt).mean()) for k, s in enumerate(sigmas)}
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        pipe.run(z, r, o, y)
+    e1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / a.steps
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    per_step = entries_per_step(a.ntrain, a.ntest, nsig)
+    value = world * per_step / (ms * 1e-3)
+
+    # end to end through the public API with host (pinned) inputs
+    e2e = None
+    if not a.no_e2e:
+        hz = torch.from_numpy(b.charges).pin_memory()
+        hr = torch.from_numpy(b.coords).pin_memory()
+        ho = torch.from_numpy(b.offsets).pin_memory()
+        hy = torch.from_numpy(np.ascontiguousarray(b.energies[:a.ntrain])).pin_memory()
+        h2d = sum(t.numel() * t.element_size() for t in (hz, hr, ho, hy))
+        out_host = torch.empty((nsig, a.ntest), dtype=torch.float64).pin_memory()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(a.steps):
+            dz, dr = hz.to(dev, non_blocking=True), hr.to(dev, non_blocking=True)
+            do, dy = ho.to(dev, non_blocking=True), hy.to(dev, non_blocking=True)
+            p = pipe.run(dz, dr, do, dy)
+            out_host.copy_(p, non_blocking=True)
+        s1.record()
+        torch.cuda.synchronize()
+        ems = s0.elapsed_time(s1) / a.steps
+        if world > 1:
+            t = torch.tensor([ems], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": world * per_step / (ems * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(nsig * a.ntest * 8),
+               "ms_per_step": ems, "api": "fml_b200.krr.KRRPipeline.run on host-pinned inputs"}
+
+    # dominant kernel: FP64 trailing update of the factorisation
+    flops, syrk_ms, nl = measure_syrk(pipe, torch, _lib.call, _lib.ptr, _lib.stream_handle())
+    peak = measure_dgemm_peak(torch)
+    achieved = flops / (syrk_ms * 1e-3) / 1e12
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "syrk_update_f64_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("bytes_per_launch")
+        except (OSError, ValueError):
+            traffic = None
+    roofline = {"bound": "fp64", "kernel": "syrk_dmma_kernel (FP64 trailing update)",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json "
+                               "holds no FP64 figure)",
+                "traffic": traffic, "launches": nl, "avg_launch_ms": syrk_ms / nl,
+                "share_of_step": syrk_ms * nsig / ms,
+                "algorithmic_flops_per_launch": flops / nl}
+
+    cpu = None
+    if rank == 0 and not a.no_cpu_baseline:
+        one, _ = cpu_krr_sample(a, sigmas, a.seed)
+        one()
+        t0 = time.perf_counter()
+        one()
+        dt = time.perf_counter() - t0
+        cpu = {"value": entries_per_step(a.cpu_ntrain, a.cpu_ntest, nsig) / dt, "unit": UNIT,
+               "cores": _CORES, "kind": "port",
+               "sample": "N_train=%d, N_test=%d, same sigmas/lambda, one step of %.1f s"
+                         % (a.cpu_ntrain, a.cpu_ntest, dt)}
+
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic seeded molecules (fml_b200/synthetic.py)",
+            "config": {"workload": workload_name(a, nsig), "n_train": a.ntrain,
+                       "n_test": a.ntest, "sigmas": sigmas, "lambda": a.lam,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (each K is %.1f GB)"
+                             % (a.ntrain ** 2 * 8 / 1e9)},
+            "solves_per_s": world * nsig / (ms * 1e-3),
+            "mae": mae, "potrf_info": [int(v) for v in info],
+            "clocks": clocks, "e2e": e2e, "gpu_launches": pipe.launches_per_run() * a.steps,
+            "roofline": roofline, "cpu_baseline": cpu,
+        }))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -145,6 +145,32 @@ int fmlb_potrf_f64(double *A, long long lda, int n, void *work, int *info, void 
 int fmlb_potrs_f64(const double *L, long long lda, int n, const void *work, double *x,
                    void *stream);
 
+/* Trailing update of the blocked factorisation: C -= P P^T on the triangle
+ * i >= j of the row-major (m, m) matrix C, P is (m, k) with stride ldp; the
+ * other triangle of C is not touched. `info` (device, may be NULL): when it
+ * holds a non-zero value the update is skipped. The step fmlb_potrf_f64 runs
+ * per panel (the LAPACK dsyrk call inside dpotrf, fcho_solve.f90:35). */
+int fmlb_syrk_lower_f64(double *C, long long ldc, int m, const double *P, long long ldp, int k,
+                        const int *info, void *stream);
+
+/* ------------------------------------------------------------------------
+ * KRR helpers, FP64.
+ * fmlb_add_diagonal_f64: A[i, i] += lambda (the user-side K + lambda I that
+ *   precedes cho_solve).
+ * fmlb_kernel_predict_f64: y[s, q] = sum_t k_s(Xq[q], Xt[t]) * alpha[s, t] for
+ *   every sigma s without storing the kernel matrix; kind 0 = Gaussian,
+ *   1 = Laplacian (same kernels as fmlb_gaussian_kernel_f64 /
+ *   fmlb_laplacian_kernel_f64). Replaces the user-side prediction
+ *   gaussian_kernel(Xq, Xt, sigma) @ alpha (pattern of fget_prediction,
+ *   fml/kernels/fkernels.f90:480-539). nsigma <= 8. Deterministic.
+ * ---------------------------------------------------------------------- */
+int fmlb_add_diagonal_f64(double *A, long long lda, int n, double lambda, void *stream);
+size_t fmlb_kernel_predict_workspace_bytes(int nq, int nt, int nsigma);
+int fmlb_kernel_predict_f64(int kind, const double *Xq, int nq, int ldq, const double *Xt, int nt,
+                            int ldt, int d, const double *sigmas_host, int nsigma,
+                            const double *alpha, long long lda_alpha, double *y, long long ldy,
+                            void *workspace, size_t ws_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

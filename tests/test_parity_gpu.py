@@ -254,3 +254,49 @@ def test_krr_plain_fp64_end_to_end(oracle_mod):
     mae_r = np.abs(oracle_mod.gaussian_kernel(Xr[te].T, Xr[tr].T, sigma) @ ar
                    - b.energies[te]).mean()
     assert abs(mae - mae_r) <= 1e-6 * mae_r, (mae, mae_r)
+
+
+@pytest.mark.parametrize("m,k,ld_pad", [(1, 1, 0), (130, 128, 0), (257, 128, 1), (300, 37, 3)])
+def test_syrk_lower_update(m, k, ld_pad):
+    """C -= P P^T on the lower triangle only (FP64 tensor-core kernel), aligned
+    (even stride) and unaligned (odd stride) operand paths, 1e-13 relative."""
+    from fml_b200 import _lib
+    rng = np.random.default_rng(m + k)
+    ld = max(m, k) + ld_pad
+    buf = rng.standard_normal((m, ld))
+    P = rng.standard_normal((m, k))
+    Pbuf = np.zeros((m, ld))
+    Pbuf[:, :k] = P
+    C = torch.from_numpy(buf.copy()).cuda()
+    Pd = torch.from_numpy(Pbuf).cuda()
+    _lib.call("fmlb_syrk_lower_f64", _lib.ptr(C), ld, m, _lib.ptr(Pd), ld, k, None,
+              _lib.stream_handle())
+    out = C.cpu().numpy()
+    ref = buf[:, :m] - P @ P.T
+    low = np.tril_indices(m)
+    np.testing.assert_allclose(out[:, :m][low], ref[low], rtol=1e-13, atol=1e-12)
+    up = np.triu_indices(m, 1)
+    np.testing.assert_array_equal(out[:, :m][up], buf[:, :m][up])
+
+
+@pytest.mark.parametrize("n", [1031, 2304])
+def test_cho_solve_multi_panel(oracle_mod, n):
+    rng = np.random.default_rng(n)
+    M = rng.standard_normal((n, n // 2))
+    A = M @ M.T / n + 0.5 * np.eye(n)
+    y = rng.standard_normal(n)
+    x = fml_b200.cho_solve(A, y)
+    ref, info = oracle_mod.cho_solve(A, y)
+    assert info == 0
+    np.testing.assert_allclose(x, ref, rtol=1e-9, atol=1e-10 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("bad", [1, 33, 300, 1000])
+def test_cho_solve_failure_column_matches_lapack(oracle_mod, bad):
+    n = 1031
+    A = np.eye(n) * 3.0 + 0.01
+    A[bad - 1, bad - 1] = -5.0
+    y = np.ones(n)
+    with pytest.warns(fml_b200.CholeskyWarning, match="error code: %d$" % bad):
+        fml_b200.cho_solve(A, y)
+    assert oracle_mod.cho_solve(A, y)[1] == bad
