@@ -40,6 +40,8 @@ SIGNATURES = {
     "fmlb_kernel_predict_workspace_bytes": (_sz, [_i, _i, _i]),
     "fmlb_kernel_predict_f64": (_i, [_i, _vp, _i, _i, _vp, _i, _i, _i, _dp, _i, _vp, _ll, _vp,
                                      _ll, _vp, _sz, _vp]),
+    "fmlb_kernel_predict_f64_noalloc": (_i, [_i, _vp, _i, _i, _vp, _i, _i, _i, _dp, _i, _vp, _ll,
+                                             _vp, _ll, _vp]),
 }
 
 FMLB_EINVAL = -22

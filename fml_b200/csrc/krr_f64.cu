@@ -190,3 +190,104 @@ extern "C" int fmlb_kernel_predict_f64(int kind, const double *Xq, int nq, int l
                                                                           nq, y, ldy);
     return launch_status("reduce_splits_kernel");
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free prediction.
+//
+// Some callers cannot allocate device memory on the call path: an inference
+// server whose memory is reserved up front by its own arena, a host library
+// that receives only its input and output buffers from a framework that owns
+// all device allocations, or code that must not reach cudaMalloc's implicit
+// synchronisation. For them this variant keeps its split partial sums in the
+// file-scope array below instead of a caller-provided workspace. The array is
+// part of the module image: every GPU that loads the library holds it
+// (8 MiB) until the process exits.
+//
+// The array's name in host code is only a host-side stand-in, so its device
+// address is looked up once per device with cudaGetSymbolAddress, with that
+// device current, on the first call made on that device. Make that first call
+// before any stream capture. All calls share the array; a call fully
+// overwrites the part it reads, so nothing needs clearing between calls, but
+// calls that overlap on the GPU (different streams, or host threads) race on
+// it and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace fmlb {
+namespace {
+
+constexpr size_t kNoAllocScratchDoubles = (size_t)1 << 20;  // 8 MiB
+__device__ __align__(256) double g_predict_scratch[kNoAllocScratchDoubles];
+
+constexpr int kMaxDevices = 64;
+double *g_scratch_ptr[kMaxDevices] = {nullptr};
+std::mutex g_scratch_mutex;
+
+int noalloc_scratch(double **out) {
+    int dev = 0;
+    FMLB_TRY(cuda_status(cudaGetDevice(&dev), "fmlb_kernel_predict_f64_noalloc: cudaGetDevice"));
+    FMLB_REQUIRE(dev >= 0 && dev < kMaxDevices,
+                 "fmlb_kernel_predict_f64_noalloc: device %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_ptr[dev]) {
+        void *p = nullptr;
+        FMLB_TRY(cuda_status(cudaGetSymbolAddress(&p, g_predict_scratch),
+                             "fmlb_kernel_predict_f64_noalloc: cudaGetSymbolAddress"));
+        g_scratch_ptr[dev] = static_cast<double *>(p);
+    }
+    *out = g_scratch_ptr[dev];
+    return FMLB_OK;
+}
+
+}  // namespace
+}  // namespace fmlb
+
+extern "C" int fmlb_kernel_predict_f64_noalloc(int kind, const double *Xq, int nq, int ldq,
+                                               const double *Xt, int nt, int ldt, int d,
+                                               const double *sigmas_host, int nsigma,
+                                               const double *alpha, long long lda_alpha,
+                                               double *y, long long ldy, void *stream) {
+    using namespace fmlb;
+    cudaStream_t st = FMLB_STREAM(stream);
+    FMLB_REQUIRE(kind == 0 || kind == 1, "fmlb_kernel_predict_f64_noalloc: kind must be 0 "
+                                         "(gaussian) or 1 (laplacian)");
+    FMLB_REQUIRE(nq >= 0 && nt >= 0 && d >= 1 && ldq >= d && ldt >= d,
+                 "fmlb_kernel_predict_f64_noalloc: bad sizes");
+    FMLB_REQUIRE(nsigma >= 1 && nsigma <= MAXSIG && sigmas_host,
+                 "fmlb_kernel_predict_f64_noalloc: nsigma must be 1..%d", MAXSIG);
+    FMLB_REQUIRE(lda_alpha >= nt && ldy >= nq,
+                 "fmlb_kernel_predict_f64_noalloc: bad alpha / y stride");
+    if (nq == 0) return FMLB_OK;
+    if (nt == 0) {
+        for (int s = 0; s < nsigma; ++s)
+            FMLB_TRY(cuda_status(cudaMemsetAsync(y + s * ldy, 0, sizeof(double) * nq, st),
+                                 "fmlb_kernel_predict_f64_noalloc: memset"));
+        return FMLB_OK;
+    }
+    const int nsplit = ceil_div(nt, CHUNK);
+    const size_t need = (size_t)nsplit * nsigma * nq;
+    FMLB_REQUIRE(need <= kNoAllocScratchDoubles,
+                 "fmlb_kernel_predict_f64_noalloc: ceil(nt/%d) * nsigma * nq = %zu exceeds the "
+                 "fixed scratch of %zu doubles (8 MiB); split the queries or use "
+                 "fmlb_kernel_predict_f64 with a workspace",
+                 CHUNK, need, kNoAllocScratchDoubles);
+    double *partial = nullptr;
+    FMLB_TRY(noalloc_scratch(&partial));
+    Scales sc;
+    for (int s = 0; s < nsigma; ++s) {
+        const double sg = sigmas_host[s];
+        sc.s[s] = kind == 1 ? -1.0 / sg : -0.5 / (sg * sg);
+    }
+    dim3 grid(ceil_div(nq, BM), nsplit);
+    FMLB_REQUIRE(grid.y <= 65535, "fmlb_kernel_predict_f64_noalloc: training set too large");
+    if (kind == 0)
+        predict_partial_kernel<false><<<grid, TPB, 0, st>>>(Xq, nq, ldq, Xt, nt, ldt, d, sc,
+                                                            nsigma, alpha, lda_alpha, partial);
+    else
+        predict_partial_kernel<true><<<grid, TPB, 0, st>>>(Xq, nq, ldq, Xt, nt, ldt, d, sc, nsigma,
+                                                           alpha, lda_alpha, partial);
+    FMLB_TRY(launch_status("predict_partial_kernel"));
+    reduce_splits_kernel<<<ceil_div((long)nsigma * nq, 256), 256, 0, st>>>(partial, nsplit, nsigma,
+                                                                          nq, y, ldy);
+    return launch_status("reduce_splits_kernel");
+}

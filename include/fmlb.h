@@ -171,6 +171,23 @@ int fmlb_kernel_predict_f64(int kind, const double *Xq, int nq, int ldq, const d
                             const double *alpha, long long lda_alpha, double *y, long long ldy,
                             void *workspace, size_t ws_bytes, void *stream);
 
+/* Allocation-free form of fmlb_kernel_predict_f64 (same arguments minus the
+ * workspace, same results). It has no counterpart in the reference: it exists
+ * for callers that cannot allocate device memory on the call path (a server
+ * whose device memory is all reserved by its own arena up front, or a host
+ * framework that hands the library only input and output buffers). Its
+ * scratch is an 8 MiB array inside the library image, held by every GPU that
+ * loads the library until the process exits, so
+ *   ceil(nt / 1024) * nsigma * nq <= 1048576
+ * and larger calls return FMLB_EINVAL. The first call on each device looks up
+ * the array's device address (with that device current); make it before any
+ * stream capture. All calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
+int fmlb_kernel_predict_f64_noalloc(int kind, const double *Xq, int nq, int ldq, const double *Xt,
+                                    int nt, int ldt, int d, const double *sigmas_host, int nsigma,
+                                    const double *alpha, long long lda_alpha, double *y,
+                                    long long ldy, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
