@@ -75,7 +75,7 @@ def build(force=False, verbose=False, jobs=None):
     if failed:
         raise RuntimeError("nvcc failed for: " + ", ".join(os.path.basename(f) for f in failed))
     tmp = OUT + ".tmp"
-    cmd = [nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs + ["-lcuda"]
+    cmd = [nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs
     subprocess.run(cmd, check=True)
     os.replace(tmp, OUT)
     return OUT

@@ -68,8 +68,53 @@ def _pairwise(A, B, sigma, fn):
     return to_output(out, as_np)
 
 
-def gaussian_kernel(A, B, sigma):
-    """K_ij = exp(-0.5 / sigma**2 * ||A_i - B_j||_2**2), FP64 direct differences."""
+def _gaussian_tc(A, B, sigma):
+    """Tensor-core (tcgen05, BF16 hi/lo x3) Gaussian kernel, FP32 result."""
+    sig, scalar = _sigma_list(sigma)
+    if len(sig) > 8:
+        raise ValueError("the tensor-core path takes at most 8 sigmas per call")
+    symmetric = A is B
+    a, as_np = _descriptor_rows(A)
+    b = a if symmetric else _descriptor_rows(B)[0]
+    if a.shape[1] != b.shape[1]:
+        raise ValueError("A and B must hold descriptors of the same length")
+    na, d = a.shape
+    nb = b.shape[0]
+    dev = device()
+    lib = _lib.load()
+    K = torch.empty((len(sig), na, nb), dtype=torch.float32, device=dev)
+    if na and nb:
+        mu = torch.empty(d, dtype=torch.float64, device=dev)
+        st = _lib.stream_handle()
+        _lib.call("fmlb_column_mean_f64", _lib.ptr(b), nb, d, d, _lib.ptr(mu), st)
+        nbytes = lib.fmlb_tc_operand_bytes(na, d) + (0 if symmetric else
+                                                      lib.fmlb_tc_operand_bytes(nb, d))
+        ws = workspace(nbytes)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        sp, keep = _lib.host_doubles(sig)
+        _lib.call("fmlb_gaussian_kernel_tc", _lib.ptr(a), na, d, _lib.ptr(b), nb, d, d,
+                  _lib.ptr(mu), sp, len(sig), _lib.ptr(K), nb, na * nb, 1 if symmetric else 0,
+                  _lib.ptr(ws), ws.numel(), _lib.ptr(status), st)
+        del keep
+        code = int(status.item())
+        if code:
+            raise _lib.FmlbError(_lib.FMLB_ETIMEDOUT,
+                                 "fmlb_gaussian_kernel_tc: a device-side wait gave up (%d)" % code)
+    out = K[0] if scalar else K
+    return to_output(out, as_np)
+
+
+def gaussian_kernel(A, B, sigma, precision="fp64"):
+    """K_ij = exp(-0.5 / sigma**2 * ||A_i - B_j||_2**2).
+
+    precision="fp64": FP64 direct differences (the reference's arithmetic);
+    precision="bf16x3": tcgen05 tensor cores, BF16 hi/lo splits of the
+    mean-centred descriptors, FP32 result.
+    """
+    if precision == "bf16x3":
+        return _gaussian_tc(A, B, sigma)
+    if precision != "fp64":
+        raise ValueError("precision must be 'fp64' or 'bf16x3'")
     return _pairwise(A, B, sigma, "fmlb_gaussian_kernel_f64")
 
 

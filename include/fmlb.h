@@ -171,6 +171,30 @@ int fmlb_kernel_predict_f64(int kind, const double *Xq, int nq, int ldq, const d
                             const double *alpha, long long lda_alpha, double *y, long long ldy,
                             void *workspace, size_t ws_bytes, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Gaussian kernel matrix on the tcgen05 tensor cores (mixed precision).
+ * Mixed-precision form of fgaussian_kernel (fml/kernels/fkernels.f90:317-349):
+ * K_s[i, j] = exp(-(|x_i|^2 + |x_j|^2 - 2 x_i.x_j) / (2 sigma_s^2)) on
+ * descriptors centred by mu, x_i.x_j from BF16 hi/lo splits with three BF16
+ * products accumulated in FP32; FP32 output (nsigma, na, nb), stride ldk.
+ * Diagonal entries of a symmetric build are exactly 1 and the result is
+ * exactly symmetric. Error against the FP64 kernel: about 6e-5 absolute at
+ * sigma = 100 on Coulomb matrices of 4..29 atoms (1e-5 relative in d^2 for
+ * distinct molecules).
+ *   mu        (d,) device, centring vector (fmlb_column_mean_f64 of the set)
+ *   workspace fmlb_tc_operand_bytes(na, d) (+ fmlb_tc_operand_bytes(nb, d)
+ *             when not symmetric) bytes
+ *   status    device int: 0, or 1..3 when a bounded device-side wait gave up
+ *             (the result is then incomplete)
+ * nsigma <= 8.
+ * ---------------------------------------------------------------------- */
+size_t fmlb_tc_operand_bytes(int n, int d);
+int fmlb_column_mean_f64(const double *X, int n, int ldx, int d, double *mu, void *stream);
+int fmlb_gaussian_kernel_tc(const double *A, int na, int lda, const double *B, int nb, int ldb,
+                            int d, const double *mu, const double *sigmas_host, int nsigma,
+                            float *K, long long ldk, long long sigma_stride, int symmetric,
+                            void *workspace, size_t ws_bytes, int *status, void *stream);
+
 /* Allocation-free form of fmlb_kernel_predict_f64 (same arguments minus the
  * workspace, same results). It has no counterpart in the reference: it exists
  * for callers that cannot allocate device memory on the call path (a server

@@ -300,3 +300,37 @@ def test_cho_solve_failure_column_matches_lapack(oracle_mod, bad):
     with pytest.warns(fml_b200.CholeskyWarning, match="error code: %d$" % bad):
         fml_b200.cho_solve(A, y)
     assert oracle_mod.cho_solve(A, y)[1] == bad
+
+
+# ---------------------------------------------------------------------------
+# tensor-core (tcgen05) Gaussian, BF16 hi/lo x3, FP32 output
+# Stated error bound: |K_tc - K_fp64| <= 2e-4 absolute for sigma >= 100 on
+# Coulomb matrices (6e-5 measured at sigma = 100 in a numpy emulation).
+# ---------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def cm_large(oracle_mod):
+    b = synthetic.generate(700, nmax=29, seed=41)
+    return oracle_mod.coulomb_matrices(b.charges, b.coords, b.offsets, 29)
+
+
+@pytest.mark.parametrize("na,nb", [(300, 300), (130, 257), (1, 129), (600, 1)])
+def test_gaussian_tc_vs_fp64(oracle_mod, cm_large, na, nb):
+    A = cm_large[:na].T
+    B = cm_large[-nb:].T
+    sig = [100.0, 400.0, 1600.0]
+    K = fml_b200.gaussian_kernel(A, B, sig, precision="bf16x3")
+    assert K.dtype == np.float32 and K.shape == (3, na, nb)
+    for k, s in enumerate(sig):
+        ref = oracle_mod.gaussian_kernel(A, B, s)
+        assert np.abs(K[k] - ref).max() <= 2e-4, (s, np.abs(K[k] - ref).max())
+
+
+def test_gaussian_tc_symmetric_exact(oracle_mod, cm_large):
+    A = cm_large[:517].T
+    sig = [100.0, 1600.0]
+    K = fml_b200.gaussian_kernel(A, A, sig, precision="bf16x3")
+    for k, s in enumerate(sig):
+        np.testing.assert_array_equal(K[k], K[k].T)
+        np.testing.assert_array_equal(np.diag(K[k]), 1.0)
+        ref = oracle_mod.gaussian_kernel(A, A, s)
+        assert np.abs(K[k] - ref).max() <= 2e-4
