@@ -54,6 +54,8 @@ def parse():
     p.add_argument("--cpu-ntest", type=int, default=1024)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--stages", action="store_true",
+                   help="time each hot-path kernel on its own (one JSON line per stage)")
     return p.parse_args()
 
 
@@ -171,27 +173,35 @@ def run_reference(a):
 # ---------------------------------------------------------------------------
 def measure_syrk(pipe, torch, lib_call, ptr, stream):
     """Per-launch timing of the dominant kernel (FP64 trailing update) over the
-    exact launch sequence of one factorisation, on the pipeline's K buffer."""
-    from fml_b200.krr import PANEL
+    launch sequence of one factorisation (the strip of each next outer block
+    and the bulk past it, with k = the outer panel width), on the pipeline's K
+    buffer."""
+    from fml_b200.krr import outer_panel
     n = pipe.n_train
+    W = outer_panel(n)
     K = pipe.K[0]
     evs = []
     flops = 0.0
-    for k0 in range(0, n, PANEL):
-        kn = min(PANEL, n - k0)
-        base = k0 + kn
-        m = n - base
-        if m <= 0:
-            break
+
+    def timed(Cv, m, Pv, strip):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        Cv = K[base:, base:]
-        Pv = K[base:, k0:k0 + kn]
-        lib_call("fmlb_syrk_lower_f64", ptr(Cv), n, m, ptr(Pv), n, kn, None, stream)
+        lib_call("fmlb_syrk_lower_f64", ptr(Cv), n, m, ptr(Pv), n, W, strip, None, stream)
         e1.record()
         evs.append((e0, e1))
-        flops += float(m) * (m + 1) * kn
+
+    for K0 in range(0, n - W, W):
+        base = K0 + W
+        m = n - base
+        w = min(W, m)
+        timed(K[base:, base:], m, K[base:, K0:K0 + W], W)
+        flops += 2.0 * W * (w * m - w * (w - 1) / 2)
+        m2 = m - W
+        if m2 > 0:
+            b2 = base + W
+            timed(K[b2:, b2:], m2, K[b2:, K0:K0 + W], 0)
+            flops += 2.0 * W * m2 * (m2 + 1) / 2
     torch.cuda.synchronize()
     ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
     return flops, ms, len(evs)
@@ -355,9 +365,208 @@ def run_ours(a):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# per-stage measurements (one JSON line each; not the headline number)
+# ---------------------------------------------------------------------------
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # nominal CUDA-core FP32 (FFMA = 2 flops)
+MUFU_PEAK_PER_S = 148 * 16 * 1.965e9                 # nominal ex2 throughput
+
+
+def _measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def _time(torch, fn, reps=3, warmup=1):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return float(np.median(ts))
+
+
+def run_stages(a):
+    import torch
+
+    import oracle
+    from fml_b200 import _lib, synthetic
+    from fml_b200.kernels import _ptp_arrays
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    lib = _lib.load()
+    st = _lib.stream_handle()
+    P = _lib.ptr
+    peaks = _measured_peaks()
+    hbm = peaks["hbm_gbs"]
+    dgemm = measure_dgemm_peak(torch)
+    out = []
+
+    def emit(d):
+        d["stage_of"] = "fml_b200 hot path"
+        out.append(d)
+        print(json.dumps(d), flush=True)
+
+    # --- descriptors ---------------------------------------------------------
+    b = synthetic.generate(40960, nmax=29, seed=2)
+    z = torch.from_numpy(b.charges).to(dev)
+    r = torch.from_numpy(b.coords).to(dev)
+    o = torch.from_numpy(b.offsets).to(dev)
+    L = 435
+    X = torch.empty((40960, L), dtype=torch.float64, device=dev)
+    ms = _time(torch, lambda: _lib.call("fmlb_coulomb_matrices", P(z), P(r), P(o), 40960, 29,
+                                        P(X), L, None, 0, None, None, st), reps=5)
+    byt = 40960 * L * 8 + len(b.charges) * 32 + 40961 * 4
+    emit({"stage": "coulomb_matrices", "config": "40960 molecules, nmax 29", "ms": ms,
+          "molecules_per_s": 40960 / (ms * 1e-3), "bound": "hbm", "achieved_gbs": byt / ms / 1e6,
+          "peak_gbs": hbm, "frac": byt / ms / 1e6 / hbm})
+
+    ba = synthetic.generate(4000, nmax=23, seed=1)
+    za = torch.from_numpy(ba.charges).to(dev)
+    ra = torch.from_numpy(ba.coords).to(dev)
+    oa = torch.from_numpy(ba.offsets).to(dev)
+    D = torch.empty((4000, 23, 5, 23), dtype=torch.float64, device=dev)
+    ms = _time(torch, lambda: _lib.call("fmlb_arad_descriptors", P(za), P(ra), P(oa), 4000, 23,
+                                        1e6, P(D), None, st), reps=5)
+    emit({"stage": "arad_descriptors", "config": "4000 molecules, size 23, cut 1e6", "ms": ms,
+          "molecules_per_s": 4000 / (ms * 1e-3), "bound": "fp64 issue (O(n^3) per molecule)"})
+
+    # --- Gaussian / Laplacian -----------------------------------------------
+    n = a.ntrain
+    sig = [float(v) for v in a.sigmas.split(",")]
+    ns = len(sig)
+    sp, keep = _lib.host_doubles(sig)
+    Xt = X[:n]
+    K = torch.empty((ns, n, n), dtype=torch.float64, device=dev)
+    ms = _time(torch, lambda: _lib.call("fmlb_gaussian_kernel_f64", P(Xt), n, L, P(Xt), n, L, L,
+                                        sp, ns, P(K), n, n * n, 1, st), reps=2)
+    fl = 3.0 * L * n * (n + 1) / 2
+    emit({"stage": "gaussian_f64_symmetric", "config": "N=%d, d=%d, %d sigmas" % (n, L, ns),
+          "ms": ms, "entries_per_s": n * n * ns / (ms * 1e-3), "bound": "fp64",
+          "achieved_tflops": fl / ms / 1e9, "peak_tflops": dgemm,
+          "frac": fl / ms / 1e9 / dgemm, "peak_source": "cuBLAS DGEMM measured in this run"})
+    del K
+    K32 = torch.empty((ns, n, n), dtype=torch.float32, device=dev)
+    mu = torch.empty(L, dtype=torch.float64, device=dev)
+    ws = torch.empty(lib.fmlb_tc_operand_bytes(n, L), dtype=torch.uint8, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def tc():
+        _lib.call("fmlb_column_mean_f64", P(Xt), n, L, L, P(mu), st)
+        _lib.call("fmlb_gaussian_kernel_tc", P(Xt), n, L, P(Xt), n, L, L, P(mu), sp, ns, P(K32), n,
+                  n * n, 1, P(ws), ws.numel(), P(status), st)
+    ms = _time(torch, tc, reps=3)
+    wbytes = 4.0 * n * n * ns
+    tfl = 3 * 2.0 * 448 * n * (n + 1) / 2
+    emit({"stage": "gaussian_tc_bf16x3_symmetric", "config": "N=%d, d=%d (448 padded), %d sigmas"
+          % (n, L, ns), "ms": ms, "entries_per_s": n * n * ns / (ms * 1e-3), "bound": "hbm",
+          "achieved_gbs": wbytes / ms / 1e6, "peak_gbs": hbm, "frac": wbytes / ms / 1e6 / hbm,
+          "tensor_tflops": tfl / ms / 1e9, "tensor_frac_of_bf16": tfl / ms / 1e9 / peaks["bf16_tflops"],
+          "status": int(status.item())})
+    del K32, ws
+    nl = min(n, 16384)
+    Kl = torch.empty((ns, nl, nl), dtype=torch.float64, device=dev)
+    Xl = X[:nl]
+    ms = _time(torch, lambda: _lib.call("fmlb_laplacian_kernel_f64", P(Xl), nl, L, P(Xl), nl, L, L,
+                                        sp, ns, P(Kl), nl, nl * nl, 1, st), reps=2)
+    fl = 3.0 * L * nl * (nl + 1) / 2
+    emit({"stage": "laplacian_f64_symmetric", "config": "N=%d, d=%d, %d sigmas" % (nl, L, ns),
+          "ms": ms, "entries_per_s": nl * nl * ns / (ms * 1e-3), "bound": "fp64",
+          "achieved_tflops": fl / ms / 1e9, "peak_tflops": dgemm, "frac": fl / ms / 1e9 / dgemm})
+    del Kl
+
+    # --- Cholesky, solve, prediction ------------------------------------------
+    K1 = torch.empty((n, n), dtype=torch.float64, device=dev)
+    one = (ctypes_double_arr := _lib.host_doubles([sig[-1]]))[0]
+    work = torch.empty(lib.fmlb_potrf_workspace_bytes(n), dtype=torch.uint8, device=dev)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def factor():
+        _lib.call("fmlb_gaussian_kernel_f64", P(Xt), n, L, P(Xt), n, L, L, one, 1, P(K1), n, n * n,
+                  1, st)
+        _lib.call("fmlb_add_diagonal_f64", P(K1), n, n, a.lam, st)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.call("fmlb_potrf_f64", P(K1), n, n, P(work), P(info), st)
+        e1.record()
+        return e0, e1
+    factor()
+    torch.cuda.synchronize()
+    tms = []
+    for _ in range(2):
+        e0, e1 = factor()
+        torch.cuda.synchronize()
+        tms.append(e0.elapsed_time(e1))
+    ms = float(np.median(tms))
+    fl = n ** 3 / 3.0
+    emit({"stage": "potrf_f64", "config": "N=%d" % n, "ms": ms, "solves_per_s_factor": 1e3 / ms,
+          "bound": "fp64", "achieved_tflops": fl / ms / 1e9, "peak_tflops": dgemm,
+          "frac": fl / ms / 1e9 / dgemm, "info": int(info.item())})
+    x = torch.from_numpy(np.ascontiguousarray(b.energies[:n])).to(dev)
+    ms = _time(torch, lambda: _lib.call("fmlb_potrs_f64", P(K1), n, n, P(work), P(x), st), reps=3)
+    byt = n * n * 8.0
+    emit({"stage": "potrs_f64", "config": "N=%d, 1 right-hand side" % n, "ms": ms, "bound": "hbm",
+          "achieved_gbs": byt / ms / 1e6, "peak_gbs": hbm, "frac": byt / ms / 1e6 / hbm})
+    nq = a.ntest
+    alpha = torch.randn((ns, n), dtype=torch.float64, device=dev)
+    y = torch.empty((ns, nq), dtype=torch.float64, device=dev)
+    pw = torch.empty(lib.fmlb_kernel_predict_workspace_bytes(nq, n, ns), dtype=torch.uint8,
+                     device=dev)
+    Xq = X[n:n + nq]
+    ms = _time(torch, lambda: _lib.call("fmlb_kernel_predict_f64", 0, P(Xq), nq, L, P(Xt), n, L, L,
+                                        sp, ns, P(alpha), n, P(y), nq, P(pw), pw.numel(), st), reps=3)
+    fl = 3.0 * L * nq * n
+    emit({"stage": "predict_f64_fused", "config": "N_test=%d, N_train=%d, %d sigmas" % (nq, n, ns),
+          "ms": ms, "bound": "fp64", "achieved_tflops": fl / ms / 1e9, "peak_tflops": dgemm,
+          "frac": fl / ms / 1e9 / dgemm})
+    del K1, work
+
+    # --- ARAD kernels (3000 training + 1000 test molecules, 5 sigmas) ----------
+    Xa = oracle.arad_descriptors(ba.charges, ba.coords, ba.offsets, 23, 1e6)
+    Z = [ba.molecule(i)[0] for i in range(ba.nmol)]
+    ntr = 3000
+    asig = [0.1, 0.5, 1.0, 2.0, 5.0]
+    asp, akeep = _lib.host_doubles(asig)
+    # neighbour pairs evaluated: per atom the prefix of neighbours within the kernel cut (6.0)
+    Pm = np.array([int(((Xa[m, :len(Z[m]), 0, :len(Z[m])] <= 6.0)).sum()) for m in range(ba.nmol)],
+                  dtype=np.float64)
+    Ptr = Pm[:ntr]
+    evals_sym = (Ptr.sum() ** 2 + (Ptr ** 2).sum()) / 2.0
+    zp, nn = _ptp_arrays(Z[:ntr], 23)
+    x1 = torch.from_numpy(np.ascontiguousarray(Xa[:ntr])).to(dev)
+    z1 = torch.from_numpy(zp).to(dev)
+    n1 = torch.from_numpy(nn).to(dev)
+    Ka = torch.empty((5, ntr, ntr), dtype=torch.float64, device=dev)
+    aws = torch.empty(lib.fmlb_arad_workspace_bytes(ntr, ntr, 23, 1), dtype=torch.uint8, device=dev)
+    for prec, name in ((1, "fp32"), (0, "fp64")):
+        ms = _time(torch, lambda: _lib.call(
+            "fmlb_arad_kernels", P(x1), P(z1), P(n1), ntr, None, None, None, ntr, 23, asp, 5, 0.2,
+            6.0, 1.0, 0.5, 1, prec, P(Ka), P(aws), aws.numel(), st), reps=1)
+        emit({"stage": "arad_symmetric_" + name, "config": "3000 molecules (size 23, cut 1e6), 5 "
+              "sigmas", "ms": ms, "kernel_entries_per_s": ntr * ntr * 5 / (ms * 1e-3),
+              "neighbour_pair_evals": evals_sym, "evals_per_s": evals_sym / (ms * 1e-3),
+              "bound": "fp32 / mufu issue" if prec else "fp64 issue",
+              "mufu_frac": evals_sym / (ms * 1e-3) / MUFU_PEAK_PER_S})
+    del keep, akeep
+    return out
+
+
 def main():
     a = parse()
-    if a.impl == "reference":
+    if a.stages:
+        run_stages(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_ours(a)

@@ -6,14 +6,16 @@
 // other triangle is never read or written. For the reference's C-order
 // argument this is its dpotrf('U') factor U = L^T.
 //
-// Per panel of NB = 128 columns:
-//   1. potf2 + in-place inversion of the diagonal block in shared memory (one
-//      CTA); a non-positive pivot records the LAPACK info (1-based column) and
-//      every later kernel of the factorisation returns at once;
+// Two levels of blocking. Inner panels of NB = 128 columns:
+//   1. potf2 + inversion of the diagonal block in shared memory (one CTA); a
+//      non-positive pivot records the LAPACK info (1-based column) and every
+//      later kernel of the factorisation returns at once;
 //   2. panel solve L21 = A21 L11^-T as a product with the stored inverse;
-//   3. trailing update A22 -= L21 L21^T on the FP64 tensor cores
-//      (mma.sync m8n8k4 f64), 128x128 tiles on or below the diagonal, operands
-//      streamed through a 3-stage cp.async pipeline.
+// outer panels of 256 or 512 columns (four inner panels at large n):
+//   3. trailing update A22 -= L21 L21^T with k = the outer width, on the FP64
+//      tensor cores (mma.sync m8n8k4 f64), 128x64 tiles on or below the
+//      diagonal, operands streamed through a 3-stage cp.async pipeline;
+// with the next outer panel factored on a second stream under step 3.
 // The inverted diagonal blocks stay in the workspace for the solve.
 #include <math.h>
 #include <stdint.h>
@@ -44,32 +46,32 @@ constexpr int SB = 32, NSB = NB / SB, LDW = SB + 1;
 constexpr size_t kPotf2Smem = ((size_t)NB * LDL + (size_t)NSB * SB * LDW + SB * LDW) *
                               sizeof(double);
 
-// lane i holds row i of the sub-block in d[0..31]; on return d holds the
-// factor row and x holds column `lane` of the inverse. Returns the 1-based
-// failing column or 0.
-__device__ __forceinline__ int warp_potrf_inv32(double (&d)[SB], double (&x)[SB]) {
-    const unsigned full = 0xffffffffu;
+// One warp factors the 32 x 32 diagonal sub-block at L[b0.., b0..] in place
+// (lane = row) and writes its inverse into W (row-major). Returns the 1-based
+// failing column or 0 (the same value in every lane).
+__device__ __forceinline__ int warp_potrf_inv32(double (*L)[NB + 1], int b0, double (*W)[SB + 1]) {
     const int lane = threadIdx.x & 31;
-#pragma unroll
+    double *row = &L[b0 + lane][b0];
     for (int j = 0; j < SB; ++j) {
-        const double piv = __shfl_sync(full, d[j], j);
+        const double piv = L[b0 + j][b0 + j];
         if (!(piv > 0.0)) return j + 1;
         const double r = sqrt(piv), inv = 1.0 / r;
-        d[j] = (lane == j) ? r : (lane > j ? d[j] * inv : d[j]);
-#pragma unroll
-        for (int c = j + 1; c < SB; ++c) {
-            const double dcj = __shfl_sync(full, d[j], c);
-            if (lane >= c) d[c] = fma(-d[j], dcj, d[c]);
-        }
+        __syncwarp();
+        if (lane == j) row[j] = r;
+        else if (lane > j) row[j] *= inv;
+        __syncwarp();
+        const double lij = row[j];
+        for (int c = j + 1; c <= lane; ++c) row[c] = fma(-lij, L[b0 + c][b0 + j], row[c]);
+        __syncwarp();
     }
-    // column `lane` of the inverse by forward substitution
-#pragma unroll
+    // column `lane` of the inverse by forward substitution: W[k][lane]
     for (int k = 0; k < SB; ++k) {
-        double s = (k == lane) ? 1.0 : 0.0;
-#pragma unroll
-        for (int q = 0; q < k; ++q) s = fma(-__shfl_sync(full, d[q], k), x[q], s);
-        x[k] = s / __shfl_sync(full, d[k], k);
+        double sacc = (k == lane) ? 1.0 : 0.0;
+        const double *lk = &L[b0 + k][b0];
+        for (int q = lane; q < k; ++q) sacc = fma(-lk[q], W[q][lane], sacc);
+        W[k][lane] = (k < lane) ? 0.0 : sacc / lk[k];
     }
+    __syncwarp();
     return 0;
 }
 
@@ -95,19 +97,8 @@ potf2_block_kernel(double *__restrict__ A, long long lda, int k0, int kn,
     for (int J = 0; J < NSB; ++J) {
         const int b0 = J * SB;
         if (warp == 0) {
-            double d[SB], x[SB];
-#pragma unroll
-            for (int c = 0; c < SB; ++c) d[c] = L[b0 + lane][b0 + c];
-            const int f = warp_potrf_inv32(d, x);
-            if (f) {
-                if (lane == 0) bad = b0 + f;
-            } else {
-#pragma unroll
-                for (int c = 0; c < SB; ++c) {
-                    if (c <= lane) L[b0 + lane][b0 + c] = d[c];
-                    W[J][c][lane] = x[c];  // inverse: row c, column lane
-                }
-            }
+            const int f = warp_potrf_inv32(L, b0, W[J]);
+            if (f && lane == 0) bad = b0 + f;
         }
         __syncthreads();
         if (bad) {
@@ -224,6 +215,8 @@ panel_trsm_kernel(double *__restrict__ A, long long lda, int n, int k0, int kn,
 // read-modify-write epilogue overlap the other's tensor-core work.
 constexpr int SY_TM = 128, SY_TN = 64, SY_TK = 16, SY_LD = 20, SY_STAGES = 3, SY_TPB = 128;
 constexpr int SY_STAGE_DOUBLES = (SY_TM + SY_TN) * SY_LD;
+constexpr int SY_CLD = SY_TN + 8;  // row pitch of the epilogue's C tile in shared memory
+static_assert(SY_TM * SY_CLD <= SY_STAGES * SY_STAGE_DOUBLES, "C tile must fit in the stages");
 constexpr size_t kSyrkSmem = (size_t)SY_STAGES * SY_STAGE_DOUBLES * sizeof(double);
 
 __device__ __forceinline__ void cp_async_16(void *smem, const void *gmem, int src_bytes) {
@@ -280,15 +273,21 @@ __device__ __forceinline__ void syrk_load_tile(double *dst, const double *__rest
 template <bool kAligned16>
 __global__ void __launch_bounds__(SY_TPB, 2)
 syrk_dmma_kernel(double *__restrict__ C, long long ldc, int m, const double *__restrict__ P,
-                 long long ldp, int k, const int *__restrict__ info) {
+                 long long ldp, int k, int strip_tiles, const int *__restrict__ info) {
     extern __shared__ __align__(16) double sy_smem[];
     if (failed(info)) return;
-    // tile t -> (row block by of 128, column block bx of 64), bx <= 2 by + 1
     const long long t = blockIdx.x;
-    int by = (int)((sqrt(4.0 * (double)t + 1.0) - 1.0) * 0.5);
-    while ((long long)by * by + by > t) --by;
-    while ((long long)(by + 1) * (by + 1) + (by + 1) <= t) ++by;
-    const int bx = (int)(t - (long long)by * by - by);
+    int by, bx;
+    if (strip_tiles > 0) {  // only the first strip_tiles column tiles of every row block
+        by = (int)(t / strip_tiles);
+        bx = (int)(t % strip_tiles);
+        if (bx > 2 * by + 1) return;
+    } else {  // tile t -> (row block by of 128, column block bx of 64), bx <= 2 by + 1
+        by = (int)((sqrt(4.0 * (double)t + 1.0) - 1.0) * 0.5);
+        while ((long long)by * by + by > t) --by;
+        while ((long long)(by + 1) * (by + 1) + (by + 1) <= t) ++by;
+        bx = (int)(t - (long long)by * by - by);
+    }
     const int row0 = by * SY_TM, col0 = bx * SY_TN;
     if (col0 >= m || row0 >= m) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -337,24 +336,50 @@ syrk_dmma_kernel(double *__restrict__ C, long long ldc, int m, const double *__r
         }
     }
     cp_async_wait<0>();
+    __syncthreads();  // every warp is done with the stage buffers
+    // Epilogue through shared memory: one coalesced pass loads the C tile,
+    // the fragments are subtracted there, one coalesced masked pass stores it
+    // (keeps the 64 read-modify-writes per thread from serialising).
+    double *Cs = sy_smem;  // SY_TM x SY_CLD doubles, fits in the stage area
+    const int tid = threadIdx.x;
+    for (int e = tid; e < SY_TM * (SY_TN / 2); e += SY_TPB) {
+        const int r = e / (SY_TN / 2), c = (e % (SY_TN / 2)) * 2;
+        const int gr = row0 + r, gc = col0 + c;
+        double v0 = 0.0, v1 = 0.0;
+        if (gr < m) {
+            const double *src = C + (size_t)gr * ldc + gc;
+            if (gc < m) v0 = src[0];
+            if (gc + 1 < m) v1 = src[1];
+        }
+        Cs[r * SY_CLD + c] = v0;
+        Cs[r * SY_CLD + c + 1] = v1;
+    }
+    __syncthreads();
     // fragment (i, j): rows wr*64 + i*8 + g, columns wc*32 + j*8 + 2*tq + {0, 1}
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        const int r = row0 + wr * 64 + i * 8 + g;
-        if (r >= m) continue;
+        const int rl = wr * 64 + i * 8 + g;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const int c = col0 + wc * 32 + j * 8 + 2 * tq;
-            double *p = C + (size_t)r * ldc + c;
-            if (c <= r) p[0] -= acc[i][j][0];
-            if (c + 1 <= r) p[1] -= acc[i][j][1];
+            const int cl = wc * 32 + j * 8 + 2 * tq;
+            Cs[rl * SY_CLD + cl] -= acc[i][j][0];
+            Cs[rl * SY_CLD + cl + 1] -= acc[i][j][1];
         }
+    }
+    __syncthreads();
+    for (int e = tid; e < SY_TM * (SY_TN / 2); e += SY_TPB) {
+        const int r = e / (SY_TN / 2), c = (e % (SY_TN / 2)) * 2;
+        const int gr = row0 + r, gc = col0 + c;
+        if (gr >= m) continue;
+        double *dst = C + (size_t)gr * ldc + gc;
+        if (gc < m && gc <= gr) dst[0] = Cs[r * SY_CLD + c];
+        if (gc + 1 < m && gc + 1 <= gr) dst[1] = Cs[r * SY_CLD + c + 1];
     }
 }
 
 template <bool kAligned16>
 int launch_syrk_impl(double *C, long long ldc, int m, const double *P, long long ldp, int k,
-                     const int *info, cudaStream_t st) {
+                     int strip_cols, const int *info, cudaStream_t st) {
     static int attr_dev = -1;
     int dev = 0;
     FMLB_TRY(cuda_status(cudaGetDevice(&dev), "syrk: cudaGetDevice"));
@@ -365,18 +390,22 @@ int launch_syrk_impl(double *C, long long ldc, int m, const double *P, long long
         attr_dev = dev;
     }
     const long long Tr = ceil_div(m, SY_TM);
-    const long long ntiles = Tr * Tr + Tr;  // row block by holds 2 by + 2 column tiles
-    syrk_dmma_kernel<kAligned16><<<(unsigned)ntiles, SY_TPB, kSyrkSmem, st>>>(C, ldc, m, P, ldp, k,
-                                                                            info);
+    const int strip_tiles = strip_cols > 0 ? ceil_div(std::min(strip_cols, m), SY_TN) : 0;
+    // full: row block by holds 2 by + 2 column tiles; strip: strip_tiles per row block
+    const long long ntiles = strip_tiles ? Tr * strip_tiles : Tr * Tr + Tr;
+    syrk_dmma_kernel<kAligned16><<<(unsigned)ntiles, SY_TPB, kSyrkSmem, st>>>(
+        C, ldc, m, P, ldp, k, strip_tiles, info);
     return launch_status("syrk_dmma_kernel");
 }
 
+// strip_cols = 0: lower triangle of the m x m block; > 0: only its first
+// strip_cols columns (the lower part of that column strip).
 int launch_syrk(double *C, long long ldc, int m, const double *P, long long ldp, int k,
-                const int *info, cudaStream_t st) {
+                const int *info, cudaStream_t st, int strip_cols = 0) {
     if (m <= 0 || k <= 0) return FMLB_OK;
     if (((uintptr_t)P % 16 == 0) && (ldp % 2 == 0))
-        return launch_syrk_impl<true>(C, ldc, m, P, ldp, k, info, st);
-    return launch_syrk_impl<false>(C, ldc, m, P, ldp, k, info, st);
+        return launch_syrk_impl<true>(C, ldc, m, P, ldp, k, strip_cols, info, st);
+    return launch_syrk_impl<false>(C, ldc, m, P, ldp, k, strip_cols, info, st);
 }
 
 // ---- solve ------------------------------------------------------------------
@@ -453,6 +482,78 @@ extern "C" size_t fmlb_potrf_workspace_bytes(int n) {
            ((size_t)n * sizeof(double) + 255) / 256 * 256;
 }
 
+// Per host thread and device: the high-priority stream that runs the panel
+// chain (strip update, diagonal block, panel solve) of the lookahead, and two
+// events to order it against the caller's stream.
+struct Lookahead {
+    cudaStream_t panel = nullptr;
+    cudaEvent_t main_done = nullptr, panel_done = nullptr;
+};
+
+static int lookahead_for_device(Lookahead **out) {
+    using namespace fmlb;
+    static thread_local Lookahead per_dev[64];
+    int dev = 0;
+    FMLB_TRY(cuda_status(cudaGetDevice(&dev), "fmlb_potrf_f64: cudaGetDevice"));
+    FMLB_REQUIRE(dev >= 0 && dev < 64, "fmlb_potrf_f64: device %d out of range", dev);
+    Lookahead &L = per_dev[dev];
+    if (!L.panel) {
+        int lo = 0, hi = 0;
+        FMLB_TRY(cuda_status(cudaDeviceGetStreamPriorityRange(&lo, &hi), "stream priorities"));
+        FMLB_TRY(cuda_status(cudaStreamCreateWithPriority(&L.panel, cudaStreamNonBlocking, hi),
+                             "fmlb_potrf_f64: panel stream"));
+        FMLB_TRY(cuda_status(cudaEventCreateWithFlags(&L.main_done, cudaEventDisableTiming),
+                             "fmlb_potrf_f64: event"));
+        FMLB_TRY(cuda_status(cudaEventCreateWithFlags(&L.panel_done, cudaEventDisableTiming),
+                             "fmlb_potrf_f64: event"));
+    }
+    *out = &L;
+    return FMLB_OK;
+}
+
+static int panel_factor(double *A, long long lda, int n, int k0, double *Li, int *info,
+                        cudaStream_t st) {
+    using namespace fmlb;
+    const int kn = std::min(NB, n - k0);
+    potf2_block_kernel<<<1, TPB, kPotf2Smem, st>>>(A, lda, k0, kn, Li, info);
+    FMLB_TRY(launch_status("potf2_block_kernel"));
+    const int rest = n - k0 - kn;
+    if (rest > 0) {
+        panel_trsm_kernel<<<ceil_div(rest, TRSM_ROWS), TPB, kTrsmSmem, st>>>(A, lda, n, k0, kn, Li,
+                                                                            info);
+        FMLB_TRY(launch_status("panel_trsm_kernel"));
+    }
+    return FMLB_OK;
+}
+
+// Factor the outer panel of columns [K0, K0 + width) on stream st: per inner
+// panel of NB columns, the diagonal block and the panel solve (all rows below),
+// then the update of the rest of the outer panel's columns by that inner panel.
+static int factor_outer_panel(double *A, long long lda, int n, int K0, int width, double *Linv,
+                              int *info, cudaStream_t st) {
+    using namespace fmlb;
+    const int end = std::min(K0 + width, n);
+    for (int k0 = K0; k0 < end; k0 += NB) {
+        FMLB_TRY(panel_factor(A, lda, n, k0, Linv + (size_t)(k0 / NB) * NB * NB, info, st));
+        const size_t b = (size_t)(k0 + NB);
+        const int rem = end - (int)b;
+        if (rem > 0)
+            FMLB_TRY(launch_syrk(A + b * lda + b, lda, n - (int)b, A + b * lda + k0, lda, NB, info,
+                                 st, rem));
+    }
+    return FMLB_OK;
+}
+
+// Outer panel width: wide panels give the trailing update a long k-loop
+// (k = 512: ~28 TFLOP/s against ~17 at k = 128 on B200).
+static int outer_width(int n) { return n >= 8192 ? 4 * fmlb::NB : 2 * fmlb::NB; }
+
+// Two-level blocked factorisation with a lookahead of depth one. For outer
+// panel K (factored), with outer block K+1 the next:
+//   panel stream:  strip update of outer block K+1 by panel K (k = width),
+//                  then the factorisation of outer panel K+1;
+//   caller stream: update of the trailing matrix past block K+1 by panel K.
+// The two regions are disjoint, so the panel chain runs under the bulk update.
 extern "C" int fmlb_potrf_f64(double *A, long long lda, int n, void *work, int *info,
                               void *stream) {
     using namespace fmlb;
@@ -463,21 +564,35 @@ extern "C" int fmlb_potrf_f64(double *A, long long lda, int n, void *work, int *
     if (n == 0) return FMLB_OK;
     FMLB_REQUIRE(A && work, "fmlb_potrf_f64: null pointer");
     FMLB_TRY(set_smem_attrs());
+    Lookahead *la = nullptr;
+    FMLB_TRY(lookahead_for_device(&la));
     double *Linv = static_cast<double *>(work);
-    for (int k0 = 0, kb = 0; k0 < n; k0 += NB, ++kb) {
-        const int kn = std::min(NB, n - k0);
-        double *Li = Linv + (size_t)kb * NB * NB;
-        potf2_block_kernel<<<1, TPB, kPotf2Smem, st>>>(A, lda, k0, kn, Li, info);
-        FMLB_TRY(launch_status("potf2_block_kernel"));
-        const int rest = n - k0 - kn;
-        if (rest <= 0) break;
-        panel_trsm_kernel<<<ceil_div(rest, TRSM_ROWS), TPB, kTrsmSmem, st>>>(A, lda, n, k0, kn, Li,
-                                                                            info);
-        FMLB_TRY(launch_status("panel_trsm_kernel"));
-        const size_t base = (size_t)(k0 + kn);
-        FMLB_TRY(launch_syrk(A + base * lda + base, lda, rest, A + base * lda + k0, lda, kn, info,
-                             st));
+    const int W = outer_width(n);
+    const int nob = ceil_div(n, W);
+    FMLB_TRY(factor_outer_panel(A, lda, n, 0, W, Linv, info, st));
+    bool panel_used = false;
+    for (int K = 0; K + 1 < nob; ++K) {
+        const int K0 = K * W;
+        const size_t base = (size_t)(K0 + W);  // first row / column of outer block K+1
+        const int rest = n - (int)base;
+        if (panel_used)  // outer panel K was factored on the panel stream
+            FMLB_TRY(cuda_status(cudaStreamWaitEvent(st, la->panel_done, 0), "wait panel"));
+        FMLB_TRY(cuda_status(cudaEventRecord(la->main_done, st), "record main"));
+        FMLB_TRY(cuda_status(cudaStreamWaitEvent(la->panel, la->main_done, 0), "wait main"));
+        FMLB_TRY(launch_syrk(A + base * lda + base, lda, rest, A + base * lda + K0, lda, W, info,
+                             la->panel, W));
+        FMLB_TRY(factor_outer_panel(A, lda, n, (int)base, W, Linv, info, la->panel));
+        FMLB_TRY(cuda_status(cudaEventRecord(la->panel_done, la->panel), "record panel"));
+        panel_used = true;
+        const int rest2 = rest - W;
+        if (rest2 > 0) {
+            const size_t b2 = base + W;
+            FMLB_TRY(launch_syrk(A + b2 * lda + b2, lda, rest2, A + b2 * lda + K0, lda, W, info,
+                                 st));
+        }
     }
+    if (panel_used)
+        FMLB_TRY(cuda_status(cudaStreamWaitEvent(st, la->panel_done, 0), "join panel stream"));
     return FMLB_OK;
 }
 
@@ -511,10 +626,12 @@ extern "C" int fmlb_potrs_f64(const double *L, long long lda, int n, const void 
 }
 
 extern "C" int fmlb_syrk_lower_f64(double *C, long long ldc, int m, const double *P,
-                                   long long ldp, int k, const int *info, void *stream) {
+                                   long long ldp, int k, int strip_cols, const int *info,
+                                   void *stream) {
     using namespace fmlb;
-    FMLB_REQUIRE(m >= 0 && k >= 0 && ldc >= m && ldp >= k, "fmlb_syrk_lower_f64: bad sizes");
+    FMLB_REQUIRE(m >= 0 && k >= 0 && ldc >= m && ldp >= k && strip_cols >= 0,
+                 "fmlb_syrk_lower_f64: bad sizes");
     if (m == 0 || k == 0) return FMLB_OK;
     FMLB_REQUIRE(C && P, "fmlb_syrk_lower_f64: null pointer");
-    return launch_syrk(C, ldc, m, P, ldp, k, info, FMLB_STREAM(stream));
+    return launch_syrk(C, ldc, m, P, ldp, k, info, FMLB_STREAM(stream), strip_cols);
 }

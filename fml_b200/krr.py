@@ -23,7 +23,28 @@ from . import _lib
 from ._tensors import device, to_device, to_output
 
 KINDS = {"gaussian": 0, "laplacian": 1}
-PANEL = 128  # panel width of the FP64 factorisation (NB in cholesky_f64.cu)
+PANEL = 128  # inner panel width of the FP64 factorisation (NB in cholesky_f64.cu)
+
+
+def outer_panel(n):
+    """Outer panel width of the FP64 factorisation (outer_width in cholesky_f64.cu)."""
+    return 4 * PANEL if n >= 8192 else 2 * PANEL
+
+
+def potrf_launches(n):
+    """Kernel launches of fmlb_potrf_f64 for an n x n matrix (mirrors its loops)."""
+    W = outer_panel(n)
+    count = 0
+    for K0 in range(0, n, W):
+        end = min(K0 + W, n)
+        for k0 in range(K0, end, PANEL):
+            count += 1 + (1 if n - k0 - PANEL > 0 else 0)  # diagonal block + panel solve
+            count += 1 if end - (k0 + PANEL) > 0 else 0     # rest of the outer panel
+        if K0 > 0:
+            count += 1                                       # strip of this outer block
+    for K0 in range(0, n - W, W):
+        count += 1 if n - (K0 + 2 * W) > 0 else 0           # bulk update
+    return count
 
 
 class KRRPipeline:
@@ -61,7 +82,7 @@ class KRRPipeline:
     def launches_per_run(self):
         """Kernel launches of one ``run`` (mirrors the loops in the C library)."""
         nblk = -(-self.n_train // PANEL)
-        potrf = 3 * nblk - 2 if nblk > 0 else 0
+        potrf = potrf_launches(self.n_train)
         potrs = 2 * nblk
         per_sigma = 1 + potrf + potrs
         return 1 + 1 + self.nsig * per_sigma + (2 if self.n_test else 0)

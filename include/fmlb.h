@@ -147,11 +147,13 @@ int fmlb_potrs_f64(const double *L, long long lda, int n, const void *work, doub
 
 /* Trailing update of the blocked factorisation: C -= P P^T on the triangle
  * i >= j of the row-major (m, m) matrix C, P is (m, k) with stride ldp; the
- * other triangle of C is not touched. `info` (device, may be NULL): when it
- * holds a non-zero value the update is skipped. The step fmlb_potrf_f64 runs
- * per panel (the LAPACK dsyrk call inside dpotrf, fcho_solve.f90:35). */
+ * other triangle of C is not touched. strip_cols = 0 updates the whole lower
+ * triangle, strip_cols > 0 only its first strip_cols columns. `info` (device,
+ * may be NULL): when it holds a non-zero value the update is skipped. The
+ * step fmlb_potrf_f64 runs per panel (the LAPACK dsyrk call inside dpotrf,
+ * fcho_solve.f90:35). */
 int fmlb_syrk_lower_f64(double *C, long long ldc, int m, const double *P, long long ldp, int k,
-                        const int *info, void *stream);
+                        int strip_cols, const int *info, void *stream);
 
 /* ------------------------------------------------------------------------
  * KRR helpers, FP64.

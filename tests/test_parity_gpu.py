@@ -269,7 +269,7 @@ def test_syrk_lower_update(m, k, ld_pad):
     Pbuf[:, :k] = P
     C = torch.from_numpy(buf.copy()).cuda()
     Pd = torch.from_numpy(Pbuf).cuda()
-    _lib.call("fmlb_syrk_lower_f64", _lib.ptr(C), ld, m, _lib.ptr(Pd), ld, k, None,
+    _lib.call("fmlb_syrk_lower_f64", _lib.ptr(C), ld, m, _lib.ptr(Pd), ld, k, 0, None,
               _lib.stream_handle())
     out = C.cpu().numpy()
     ref = buf[:, :m] - P @ P.T
@@ -334,3 +334,40 @@ def test_gaussian_tc_symmetric_exact(oracle_mod, cm_large):
         np.testing.assert_array_equal(np.diag(K[k]), 1.0)
         ref = oracle_mod.gaussian_kernel(A, A, s)
         assert np.abs(K[k] - ref).max() <= 2e-4
+
+
+@pytest.mark.parametrize("m,strip", [(300, 128), (100, 128), (257, 64)])
+def test_syrk_lower_strip(m, strip):
+    """strip_cols > 0 updates only the first strip_cols columns of the lower triangle."""
+    from fml_b200 import _lib
+    rng = np.random.default_rng(m)
+    k = 128
+    buf = rng.standard_normal((m, m))
+    P = rng.standard_normal((m, k))
+    C = torch.from_numpy(buf.copy()).cuda()
+    Pd = torch.from_numpy(P).cuda()
+    _lib.call("fmlb_syrk_lower_f64", _lib.ptr(C), m, m, _lib.ptr(Pd), k, k, strip, None,
+              _lib.stream_handle())
+    out = C.cpu().numpy()
+    ref = buf - P @ P.T
+    r, c = np.indices((m, m))
+    upd = (c <= r) & (c < strip)
+    np.testing.assert_allclose(out[upd], ref[upd], rtol=1e-13, atol=1e-12)
+    np.testing.assert_array_equal(out[~upd], buf[~upd])
+
+
+def test_cho_solve_wide_outer_panels(oracle_mod):
+    """n >= 8192 takes 512-column outer panels; n = 8300 ends in a partial one."""
+    n = 8300
+    rng = np.random.default_rng(7)
+    M = rng.standard_normal((n, 600))
+    A = M @ M.T / 600 + 0.25 * np.eye(n)
+    y = rng.standard_normal(n)
+    x = fml_b200.cho_solve(A, y)
+    ref, info = oracle_mod.cho_solve(A, y)
+    assert info == 0
+    np.testing.assert_allclose(x, ref, rtol=1e-9, atol=1e-10 * np.abs(ref).max())
+    B = A.copy()
+    B[5001, 5001] = -1.0
+    with pytest.warns(fml_b200.CholeskyWarning, match="error code: 5002$"):
+        fml_b200.cho_solve(B, y)
