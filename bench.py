@@ -54,8 +54,11 @@ def parse():
     p.add_argument("--cpu-ntest", type=int, default=1024)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--stages", action="store_true",
-                   help="time each hot-path kernel on its own (one JSON line per stage)")
+    p.add_argument("--stages", nargs="?", const="all", default=None,
+                   help="time each hot-path kernel on its own (one JSON line per stage); "
+                        "'arad' times only the ARAD kernels")
+    p.add_argument("--arad-nmol", type=int, default=4000,
+                   help="molecules of the ARAD stage (the first 3/4 form the symmetric set)")
     return p.parse_args()
 
 
@@ -417,6 +420,8 @@ def run_stages(a):
         out.append(d)
         print(json.dumps(d), flush=True)
 
+    if a.stages == "arad":
+        return run_arad_stage(a, torch, lib, st, P)
     # --- descriptors ---------------------------------------------------------
     b = synthetic.generate(40960, nmax=29, seed=2)
     z = torch.from_numpy(b.charges).to(dev)
@@ -532,10 +537,24 @@ def run_stages(a):
           "frac": fl / ms / 1e9 / dgemm})
     del K1, work
 
-    # --- ARAD kernels (3000 training + 1000 test molecules, 5 sigmas) ----------
+    del keep
+    out += run_arad_stage(a, torch, lib, st, P)
+    return out
+
+
+def run_arad_stage(a, torch, lib, st, P):
+    """ARAD kernels: symmetric set of 3/4 of --arad-nmol molecules (3000 of the
+    4000-molecule configuration), size 23, descriptor cut 1e6, 5 sigmas."""
+    import oracle
+    from fml_b200 import _lib, synthetic
+    from fml_b200.kernels import _ptp_arrays
+
+    out = []
+    dev = torch.device("cuda", 0)
+    ba = synthetic.generate(a.arad_nmol, nmax=23, seed=1)
     Xa = oracle.arad_descriptors(ba.charges, ba.coords, ba.offsets, 23, 1e6)
     Z = [ba.molecule(i)[0] for i in range(ba.nmol)]
-    ntr = 3000
+    ntr = (3 * a.arad_nmol) // 4
     asig = [0.1, 0.5, 1.0, 2.0, 5.0]
     asp, akeep = _lib.host_doubles(asig)
     # neighbour pairs evaluated: per atom the prefix of neighbours within the kernel cut (6.0)
@@ -553,12 +572,14 @@ def run_stages(a):
         ms = _time(torch, lambda: _lib.call(
             "fmlb_arad_kernels", P(x1), P(z1), P(n1), ntr, None, None, None, ntr, 23, asp, 5, 0.2,
             6.0, 1.0, 0.5, 1, prec, P(Ka), P(aws), aws.numel(), st), reps=1)
-        emit({"stage": "arad_symmetric_" + name, "config": "3000 molecules (size 23, cut 1e6), 5 "
-              "sigmas", "ms": ms, "kernel_entries_per_s": ntr * ntr * 5 / (ms * 1e-3),
-              "neighbour_pair_evals": evals_sym, "evals_per_s": evals_sym / (ms * 1e-3),
-              "bound": "fp32 / mufu issue" if prec else "fp64 issue",
-              "mufu_frac": evals_sym / (ms * 1e-3) / MUFU_PEAK_PER_S})
-    del keep, akeep
+        d = {"stage": "arad_symmetric_" + name, "config": "%d molecules (size 23, cut 1e6), 5 "
+             "sigmas" % ntr, "ms": ms, "kernel_entries_per_s": ntr * ntr * 5 / (ms * 1e-3),
+             "neighbour_pair_evals": evals_sym, "evals_per_s": evals_sym / (ms * 1e-3),
+             "bound": "fp32 / mufu issue" if prec else "fp64 issue",
+             "mufu_frac": evals_sym / (ms * 1e-3) / MUFU_PEAK_PER_S, "stage_of": "fml_b200 hot path"}
+        out.append(d)
+        print(json.dumps(d), flush=True)
+    del akeep
     return out
 
 

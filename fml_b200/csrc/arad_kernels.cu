@@ -35,12 +35,27 @@ struct AradParams {
 
 // Per-set workspace views.
 struct SetWs {
-    int *nnb;        // (nm, amax)      neighbour prefix length
-    double *xi;      // (nm, amax, amax) sine factors (FP64 path)
-    double *self;    // (nm, amax)      self terms (FP64 path)
-    float4 *pk;      // (nm, amax, amax) {r, xi, xi*c, xi*s} (FP32 path)
-    float2 *pz;      // (nm, amax, amax) {row, col}         (FP32 path)
-    float *self32;   // (nm, amax)
+    int *nnb;             // (nm, amax)       neighbour prefix length
+    double *xi;           // (nm, amax, amax) sine factors (FP64 path)
+    double *self;         // (nm, amax)       self terms (FP64 path)
+    float4 *pk;           // (nm, amax, amax) {r, xi, xi*c, xi*s} (FP32 paths)
+    float2 *pz;           // (nm, amax, amax) {row, col}         (generic FP32 path)
+    float *self32;        // (nm, amax)       self terms (generic FP32 path)
+    signed char *cls;     // (nm, amax, amax) element class of each neighbour (fast path)
+    signed char *acls;    // (nm, amax)       element class of each atom (fast path)
+    float *selff;         // (nm, amax)       self terms (fast path)
+};
+
+// Element classes (distinct periodic-table positions) of the fast FP32 path:
+// the stoichiometric factor between two classes comes from a small table.
+constexpr int FC_MAXC = 16;
+constexpr int FC_NPOS = 8 * 34;  // (row 0..7) * 34 + (col 0..33)
+struct ClassInfo {
+    int flag;                 // 0: fast path usable; otherwise why not
+    int ncls;
+    int present[FC_NPOS];
+    signed char map[FC_NPOS]; // position -> class, -1 if absent
+    float stoch[FC_MAXC * FC_MAXC];
 };
 
 __host__ __device__ inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -49,7 +64,8 @@ size_t set_ws_bytes(int nm, int amax) {
     const size_t a2 = (size_t)nm * amax * amax, a1 = (size_t)nm * amax;
     return align256(a1 * sizeof(int)) + align256(a2 * sizeof(double)) +
            align256(a1 * sizeof(double)) + align256(a2 * sizeof(float4)) +
-           align256(a2 * sizeof(float2)) + align256(a1 * sizeof(float));
+           align256(a2 * sizeof(float2)) + align256(a1 * sizeof(float)) + align256(a2) +
+           align256(a1) + align256(a1 * sizeof(float));
 }
 
 SetWs carve(char *&p, int nm, int amax) {
@@ -61,6 +77,9 @@ SetWs carve(char *&p, int nm, int amax) {
     w.pk = reinterpret_cast<float4 *>(p); p += align256(a2 * sizeof(float4));
     w.pz = reinterpret_cast<float2 *>(p); p += align256(a2 * sizeof(float2));
     w.self32 = reinterpret_cast<float *>(p); p += align256(a1 * sizeof(float));
+    w.cls = reinterpret_cast<signed char *>(p); p += align256(a2);
+    w.acls = reinterpret_cast<signed char *>(p); p += align256(a1);
+    w.selff = reinterpret_cast<float *>(p); p += align256(a1 * sizeof(float));
     return w;
 }
 
@@ -95,10 +114,12 @@ __device__ double distl2_f64(const double *x1, const double *xi1, int n1, const 
     return aad;
 }
 
-// FP32 form over the packed neighbour records.
+// FP32 form over the packed neighbour records. The records hold the distance
+// pre-scaled by rs = sqrt(-inv_width * log2 e), so exp(dr^2 inv_width) =
+// exp2(-(dr')^2) and the window (dr)^2 < (8 w)^2 is (dr')^2 < maxg2s.
 __device__ __forceinline__ float distl2_f32(const float4 *a, const float2 *za, int n1,
                                             const float4 *b, const float2 *zb, int n2,
-                                            float inv_w_log2, float maxg2, float rw2, float cw2) {
+                                            float maxg2s, float rw2, float cw2) {
     float aad = 0.0f;
     for (int m1 = 0; m1 < n1; ++m1) {
         const float4 u = a[m1];
@@ -107,16 +128,20 @@ __device__ __forceinline__ float distl2_f32(const float4 *a, const float2 *za, i
             const float4 v = b[m2];
             const float dr = v.x - u.x;
             const float t = dr * dr;
-            if (t < maxg2) {
+            if (t < maxg2s) {
                 const float2 zv = zb[m2];
                 const float dp = zu.x - zv.x, dg = zu.y - zv.y;
                 const float st = __fdividef(rw2, rw2 + dp * dp) * __fdividef(cw2, cw2 + dg * dg);
                 const float g = fmaf(u.z, v.z, fmaf(u.w, v.w, u.y * v.y));
-                aad = fmaf(exp2f(t * inv_w_log2) * st, g, aad);
+                aad = fmaf(exp2f(-t) * st, g, aad);
             }
         }
     }
     return aad;
+}
+
+__host__ __device__ inline double fp32_scale(const AradParams &P) {
+    return sqrt(-P.inv_width * 1.4426950408889634);
 }
 
 // Stage 1: one thread per (molecule, atom).
@@ -148,14 +173,14 @@ __global__ void arad_prep_kernel(const double *__restrict__ X, const int *__rest
         xi[k] = s;
         if (k < cnt) {
             const double c = x[3 * amax + k], sn = x[4 * amax + k];
-            pk[k] = make_float4((float)r, (float)s, (float)(s * c), (float)(s * sn));
+            pk[k] = make_float4((float)(r * fp32_scale(P)), (float)s, (float)(s * c),
+                                (float)(s * sn));
             pz[k] = make_float2((float)x[amax + k], (float)x[2 * amax + k]);
         }
     }
     w.self[base] = distl2_f64(x, xi, cnt, x, xi, cnt, amax, P);
-    const float inv_w_log2 = (float)(P.inv_width * 1.4426950408889634);
-    w.self32[base] = distl2_f32(pk, pz, cnt, pk, pz, cnt, inv_w_log2, (float)P.maxg2,
-                                (float)P.rw2, (float)P.cw2);
+    const float maxg2s = (float)(P.maxg2 * fp32_scale(P) * fp32_scale(P));
+    w.self32[base] = distl2_f32(pk, pz, cnt, pk, pz, cnt, maxg2s, (float)P.rw2, (float)P.cw2);
 }
 
 __device__ __forceinline__ void pair_index(long long t, int symmetric, int nm2, int &I, int &J) {
@@ -178,14 +203,16 @@ arad_pair_kernel(const double *__restrict__ X1, const double *__restrict__ Z1,
                  const int *__restrict__ N1, SetWs w1, int nm1, const double *__restrict__ X2,
                  const double *__restrict__ Z2, const int *__restrict__ N2, SetWs w2, int nm2,
                  int amax, AradParams P, SigmaTable sig, int nsig, int symmetric,
-                 double *__restrict__ K) {
+                 double *__restrict__ K, const ClassInfo *fast_ci) {
+    // when the fast FP32 kernel handled this call, the generic one does nothing
+    if (fast_ci && fast_ci->flag == 0) return;
     const int lane = threadIdx.x & 31;
     const long long npairs = symmetric ? (long long)nm1 * (nm1 + 1) / 2 : (long long)nm1 * nm2;
     const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     const double eps = (double)5.0e-12f;  // single-precision literal in the source (:505)
-    const float inv_w_log2 = (float)(P.inv_width * 1.4426950408889634);
-    const float maxg2 = (float)P.maxg2, rw2f = (float)P.rw2, cw2f = (float)P.cw2;
+    const float maxg2s = (float)(P.maxg2 * fp32_scale(P) * fp32_scale(P));
+    const float rw2f = (float)P.rw2, cw2f = (float)P.cw2;
 
     for (long long t = warp0; t < npairs; t += nwarps) {
         int I, J;
@@ -213,7 +240,7 @@ arad_pair_kernel(const double *__restrict__ X1, const double *__restrict__ Z1,
             } else {
                 const float S = distl2_f32(w1.pk + b1 * amax, w1.pz + b1 * amax, w1.nnb[b1],
                                            w2.pk + b2 * amax, w2.pz + b2 * amax, w2.nnb[b2],
-                                           inv_w_log2, maxg2, rw2f, cw2f);
+                                           maxg2s, rw2f, cw2f);
                 l2 = (double)(w1.self32[b1] + w2.self32[b2] - 2.0f * S * (float)stoch);
             }
             if (fabs(l2) < eps) l2 = 0.0;  // :594
@@ -235,12 +262,344 @@ arad_pair_kernel(const double *__restrict__ X1, const double *__restrict__ Z1,
     }
 }
 
+// ---------------------------------------------------------------------------
+// Fast FP32 path.
+//
+// Molecule I's neighbour records (one record = one neighbour m1 of one atom
+// i1) are packed, whole atoms at a time, into passes of 32 lanes; molecule J
+// is staged in shared memory. A work item (pass p, atom j1 of J) lets every
+// lane sum its record against all of j1's neighbours (broadcast reads), then a
+// segmented warp scan forms S(i1, j1) for every atom i1 of the pass at the
+// last lane of its segment, which applies the kernel exponentials for every
+// sigma. Self terms come from the same code (J = I), so l2 cancels exactly for
+// identical environments.
+// ---------------------------------------------------------------------------
+constexpr int FC_BM = 8, FC_WARPS = 4, FC_MAXREC = 1024, FC_MAXA = 32, FC_MAXSIG = 8;
+constexpr int FC_SST = FC_MAXC + 1;
+
+__device__ __forceinline__ int ptp_pos(double row, double col) {
+    const double r = rint(row), c = rint(col);
+    if (r != row || c != col || r < 0.0 || r > 7.0 || c < 0.0 || c > 33.0) return -1;
+    return (int)r * 34 + (int)c;
+}
+
+// marks the periodic-table positions of the atoms and their neighbours
+__global__ void arad_class_scan_kernel(const double *__restrict__ X, const double *__restrict__ Z,
+                                       const int *__restrict__ N, int nm, int amax, double cut,
+                                       ClassInfo *ci) {
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long long)nm * amax) return;
+    const int m = (int)(gid / amax), a = (int)(gid % amax);
+    const int n = min(max(N[m], 0), amax);
+    if (a >= n) return;
+    const size_t base = (size_t)m * amax + a;
+    int pos = ptp_pos(Z[base * 2 + 0], Z[base * 2 + 1]);
+    if (pos < 0) { atomicOr(&ci->flag, 1); return; }
+    atomicOr(&ci->present[pos], 1);
+    const double *x = X + base * 5 * amax;
+    for (int k = 0; k < n && !(x[k] > cut); ++k) {
+        pos = ptp_pos(x[amax + k], x[2 * amax + k]);
+        if (pos < 0) { atomicOr(&ci->flag, 1); return; }
+        atomicOr(&ci->present[pos], 1);
+    }
+}
+
+// one thread: class ids and the stoichiometric table (farad_kernels.f90:80-81)
+__global__ void arad_class_build_kernel(ClassInfo *ci, double rw2, double cw2) {
+    int rows[FC_MAXC], cols[FC_MAXC];
+    int nc = 0;
+    for (int pos = 0; pos < FC_NPOS; ++pos) {
+        ci->map[pos] = -1;
+        if (ci->present[pos]) {
+            if (nc == FC_MAXC) { ci->flag |= 2; break; }
+            rows[nc] = pos / 34;
+            cols[nc] = pos % 34;
+            ci->map[pos] = (signed char)nc;
+            ++nc;
+        }
+    }
+    ci->ncls = nc;
+    for (int a = 0; a < FC_MAXC; ++a)
+        for (int b = 0; b < FC_MAXC; ++b) {
+            double v = 0.0;
+            if (a < nc && b < nc) {
+                const double dr = (double)(rows[a] - rows[b]), dc = (double)(cols[a] - cols[b]);
+                v = rw2 / (rw2 + dr * dr) * cw2 / (cw2 + dc * dc);
+            }
+            ci->stoch[a * FC_MAXC + b] = (float)v;
+        }
+}
+
+// element classes of every neighbour record and atom (after the class build)
+__global__ void arad_class_assign_kernel(const double *__restrict__ X, const double *__restrict__ Z,
+                                         const int *__restrict__ N, int nm, int amax,
+                                         const ClassInfo *ci, SetWs w) {
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long long)nm * amax) return;
+    const int m = (int)(gid / amax), a = (int)(gid % amax);
+    const int n = min(max(N[m], 0), amax);
+    const size_t base = (size_t)m * amax + a;
+    if (a >= n) { w.acls[base] = 0; return; }
+    int pos = ptp_pos(Z[base * 2 + 0], Z[base * 2 + 1]);
+    w.acls[base] = pos >= 0 ? max((int)ci->map[pos], 0) : 0;
+    const double *x = X + base * 5 * amax;
+    const int cnt = w.nnb[base];
+    for (int k = 0; k < cnt; ++k) {
+        pos = ptp_pos(x[amax + k], x[2 * amax + k]);
+        w.cls[base * amax + k] = pos >= 0 ? (signed char)max((int)ci->map[pos], 0) : 0;
+    }
+}
+
+struct FastSmem {
+    float4 recI[FC_MAXREC];      // molecule I, dense by atom, 32 records per pass
+    int metaI[FC_MAXREC];        // atom | seg_start << 8 | active << 24 | tail << 25
+    float selfI[FC_MAXA];
+    int aclsI[FC_MAXA];
+    float4 recJ[FC_MAXREC];      // molecule J, dense by atom
+    signed char clsJ[FC_MAXREC]; // element class of each record of J
+    int offJ[FC_MAXA + 1];
+    float selfJ[FC_MAXA];
+    int aclsJ[FC_MAXA];
+    float stoch[FC_MAXC * FC_SST];  // row stride 17: lanes of different classes hit distinct banks
+    float S[FC_MAXA * FC_MAXA];  // S(i1, j1) of the current molecule pair
+    float red[FC_WARPS][FC_MAXSIG];
+    int npassI, nI, nJ;
+};
+
+// Molecule I, dense: pass p holds records [32 p, 32 p + 32). Whole CTA; the
+// caller synchronises before the records are read.
+__device__ void fast_load_I(FastSmem &sm, const SetWs &w, int I, int amax, int nI,
+                            bool use_self) {
+    __shared__ int offI[FC_MAXA + 1];
+    if (threadIdx.x < 32) {  // exclusive prefix of the neighbour counts (nI <= 32)
+        const int a = threadIdx.x;
+        const int cnt = a < nI ? w.nnb[(size_t)I * amax + a] : 0;
+        int incl = cnt;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int o = __shfl_up_sync(0xffffffffu, incl, d);
+            if (a >= d) incl += o;
+        }
+        offI[a] = incl - cnt;
+        if (a == 31) {
+            offI[32] = incl;
+            sm.npassI = (incl + 31) / 32;
+            sm.nI = nI;
+        }
+    }
+    __syncthreads();
+    const int nrec = offI[32];
+    const int nslot = sm.npassI * 32;
+    for (int slot = nrec + threadIdx.x; slot < nslot; slot += blockDim.x) {
+        sm.metaI[slot] = ((slot & 31) << 8);  // inactive lane, own segment, no tail
+        sm.recI[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    for (int t = threadIdx.x; t < nI * amax; t += blockDim.x) {
+        const int a = t / amax, k = t % amax;
+        const int beg = offI[a], cnt = offI[a + 1] - beg;
+        if (k < cnt) {
+            const int slot = beg + k;
+            // segment = this atom's records inside this pass
+            const int seg = max(beg, slot & ~31) & 31;
+            const bool tail = (k == cnt - 1) || ((slot & 31) == 31);
+            const size_t src = ((size_t)I * amax + a) * amax + k;
+            sm.metaI[slot] = a | (seg << 8) | ((int)w.cls[src] << 16) | (1 << 24) |
+                             ((tail ? 1 : 0) << 25);
+            sm.recI[slot] = w.pk[src];
+        }
+    }
+    for (int a = threadIdx.x; a < nI; a += blockDim.x) {
+        sm.selfI[a] = use_self ? w.selff[(size_t)I * amax + a] : 0.0f;
+        sm.aclsI[a] = w.acls[(size_t)I * amax + a];
+    }
+}
+
+// Molecule J, dense by atom. Whole CTA; the caller synchronises before the
+// records are read.
+__device__ void fast_load_J(FastSmem &sm, const SetWs &w, int J, int amax, int nJ,
+                            bool use_self) {
+    if (threadIdx.x < 32) {  // exclusive prefix of the neighbour counts (nJ <= 32)
+        const int a = threadIdx.x;
+        const int cnt = a < nJ ? w.nnb[(size_t)J * amax + a] : 0;
+        int incl = cnt;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int o = __shfl_up_sync(0xffffffffu, incl, d);
+            if (a >= d) incl += o;
+        }
+        sm.offJ[a] = incl - cnt;
+        if (a == 31) {
+            sm.offJ[32] = incl;
+            sm.nJ = nJ;
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < nJ * amax; t += blockDim.x) {
+        const int a = t / amax, k = t % amax;
+        if (k < sm.offJ[a + 1] - sm.offJ[a]) {
+            const int d = sm.offJ[a] + k;
+            const size_t src = ((size_t)J * amax + a) * amax + k;
+            sm.recJ[d] = w.pk[src];
+            sm.clsJ[d] = w.cls[src];
+        }
+    }
+    for (int a = threadIdx.x; a < nJ; a += blockDim.x) {
+        sm.selfJ[a] = use_self ? w.selff[(size_t)J * amax + a] : 0.0f;
+        sm.aclsJ[a] = w.acls[(size_t)J * amax + a];
+    }
+}
+
+// Work item (pass p, atom j1): the segment sums of the pass against j1 are
+// added into S[i1][j1] by each segment's last lane (an atom split across two
+// passes contributes two partial sums; two terms commute, so the result does
+// not depend on their order).
+__device__ __forceinline__ void fast_item(FastSmem &sm, int p, int j1, float maxg2s) {
+    const int lane = threadIdx.x & 31;
+    const float4 u = sm.recI[p * 32 + lane];
+    const int meta = sm.metaI[p * 32 + lane];
+    const float *strow = sm.stoch + ((meta >> 16) & 0xff) * FC_SST;
+    const int beg = sm.offJ[j1], end = sm.offJ[j1 + 1];
+    float acc = 0.0f;
+#pragma unroll 4
+    for (int m2 = beg; m2 < end; ++m2) {
+        const float4 q = sm.recJ[m2];
+        const float dr = q.x - u.x;
+        const float t = dr * dr;
+        float e;
+        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(-t));
+        const float g = fmaf(u.w, q.w, fmaf(u.z, q.z, u.y * q.y));
+        const float eg = e * strow[sm.clsJ[m2]];
+        if (t < maxg2s) acc = fmaf(eg, g, acc);
+    }
+    const int seg = (meta >> 8) & 0xff;
+    float v = acc;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const float o = __shfl_up_sync(0xffffffffu, v, d);
+        if (lane - d >= seg) v += o;
+    }
+    if ((meta >> 25) & 1) atomicAdd(&sm.S[(meta & 0xff) * FC_MAXA + j1], v);
+}
+
+// All work items of one molecule pair, S cleared first. Whole CTA.
+__device__ __forceinline__ void fast_pair_sums(FastSmem &sm, int nJ, float maxg2s) {
+    for (int t = threadIdx.x; t < FC_MAXA * FC_MAXA; t += blockDim.x) sm.S[t] = 0.0f;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5;
+    const int items = sm.npassI * nJ;
+    for (int it = warp; it < items; it += FC_WARPS) fast_item(sm, it / nJ, it % nJ, maxg2s);
+    __syncthreads();
+}
+
+__device__ __forceinline__ void pair_block(long long t, int symmetric, int nbj, int &bi, int &bj) {
+    if (symmetric) {  // blocks bi <= bj
+        int r = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+        while ((long long)r * (r + 1) / 2 > t) --r;
+        while ((long long)(r + 1) * (r + 2) / 2 <= t) ++r;
+        bj = r;
+        bi = (int)(t - (long long)r * (r + 1) / 2);
+    } else {
+        bi = (int)(t / nbj);
+        bj = (int)(t % nbj);
+    }
+}
+
+// Self terms S(a, a) through the same passes, scan and partial sums as the
+// pair kernel, so that l2 = s + s - 2 S cancels exactly for an atom with itself.
+__global__ void __launch_bounds__(FC_WARPS * 32)
+arad_fast_self_kernel(SetWs w, const int *__restrict__ N, int nm, int amax, AradParams P,
+                      const ClassInfo *ci) {
+    __shared__ FastSmem sm;
+    if (ci->flag) return;
+    const int I = blockIdx.x;
+    if (I >= nm) return;
+    for (int t = threadIdx.x; t < FC_MAXC * FC_MAXC; t += blockDim.x)
+        sm.stoch[(t / FC_MAXC) * FC_SST + t % FC_MAXC] = ci->stoch[t];
+    const int nI = min(max(N[I], 0), amax);
+    fast_load_I(sm, w, I, amax, nI, false);
+    fast_load_J(sm, w, I, amax, nI, false);
+    __syncthreads();
+    const float maxg2s = (float)(P.maxg2 * fp32_scale(P) * fp32_scale(P));
+    fast_pair_sums(sm, nI, maxg2s);
+    for (int a = threadIdx.x; a < nI; a += blockDim.x)
+        w.selff[(size_t)I * amax + a] = sm.S[a * FC_MAXA + a];
+}
+
+__global__ void __launch_bounds__(FC_WARPS * 32)
+arad_fast_pair_kernel(SetWs w1, const int *__restrict__ N1, int nm1, SetWs w2,
+                      const int *__restrict__ N2, int nm2, int amax, AradParams P,
+                      const ClassInfo *ci, SigmaTable sig, int nsig, int symmetric,
+                      double *__restrict__ K) {
+    __shared__ FastSmem sm;
+    if (ci->flag) return;
+    const int nbj = (nm2 + FC_BM - 1) / FC_BM;
+    int bi, bj;
+    pair_block(blockIdx.x, symmetric, nbj, bi, bj);
+    for (int t = threadIdx.x; t < FC_MAXC * FC_MAXC; t += blockDim.x)
+        sm.stoch[(t / FC_MAXC) * FC_SST + t % FC_MAXC] = ci->stoch[t];
+    const float maxg2s = (float)(P.maxg2 * fp32_scale(P) * fp32_scale(P));
+    const float eps = 5.0e-12f;
+    float sc[FC_MAXSIG];
+#pragma unroll
+    for (int s = 0; s < FC_MAXSIG; ++s)
+        sc[s] = s < nsig ? (float)(sig.inv_sigma2[s] * 1.4426950408889634) : 0.0f;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int il = 0; il < FC_BM; ++il) {
+        const int I = bi * FC_BM + il;
+        if (I >= nm1) break;
+        __syncthreads();
+        const int nI = min(max(N1[I], 0), amax);
+        fast_load_I(sm, w1, I, amax, nI, true);
+        for (int jl = 0; jl < FC_BM; ++jl) {
+            const int J = bj * FC_BM + jl;
+            if (J >= nm2) break;
+            if (symmetric && J < I) continue;
+            __syncthreads();
+            const int nJ = min(max(N2[J], 0), amax);
+            fast_load_J(sm, w2, J, amax, nJ, true);
+            __syncthreads();
+            fast_pair_sums(sm, nJ, maxg2s);
+            // phase 2: l2 and the kernel exponentials of every atom pair
+            float kacc[FC_MAXSIG];
+#pragma unroll
+            for (int s = 0; s < FC_MAXSIG; ++s) kacc[s] = 0.0f;
+            for (int t = threadIdx.x; t < nI * nJ; t += blockDim.x) {
+                const int a = t / nJ, j1 = t - a * nJ;
+                const float stz = sm.stoch[sm.aclsI[a] * FC_SST + sm.aclsJ[j1]];
+                float l2 = sm.selfI[a] + sm.selfJ[j1] - 2.0f * sm.S[a * FC_MAXA + j1] * stz;
+                if (fabsf(l2) < eps) l2 = 0.0f;  // farad_kernels.f90:594
+#pragma unroll
+                for (int s = 0; s < FC_MAXSIG; ++s) {
+                    if (s < nsig) {
+                        float e;
+                        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(l2 * sc[s]));
+                        kacc[s] += e;
+                    }
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < FC_MAXSIG; ++s) {
+                float v = kacc[s];
+                for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0) sm.red[warp][s] = v;
+            }
+            __syncthreads();
+            if (threadIdx.x < nsig) {
+                const int s = threadIdx.x;
+                double v = 0.0;
+                for (int q = 0; q < FC_WARPS; ++q) v += (double)sm.red[q][s];
+                K[((size_t)s * nm1 + I) * nm2 + J] = v;
+                if (symmetric) K[((size_t)s * nm1 + J) * nm2 + I] = v;
+            }
+        }
+    }
+}
+
 }  // namespace
 }  // namespace fmlb
 
 extern "C" size_t fmlb_arad_workspace_bytes(int nm1, int nm2, int amax, int symmetric) {
     if (nm1 < 0 || nm2 < 0 || amax < 1) return 0;
-    return fmlb::set_ws_bytes(nm1, amax) + (symmetric ? 0 : fmlb::set_ws_bytes(nm2, amax));
+    return fmlb::set_ws_bytes(nm1, amax) + (symmetric ? 0 : fmlb::set_ws_bytes(nm2, amax)) +
+           fmlb::align256(sizeof(fmlb::ClassInfo));
 }
 
 extern "C" int fmlb_arad_kernels(const double *X1, const double *Z1, const int *N1, int nm1,
@@ -278,6 +637,7 @@ extern "C" int fmlb_arad_kernels(const double *X1, const double *Z1, const int *
     char *p = static_cast<char *>(workspace);
     SetWs w1 = carve(p, nm1, amax);
     SetWs w2 = symmetric ? w1 : carve(p, nm2, amax);
+    ClassInfo *ci = reinterpret_cast<ClassInfo *>(p);
     const int tpb = 128;
     {
         const long long n = (long long)nm1 * amax;
@@ -290,20 +650,50 @@ extern "C" int fmlb_arad_kernels(const double *X1, const double *Z1, const int *
         arad_prep_kernel<<<ceil_div(n, tpb), tpb, 0, st>>>(X2, N2, nm2, amax, P, 1, w2);
         FMLB_TRY(launch_status("arad_prep_kernel"));
     }
+    // fast FP32 path: amax <= 32 and at most 16 element classes (decided on the device)
+    const bool try_fast = precision == 1 && amax <= FC_MAXA;
+    if (try_fast) {
+        FMLB_TRY(cuda_status(cudaMemsetAsync(ci, 0, sizeof(ClassInfo), st), "clear class info"));
+        arad_class_scan_kernel<<<ceil_div((long long)nm1 * amax, tpb), tpb, 0, st>>>(
+            X1, Z1, N1, nm1, amax, P.cut, ci);
+        if (!symmetric)
+            arad_class_scan_kernel<<<ceil_div((long long)nm2 * amax, tpb), tpb, 0, st>>>(
+                X2, Z2, N2, nm2, amax, P.cut, ci);
+        arad_class_build_kernel<<<1, 1, 0, st>>>(ci, P.rw2, P.cw2);
+        arad_class_assign_kernel<<<ceil_div((long long)nm1 * amax, tpb), tpb, 0, st>>>(
+            X1, Z1, N1, nm1, amax, ci, w1);
+        if (!symmetric)
+            arad_class_assign_kernel<<<ceil_div((long long)nm2 * amax, tpb), tpb, 0, st>>>(
+                X2, Z2, N2, nm2, amax, ci, w2);
+        arad_fast_self_kernel<<<nm1, FC_WARPS * 32, 0, st>>>(w1, N1, nm1, amax, P, ci);
+        if (!symmetric) arad_fast_self_kernel<<<nm2, FC_WARPS * 32, 0, st>>>(w2, N2, nm2, amax, P, ci);
+        FMLB_TRY(launch_status("arad fast-path preparation"));
+    }
     const long long npairs = symmetric ? (long long)nm1 * (nm1 + 1) / 2 : (long long)nm1 * nm2;
     const int blocks = (int)std::min<long long>(ceil_div(npairs, tpb / 32), (long long)sm_count() * 64);
-    for (int s0 = 0; s0 < nsigma; s0 += MAXSIG) {
-        const int ns = nsigma - s0 < MAXSIG ? nsigma - s0 : MAXSIG;
+    const int chunk = try_fast ? FC_MAXSIG : MAXSIG;
+    for (int s0 = 0; s0 < nsigma; s0 += chunk) {
+        const int ns = nsigma - s0 < chunk ? nsigma - s0 : chunk;
         SigmaTable sig;
         for (int s = 0; s < ns; ++s)
             sig.inv_sigma2[s] = -1.0 / (sigmas_host[s0 + s] * sigmas_host[s0 + s]);
         double *Ks = K + (size_t)s0 * nm1 * nm2;
-        if (precision == 0)
+        if (precision == 0) {
             arad_pair_kernel<true><<<blocks, tpb, 0, st>>>(X1, Z1, N1, w1, nm1, X2, Z2, N2, w2, nm2,
-                                                           amax, P, sig, ns, symmetric, Ks);
-        else
+                                                           amax, P, sig, ns, symmetric, Ks, nullptr);
+        } else {
+            if (try_fast) {
+                const long long nbi = ceil_div(nm1, FC_BM), nbj = ceil_div(nm2, FC_BM);
+                const long long nblk = symmetric ? nbi * (nbi + 1) / 2 : nbi * nbj;
+                FMLB_REQUIRE(nblk < (1LL << 31), "fmlb_arad_kernels: too many molecule blocks");
+                arad_fast_pair_kernel<<<(unsigned)nblk, FC_WARPS * 32, 0, st>>>(
+                    w1, N1, nm1, w2, N2, nm2, amax, P, ci, sig, ns, symmetric, Ks);
+                FMLB_TRY(launch_status("arad_fast_pair_kernel"));
+            }
             arad_pair_kernel<false><<<blocks, tpb, 0, st>>>(X1, Z1, N1, w1, nm1, X2, Z2, N2, w2,
-                                                            nm2, amax, P, sig, ns, symmetric, Ks);
+                                                            nm2, amax, P, sig, ns, symmetric, Ks,
+                                                            try_fast ? ci : nullptr);
+        }
         FMLB_TRY(launch_status("arad_pair_kernel"));
     }
     return FMLB_OK;

@@ -371,3 +371,45 @@ def test_cho_solve_wide_outer_panels(oracle_mod):
     B[5001, 5001] = -1.0
     with pytest.warns(fml_b200.CholeskyWarning, match="error code: 5002$"):
         fml_b200.cho_solve(B, y)
+
+
+def _arad_set(oracle_mod, nmol, nmax, seed, cut, zpool=None):
+    b = synthetic.generate(nmol, nmax=nmax, seed=seed)
+    charges = b.charges.copy()
+    if zpool is not None:
+        rng = np.random.default_rng(seed)
+        charges = rng.choice(np.asarray(zpool, dtype=np.float64), size=len(charges))
+    X = oracle_mod.arad_descriptors(charges, b.coords, b.offsets, nmax, cut)
+    Z = [charges[b.offsets[i]:b.offsets[i + 1]] for i in range(nmol)]
+    return X, Z
+
+
+@pytest.mark.parametrize("zpool,nmax", [(None, 23), ([1, 3, 4, 5, 6, 7, 8, 9, 11, 12, 13, 14, 15,
+                                                      16, 17, 19, 20, 35], 23), (None, 40)])
+def test_arad_fp32_paths_vs_fp64(oracle_mod, zpool, nmax):
+    """FP32 ARAD kernels (the fast path for <= 16 element classes and amax <= 32,
+    the generic path otherwise) against the FP64 oracle: relative error <= 2e-3
+    for sigma >= 0.5 (FP32 cancellation in l2 = s1 + s2 - 2 S stoch)."""
+    X, Z = _arad_set(oracle_mod, 30, nmax, 77, 1e6, zpool)
+    sig = [0.5, 1.0, 2.0, 5.0]
+    K32 = fml_b200.get_atomic_kernels_arad(X[:17], X[17:], Z[:17], Z[17:], sig, precision="fp32")
+    K64 = oracle_mod.get_atomic_kernels_arad(X[:17], X[17:], Z[:17], Z[17:], sig)
+    rel = np.abs(K32 - K64) / np.maximum(np.abs(K64), 1e-300)
+    assert rel.max() < 2e-3, rel.max()
+    S32 = fml_b200.get_atomic_symmetric_kernels_arad(X, Z, sig, precision="fp32")
+    S64 = oracle_mod.get_atomic_symmetric_kernels_arad(X, Z, sig)
+    rel = np.abs(S32 - S64) / np.maximum(np.abs(S64), 1e-300)
+    assert rel.max() < 2e-3, rel.max()
+    np.testing.assert_array_equal(S32, np.swapaxes(S32, 1, 2))
+
+
+def test_arad_fp32_fixtures_sigma_sweep(golden):
+    """Reference fixtures (tests/test_arad.py sigmas): FP32 max-abs error stated per sigma."""
+    g = golden
+    x = g["arad_xyz_s30_c5"]
+    Z = [list(z) for z, _ in _mols(g, "xyz_")]
+    K32 = fml_b200.get_atomic_kernels_arad(x[:5], x[5:], Z[:5], Z[5:], list(g["testarad_sigmas"]),
+                                           precision="fp32")
+    ref = g["testarad_K_5v5"]
+    for k in range(len(g["testarad_sigmas"])):
+        assert np.abs(K32[k] - ref[k]).max() <= 2e-3 * np.abs(ref[k]).max() + 1e-6
