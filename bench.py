@@ -489,6 +489,16 @@ def run_stages(a):
           "ms": ms, "entries_per_s": nl * nl * ns / (ms * 1e-3), "bound": "fp64",
           "achieved_tflops": fl / ms / 1e9, "peak_tflops": dgemm, "frac": fl / ms / 1e9 / dgemm})
     del Kl
+    Kl32 = torch.empty((ns, n, n), dtype=torch.float32, device=dev)
+    ms = _time(torch, lambda: _lib.call("fmlb_laplacian_kernel_f32", P(Xt), n, L, P(Xt), n, L, L,
+                                        sp, ns, P(Kl32), n, n * n, 1, st), reps=2)
+    terms = float(L) * n * (n + 1) / 2
+    fp32_tf = 2.0 * terms / ms / 1e9  # 2 FP32 instructions (sub, abs-add) per term
+    emit({"stage": "laplacian_f32_symmetric", "config": "N=%d, d=%d, %d sigmas" % (n, L, ns),
+          "ms": ms, "entries_per_s": n * n * ns / (ms * 1e-3), "bound": "fp32 issue",
+          "achieved_fp32_tinst": fp32_tf, "peak_fp32_tinst": FP32_PEAK_TFLOPS / 2,
+          "frac": fp32_tf / (FP32_PEAK_TFLOPS / 2)})
+    del Kl32
 
     # --- Cholesky, solve, prediction ------------------------------------------
     K1 = torch.empty((n, n), dtype=torch.float64, device=dev)

@@ -40,10 +40,15 @@ SIGNATURES = {
     "fmlb_kernel_predict_workspace_bytes": (_sz, [_i, _i, _i]),
     "fmlb_kernel_predict_f64": (_i, [_i, _vp, _i, _i, _vp, _i, _i, _i, _dp, _i, _vp, _ll, _vp,
                                      _ll, _vp, _sz, _vp]),
+    "fmlb_laplacian_kernel_f32": (_i, [_vp, _i, _i, _vp, _i, _i, _i, _dp, _i, _vp, _ll, _ll, _i,
+                                       _vp]),
     "fmlb_tc_operand_bytes": (_sz, [_i, _i]),
     "fmlb_column_mean_f64": (_i, [_vp, _i, _i, _i, _vp, _vp]),
     "fmlb_gaussian_kernel_tc": (_i, [_vp, _i, _i, _vp, _i, _i, _i, _vp, _dp, _i, _vp, _ll, _ll,
                                      _i, _vp, _sz, _vp, _vp]),
+    "fmlb_batch_problem_bytes": (_sz, []),
+    "fmlb_batch_buffer_doubles": (_sz, [_i]),
+    "fmlb_krr_batched_f64": (_i, [_vp, _vp, _i, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _i, _vp]),
     "fmlb_kernel_predict_f64_noalloc": (_i, [_i, _vp, _i, _i, _vp, _i, _i, _i, _dp, _i, _vp, _ll,
                                              _vp, _ll, _vp]),
 }

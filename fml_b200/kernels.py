@@ -49,7 +49,7 @@ def _descriptor_rows(A):
     return rows, True
 
 
-def _pairwise(A, B, sigma, fn):
+def _pairwise(A, B, sigma, fn, out_dtype=torch.float64):
     sig, scalar = _sigma_list(sigma)
     symmetric = A is B
     a, as_np = _descriptor_rows(A)
@@ -58,7 +58,7 @@ def _pairwise(A, B, sigma, fn):
         raise ValueError("A and B must hold descriptors of the same length")
     na, d = a.shape
     nb = b.shape[0]
-    K = torch.empty((len(sig), na, nb), dtype=torch.float64, device=device())
+    K = torch.empty((len(sig), na, nb), dtype=out_dtype, device=device())
     sp, keep = _lib.host_doubles(sig)
     if na and nb:
         _lib.call(fn, _lib.ptr(a), na, d, _lib.ptr(b), nb, d, d, sp, len(sig), _lib.ptr(K), nb,
@@ -118,8 +118,16 @@ def gaussian_kernel(A, B, sigma, precision="fp64"):
     return _pairwise(A, B, sigma, "fmlb_gaussian_kernel_f64")
 
 
-def laplacian_kernel(A, B, sigma):
-    """K_ij = exp(-1 / sigma * ||A_i - B_j||_1), FP64 direct differences."""
+def laplacian_kernel(A, B, sigma, precision="fp64"):
+    """K_ij = exp(-1 / sigma * ||A_i - B_j||_1).
+
+    precision="fp64": FP64 direct differences (the reference's arithmetic);
+    precision="fp32": FP32 CUDA-core kernel, FP32 result.
+    """
+    if precision == "fp32":
+        return _pairwise(A, B, sigma, "fmlb_laplacian_kernel_f32", torch.float32)
+    if precision != "fp64":
+        raise ValueError("precision must be 'fp64' or 'fp32'")
     return _pairwise(A, B, sigma, "fmlb_laplacian_kernel_f64")
 
 

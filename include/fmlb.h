@@ -174,6 +174,17 @@ int fmlb_kernel_predict_f64(int kind, const double *Xq, int nq, int ldq, const d
                             void *workspace, size_t ws_bytes, void *stream);
 
 /* ------------------------------------------------------------------------
+ * Laplacian kernel matrix in FP32 (mixed precision), the FP32 form of
+ * flaplacian_kernel (fml/kernels/fkernels.f90:351-377): same arguments as
+ * fmlb_laplacian_kernel_f64 with an FP32 output. Descriptors are read in FP64
+ * and converted to FP32; the L1 sums are FP32. Relative error against the FP64
+ * kernel about 1e-6 * sum|a-b| / sigma.
+ * ---------------------------------------------------------------------- */
+int fmlb_laplacian_kernel_f32(const double *A, int na, int lda, const double *B, int nb, int ldb,
+                              int d, const double *sigmas_host, int nsigma, float *K,
+                              long long ldk, long long sigma_stride, int symmetric, void *stream);
+
+/* ------------------------------------------------------------------------
  * Gaussian kernel matrix on the tcgen05 tensor cores (mixed precision).
  * Mixed-precision form of fgaussian_kernel (fml/kernels/fkernels.f90:317-349):
  * K_s[i, j] = exp(-(|x_i|^2 + |x_j|^2 - 2 x_i.x_j) / (2 sigma_s^2)) on
@@ -196,6 +207,27 @@ int fmlb_gaussian_kernel_tc(const double *A, int na, int lda, const double *B, i
                             int d, const double *mu, const double *sigmas_host, int nsigma,
                             float *K, long long ldk, long long sigma_stride, int symmetric,
                             void *workspace, size_t ws_bytes, int *status, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Batched KRR: many independent problems of uneven size in ONE persistent
+ * launch (the user-side composition of gaussian_kernel, cho_solve and the
+ * prediction, fml/kernels/kernels.py:167-196 and fml/math/cho_solve.py:33-58,
+ * per problem). `grid` CTAs (<= 0: one per SM) pull problems from a device
+ * queue in the order `order` (largest first is best); each CTA runs a whole
+ * problem: kernel matrix (Gaussian of descriptor rows, or precomputed),
+ * + lambda I, blocked FP64 Cholesky, solve, prediction of its test rows.
+ *   problems  device array of nprob records of fmlb_batch_problem_bytes()
+ *             bytes (layout in fml_b200/batched.py)
+ *   counter   device int (work-queue head; reset by the call)
+ *   X (rows, ldx) descriptors, Y targets, pred outputs, buf: per-problem
+ *             matrices + workspaces (fmlb_batch_buffer_doubles(n) each)
+ *   info      device int per problem: LAPACK-style Cholesky info (0 = ok)
+ * ---------------------------------------------------------------------- */
+size_t fmlb_batch_problem_bytes(void);
+size_t fmlb_batch_buffer_doubles(int n);
+int fmlb_krr_batched_f64(const void *problems, const int *order, int nprob, int *counter,
+                         const double *X, int ldx, int d, const double *Y, double *pred,
+                         double *buf, int *info, int grid, void *stream);
 
 /* Allocation-free form of fmlb_kernel_predict_f64 (same arguments minus the
  * workspace, same results). It has no counterpart in the reference: it exists

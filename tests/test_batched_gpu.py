@@ -1,0 +1,82 @@
+"""Batched uneven KRR (one persistent launch + multi-CTA path for large
+problems) against the oracle solved problem by problem.
+
+Tolerance: predictions to 1e-8 relative (well-conditioned problems, lambda
+>= 1e-4)."""
+
+import numpy as np
+import pytest
+import torch
+
+from fml_b200 import synthetic
+from fml_b200.batched import BatchedKRR, GaussianProblem, PrecomputedProblem
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_predict(oracle_mod, Xtr, y, Xte, sigma, lam):
+    K = oracle_mod.gaussian_kernel(Xtr.T, Xtr.T, sigma)
+    K[np.diag_indices_from(K)] += lam
+    alpha, info = oracle_mod.cho_solve(K, y)
+    return oracle_mod.gaussian_kernel(Xte.T, Xtr.T, sigma) @ alpha, info
+
+
+@pytest.fixture(scope="module")
+def problems(oracle_mod):
+    rng = np.random.default_rng(3)
+    sizes = [70, 130, 257, 64, 1, 500, 900, 33, 200, 1300]
+    out = []
+    for i, n in enumerate(sizes):
+        b = synthetic.generate(n + 40, nmax=23, seed=100 + i)
+        X = oracle_mod.coulomb_matrices(b.charges, b.coords, b.offsets, 23)
+        out.append(GaussianProblem(X[:n], b.energies[:n], X[n:], float(rng.uniform(200, 1000)),
+                                   float(10 ** rng.uniform(-4, -2))))
+    return out
+
+
+def test_batched_matches_per_problem_oracle(oracle_mod, problems):
+    bk = BatchedKRR(problems, split_threshold=600, grid=0)
+    assert bk.big and bk.small  # both paths exercised
+    bk.run()
+    torch.cuda.synchronize()
+    assert (bk.infos() == 0).all()
+    for p, pred in zip(problems, bk.predictions()):
+        ref, info = _oracle_predict(oracle_mod, p.X_train, p.y, p.X_test, p.sigma, p.lam)
+        assert info == 0
+        np.testing.assert_allclose(pred, ref, rtol=1e-8, atol=1e-8 * np.abs(ref).max())
+
+
+def test_batched_graph_replay_is_identical(problems):
+    bk = BatchedKRR(problems, split_threshold=600, grid=0)
+    bk.run()
+    torch.cuda.synchronize()
+    first = [p.copy() for p in bk.predictions()]
+    g = bk.capture()
+    bk.pred.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    for a, b in zip(first, bk.predictions()):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_batched_precomputed_kernels_and_failure_isolation(oracle_mod, problems):
+    # two ARAD problems (precomputed kernels) and one indefinite problem
+    b = synthetic.generate(60, nmax=12, seed=9)
+    X = oracle_mod.arad_descriptors(b.charges, b.coords, b.offsets, 12, 1e6)
+    Z = [b.molecule(i)[0] for i in range(b.nmol)]
+    Ktr = oracle_mod.get_atomic_symmetric_kernels_arad(X[:45], Z[:45], [2.0])[0]
+    Kte = oracle_mod.get_atomic_kernels_arad(X[45:], X[:45], Z[45:], Z[:45], [2.0])[0]
+    arad = PrecomputedProblem(Ktr, Kte, b.energies[:45], 1e-3)
+    bad = PrecomputedProblem(-np.eye(20), np.ones((3, 20)), np.ones(20), 0.0)
+    probs = problems[:4] + [arad, bad]
+    bk = BatchedKRR(probs, split_threshold=10000, grid=0)
+    bk.run()
+    torch.cuda.synchronize()
+    info = bk.infos()
+    assert info[5] == 1 and (info[:5] == 0).all()
+    Ka = Ktr + 1e-3 * np.eye(45)
+    alpha, _ = oracle_mod.cho_solve(Ka, b.energies[:45])
+    np.testing.assert_allclose(bk.predictions()[4], Kte @ alpha, rtol=1e-8)
+    for p, pred in zip(problems[:4], bk.predictions()[:4]):
+        ref, _ = _oracle_predict(oracle_mod, p.X_train, p.y, p.X_test, p.sigma, p.lam)
+        np.testing.assert_allclose(pred, ref, rtol=1e-8, atol=1e-8 * np.abs(ref).max())

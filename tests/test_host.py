@@ -69,3 +69,16 @@ def test_arad_size_asserts():
         fml_b200.get_atomic_kernels_arad(X, np.zeros((2, 4, 5, 4)), [[1], [1]], [[1], [1]], [1.0])
     with pytest.raises(AssertionError, match="code = 4"):
         fml_b200.get_atomic_symmetric_kernels_arad(X, [[1]], [1.0])
+
+
+def test_autotune_cache_roundtrip(tmp_path, monkeypatch):
+    from fml_b200 import autotune
+    from fml_b200.batched import GaussianProblem
+    monkeypatch.setenv("FMLB_AUTOTUNE_CACHE", str(tmp_path / "cache.json"))
+    monkeypatch.setenv("FMLB_AUTOTUNE", "0")
+    probs = [GaussianProblem(np.zeros((n, 3)), np.zeros(n), np.zeros((2, 3)), 1.0, 1e-3)
+             for n in (100, 300, 3000)]
+    assert autotune.batched_config(probs) == autotune.DEFAULT
+    key = "batched_krr|%s|%s" % (autotune.shape_class(probs), autotune.gpu_key())
+    autotune._store({key: {"split_threshold": 2048, "grid": 296}})
+    assert autotune.batched_config(probs)["split_threshold"] == 2048

@@ -413,3 +413,26 @@ def test_arad_fp32_fixtures_sigma_sweep(golden):
     ref = g["testarad_K_5v5"]
     for k in range(len(g["testarad_sigmas"])):
         assert np.abs(K32[k] - ref[k]).max() <= 2e-3 * np.abs(ref[k]).max() + 1e-6
+
+
+@pytest.mark.parametrize("na,nb", [(300, 300), (130, 257), (1, 129)])
+def test_laplacian_fp32_vs_fp64(oracle_mod, cm_large, na, nb):
+    """FP32 Laplacian: relative error <= 1e-4 where K > 1e-30 (FP32 L1 sums)."""
+    A = cm_large[:na].T
+    B = cm_large[-nb:].T
+    sig = [100.0, 400.0, 1600.0]
+    K = fml_b200.laplacian_kernel(A, B, sig, precision="fp32")
+    assert K.dtype == np.float32
+    for k, s in enumerate(sig):
+        ref = oracle_mod.laplacian_kernel(A, B, s)
+        big = ref > 1e-30
+        assert (np.abs(K[k][big] - ref[big]) / ref[big]).max() <= 1e-4
+        assert np.abs(K[k][~big]).max(initial=0.0) <= 1e-30
+
+
+def test_laplacian_fp32_symmetric(cm_large):
+    A = cm_large[:333].T
+    K = fml_b200.laplacian_kernel(A, A, [200.0, 800.0], precision="fp32")
+    for k in range(2):
+        np.testing.assert_array_equal(K[k], K[k].T)
+        np.testing.assert_array_equal(np.diag(K[k]), 1.0)
