@@ -57,6 +57,10 @@ def parse():
     p.add_argument("--stages", nargs="?", const="all", default=None,
                    help="time each hot-path kernel on its own (one JSON line per stage); "
                         "'arad' times only the ARAD kernels")
+    p.add_argument("--workload", default="krr", choices=["krr", "batched", "serving"],
+                   help="krr: the large-N KRR step (default, the headline line); batched: "
+                        "256 uneven problems in one persistent launch; serving: the request loop")
+    p.add_argument("--nprob", type=int, default=256)
     p.add_argument("--arad-nmol", type=int, default=4000,
                    help="molecules of the ARAD stage (the first 3/4 form the symmetric set)")
     return p.parse_args()
@@ -593,8 +597,246 @@ def run_arad_stage(a, torch, lib, st, P):
     return out
 
 
+# ---------------------------------------------------------------------------
+# batched uneven KRR (256 problems, one persistent launch, CUDA graph)
+# ---------------------------------------------------------------------------
+def batched_problems(nprob, nt=500, arad_fraction=0.5):
+    """Uneven KRR problems: problem p draws from seed 1000+p its descriptor kind
+    (ARAD with probability ``arad_fraction``, else the sorted CM, nmax 23), its
+    training size (log-uniform 100..4000), sigma and lambda (log-uniform
+    1e-10..1e-6). CM problems take sigma log-uniform in [50, 2000]; ARAD
+    problems take the same quantile of [0.1, 5] (ARAD kernel entries are sums of
+    exp(-l2/sigma^2) with l2 of order one, so sigma >= 50 makes every term ~1
+    and K numerically rank one). ARAD descriptors use the Molecule default
+    cut 5.0 (fml/fml.py:80-86)."""
+    import torch
+
+    import fml_b200
+    from fml_b200 import synthetic
+    from fml_b200.batched import AradProblem, GaussianProblem
+
+    probs, kinds, ytest = [], [], []
+    for p in range(nprob):
+        rng = np.random.default_rng(1000 + p)
+        is_arad = rng.random() < arad_fraction
+        n = int(round(np.exp(rng.uniform(np.log(100), np.log(4000)))))
+        u = rng.random()
+        lam = float(np.exp(rng.uniform(np.log(1e-10), np.log(1e-6))))
+        b = synthetic.generate(n + nt, nmax=23, seed=1000 + p)
+        y = b.energies[:n]
+        if is_arad:
+            sigma = float(0.1 * 50.0 ** u)
+            X = fml_b200.generate_arad_descriptors(torch.from_numpy(b.charges).cuda(),
+                                                   torch.from_numpy(b.coords).cuda(),
+                                                   torch.from_numpy(b.offsets).cuda(), size=23)
+            Z = [b.charges[b.offsets[i]:b.offsets[i + 1]] for i in range(n + nt)]
+            probs.append(AradProblem(X[:n], Z[:n], y, X[n:], Z[n:], sigma, lam))
+        else:
+            sigma = float(50.0 * 40.0 ** u)
+            X = fml_b200.generate_coulomb_matrices(b.charges, b.coords, b.offsets, size=23)
+            probs.append(GaussianProblem(X[:n], y, X[n:], sigma, lam))
+        kinds.append("arad" if is_arad else "cm")
+        ytest.append(b.energies[n:])
+    return probs, kinds, ytest, nt
+
+
+class PlainLoop:
+    """The plain FP64 GPU path looped over the problems: FP64 kernel build,
+    K + lambda I, blocked Cholesky, solve, prediction, one problem at a time."""
+
+    def __init__(self, probs):
+        import ctypes
+
+        import torch
+
+        from fml_b200 import _lib
+        from fml_b200.batched import AradProblem
+        from fml_b200.kernels import _ptp_arrays
+        self.lib = _lib.load()
+        self.probs = probs
+        nmax = max(len(p.y) for p in probs)
+        ntmax = max(len(p.Z_test) if isinstance(p, AradProblem) else p.X_test.shape[0]
+                    for p in probs)
+        dev = torch.device("cuda")
+        self.K = torch.empty(nmax * nmax, dtype=torch.float64, device=dev)
+        self.Kt = torch.empty(max(ntmax * nmax, 1), dtype=torch.float64, device=dev)
+        self.work = torch.empty(self.lib.fmlb_potrf_workspace_bytes(nmax), dtype=torch.uint8,
+                                device=dev)
+        self.pwork = torch.empty(self.lib.fmlb_kernel_predict_workspace_bytes(ntmax, nmax, 1),
+                                 dtype=torch.uint8, device=dev)
+        self.info = torch.zeros(len(probs), dtype=torch.int32, device=dev)
+        self.pred, self.staged = [], []
+        wsb = 256
+        for p in probs:
+            n = len(p.y)
+            st = {"y": torch.from_numpy(np.asarray(p.y, np.float64)).to(dev),
+                  "alpha": torch.empty(n, dtype=torch.float64, device=dev),
+                  "sig": (ctypes.c_double * 1)(p.sigma)}
+            if isinstance(p, AradProblem):
+                amax = p.X_train.shape[1]
+                z1, n1 = _ptp_arrays(p.Z_train, amax)
+                z2, n2 = _ptp_arrays(p.Z_test, amax)
+                st.update(X1=p.X_train.contiguous(), X2=p.X_test.contiguous(),
+                          Z1=torch.from_numpy(z1).to(dev), N1=torch.from_numpy(n1).to(dev),
+                          Z2=torch.from_numpy(z2).to(dev), N2=torch.from_numpy(n2).to(dev),
+                          nt=len(p.Z_test), amax=amax)
+                wsb = max(wsb, self.lib.fmlb_arad_workspace_bytes(n, n, amax, 1),
+                          self.lib.fmlb_arad_workspace_bytes(len(p.Z_test), n, amax, 0))
+            else:
+                st.update(Xtr=torch.from_numpy(np.ascontiguousarray(p.X_train)).to(dev),
+                          Xte=torch.from_numpy(np.ascontiguousarray(p.X_test)).to(dev),
+                          nt=p.X_test.shape[0], d=p.X_train.shape[1])
+            self.pred.append(torch.empty(max(st["nt"], 1), dtype=torch.float64, device=dev))
+            self.staged.append(st)
+        self.ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+
+    def launches(self):
+        from fml_b200.kernels import arad_launches
+        from fml_b200.krr import potrf_launches
+        c = 0
+        for st, p in zip(self.staged, self.probs):
+            n = len(p.y)
+            if "X1" in st:
+                c += arad_launches(True, "fp64", st["amax"], 1) + \
+                    arad_launches(False, "fp64", st["amax"], 1) + 1
+            else:
+                c += 1 + 2
+            c += 1 + potrf_launches(n) + 2 * -(-n // 128)
+        return c
+
+    def run(self):
+        import ctypes
+
+        import torch
+
+        from fml_b200 import _lib
+        P = _lib.ptr
+        s = _lib.stream_handle()
+        for k, (st, p) in enumerate(zip(self.staged, self.probs)):
+            n, nt = len(p.y), st["nt"]
+            sp = ctypes.cast(st["sig"], ctypes.POINTER(ctypes.c_double))
+            if "X1" in st:
+                _lib.call("fmlb_arad_kernels", P(st["X1"]), P(st["Z1"]), P(st["N1"]), n, None,
+                          None, None, n, st["amax"], sp, 1, 0.2, 6.0, 1.0, 0.5, 1, 0, P(self.K),
+                          P(self.ws), self.ws.numel(), s)
+            else:
+                d = st["d"]
+                _lib.call("fmlb_gaussian_kernel_f64", P(st["Xtr"]), n, d, P(st["Xtr"]), n, d, d,
+                          sp, 1, P(self.K), n, n * n, 1, s)
+            _lib.call("fmlb_add_diagonal_f64", P(self.K), n, n, p.lam, s)
+            _lib.call("fmlb_potrf_f64", P(self.K), n, n, P(self.work), P(self.info[k:k + 1]), s)
+            st["alpha"].copy_(st["y"])
+            _lib.call("fmlb_potrs_f64", P(self.K), n, n, P(self.work), P(st["alpha"]), s)
+            if "X1" in st:
+                _lib.call("fmlb_arad_kernels", P(st["X2"]), P(st["Z2"]), P(st["N2"]), nt,
+                          P(st["X1"]), P(st["Z1"]), P(st["N1"]), n, st["amax"], sp, 1, 0.2, 6.0,
+                          1.0, 0.5, 0, 0, P(self.Kt), P(self.ws), self.ws.numel(), s)
+                _lib.call("fmlb_gemv_f64", P(self.Kt), n, nt, n, P(st["alpha"]),
+                          P(self.pred[k]), s)
+            else:
+                d = st["d"]
+                _lib.call("fmlb_kernel_predict_f64", 0, P(st["Xte"]), nt, d, P(st["Xtr"]), n, d,
+                          d, sp, 1, P(st["alpha"]), n, P(self.pred[k]), nt, P(self.pwork),
+                          self.pwork.numel(), s)
+        return torch.cuda.current_stream()
+
+
+def run_batched(a):
+    """256 uneven KRR problems (CM Gaussian and ARAD) in one pass: ARAD kernel
+    builds on side streams, then one persistent launch that builds the Gaussian
+    kernels and factors / solves / predicts every problem up to the autotuned
+    split (larger ones on the multi-CTA path), all captured in one CUDA graph.
+    Compared with the plain FP64 path looped over the problems."""
+    import torch
+
+    from fml_b200 import autotune
+    from fml_b200.batched import BatchedKRR
+
+    torch.cuda.set_device(0)
+    probs, kinds, ytest, nt = batched_problems(a.nprob)
+    bk = BatchedKRR(probs, split_threshold=autotune.DEFAULT["split_threshold"],
+                    grid=autotune.DEFAULT["grid"])
+    cfg = autotune.batched_config(probs, tune=True, batch=bk)
+    bk.configure(cfg["split_threshold"], cfg["grid"])
+    g = bk.capture()
+    for _ in range(max(a.warmup - 1, 0)):
+        g.replay()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / a.steps
+    preds = bk.predictions()
+    info_b = bk.infos()
+    # the solve pass alone (ARAD kernels restored, not rebuilt)
+    bk.keep_kernels()
+    gs = bk.capture(builds=False)
+    gs.replay()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(a.steps):
+        gs.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms_solve = e0.elapsed_time(e1) / a.steps
+    del gs, g
+    # the plain FP64 path looped per problem (timed once, after one warm-up pass)
+    loop = PlainLoop(probs)
+    loop.run()
+    torch.cuda.synchronize()
+    e0.record()
+    loop.run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms_loop = e0.elapsed_time(e1)
+    info_l = loop.info.cpu().numpy()
+    rel_mae, max_diff = {"cm": [], "arad": []}, {"cm": 0.0, "arad": 0.0}
+    ok = (info_b == 0) & (info_l == 0)
+    for k, (pr, pl, kind, yt) in enumerate(zip(preds, loop.pred, kinds, ytest)):
+        if not ok[k]:
+            continue
+        pl = pl.cpu().numpy()[:len(pr)]
+        max_diff[kind] = max(max_diff[kind], float(np.max(np.abs(pr - pl))))
+        mae_b, mae_l = np.mean(np.abs(pr - yt)), np.mean(np.abs(pl - yt))
+        rel_mae[kind].append(abs(mae_b - mae_l) / mae_l)
+    mae_stats = {k: {"median": float(np.median(v)), "max": float(np.max(v)), "n": len(v)}
+                 for k, v in rel_mae.items() if v}
+    ns = np.array([len(p.y) for p in probs])
+    entries = float(np.sum(ns.astype(np.float64) ** 2 + nt * ns))
+    narad = sum(k == "arad" for k in kinds)
+    print(json.dumps({
+        "metric": METRIC,
+        "workload": "batched uneven KRR: %d problems (%d ARAD, %d CM Gaussian), n_train "
+                    "log-uniform 100..4000, n_test %d, nmax 23, lambda log-uniform 1e-10..1e-6; "
+                    "CM kernels FP64 inside the persistent launch, ARAD kernels FP32; FP64 "
+                    "Cholesky / solve / prediction" % (a.nprob, narad, a.nprob - narad, nt),
+        "value": a.nprob / (ms * 1e-3), "unit": "KRR solves/s", "ms_per_step": ms,
+        "ms_solve_pass_without_arad_builds": ms_solve,
+        "looped_plain_fp64_ms": ms_loop, "speedup_vs_looped": ms_loop / ms,
+        "kernel_entries_per_s": entries / (ms * 1e-3),
+        "autotune": {k: cfg[k] for k in ("split_threshold", "grid") if k in cfg},
+        "n_multi_cta": len(bk.big), "cholesky_failures": {"batched": int((info_b != 0).sum()),
+                                                          "looped": int((info_l != 0).sum())},
+        "max_abs_pred_diff_vs_looped_fp64": max_diff,
+        "rel_mae_diff_vs_looped_fp64": mae_stats, "clocks": clocks,
+        "gpu_launches_per_step": bk.launches_per_run(),
+        "gpu_launches_looped": loop.launches(), "cuda_graph": True}))
+
+
 def main():
     a = parse()
+    if a.workload == "batched":
+        return run_batched(a)
+    if a.workload == "serving":
+        from fml_b200 import serving
+        return serving.bench(a)
     if a.stages:
         run_stages(a)
     elif a.impl == "reference":

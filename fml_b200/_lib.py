@@ -37,6 +37,7 @@ SIGNATURES = {
     "fmlb_potrs_f64": (_i, [_vp, _ll, _i, _vp, _vp, _vp]),
     "fmlb_syrk_lower_f64": (_i, [_vp, _ll, _i, _vp, _ll, _i, _i, _vp, _vp]),
     "fmlb_add_diagonal_f64": (_i, [_vp, _ll, _i, _d, _vp]),
+    "fmlb_gemv_f64": (_i, [_vp, _ll, _i, _i, _vp, _vp, _vp]),
     "fmlb_kernel_predict_workspace_bytes": (_sz, [_i, _i, _i]),
     "fmlb_kernel_predict_f64": (_i, [_i, _vp, _i, _i, _vp, _i, _i, _i, _dp, _i, _vp, _ll, _vp,
                                      _ll, _vp, _sz, _vp]),

@@ -48,8 +48,8 @@ def _store(data):
 
 def shape_class(problems):
     """Coarse key: problem count and the training-size distribution (log2 bins)."""
-    ns = np.array([p.X_train.shape[0] if hasattr(p, "X_train") else p.K.shape[0]
-                   for p in problems])
+    from .batched import n_train_of
+    ns = np.array([n_train_of(p) for p in problems])
     if len(ns) == 0:
         return "empty"
     hist = np.bincount(np.clip(np.log2(np.maximum(ns, 1)).astype(int), 0, 20), minlength=21)
@@ -63,8 +63,9 @@ def gpu_key():
     return torch.cuda.get_device_name(torch.cuda.current_device()).replace(" ", "_")
 
 
-def batched_config(problems, tune=None):
-    """Cached or default configuration; tunes when FMLB_AUTOTUNE=1 or tune=True."""
+def batched_config(problems, tune=None, batch=None):
+    """Cached or default configuration; tunes when FMLB_AUTOTUNE=1 or tune=True
+    (on ``batch``, an existing BatchedKRR of these problems, when given)."""
     key = "batched_krr|%s|%s" % (shape_class(problems), gpu_key())
     with _LOCK:
         cached = _load().get(key)
@@ -74,29 +75,36 @@ def batched_config(problems, tune=None):
         tune = os.environ.get("FMLB_AUTOTUNE", "0") == "1"
     if not tune:
         return dict(DEFAULT)
-    return tune_batched(problems, key)
+    return tune_batched(problems, key, batch=batch)
 
 
-def tune_batched(problems, key=None, reps=2):
-    """Time every candidate (threshold x grid) and keep the fastest."""
+def tune_batched(problems, key=None, reps=2, batch=None):
+    """Time every candidate (threshold x grid) and keep the fastest.
+
+    The kernel builds that do not depend on the candidate (the ARAD kernels)
+    run once; every candidate then times the solve pass with them restored.
+    """
     from . import _lib
     from .batched import BatchedKRR
     sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    b = batch if batch is not None else BatchedKRR(problems, split_threshold=DEFAULT[
+        "split_threshold"], grid=DEFAULT["grid"])
+    b.keep_kernels()
     results = []
     for thr in CANDIDATE_THRESHOLDS:
         for gm in CANDIDATE_GRID_MULT:
-            b = BatchedKRR(problems, split_threshold=thr, grid=gm * sms)
-            b.run()
+            b.configure(thr, gm * sms)
+            b.run(builds=False)
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
             for _ in range(reps):
-                b.run()
+                b.run(builds=False)
             e1.record()
             torch.cuda.synchronize()
             results.append((e0.elapsed_time(e1) / reps, thr, gm * sms))
-            del b
+    b._pristine = None
     ms, thr, grid = min(results)
     cfg = {"split_threshold": thr, "grid": grid, "ms": ms,
            "candidates": [[r[1], r[2], r[0]] for r in results]}

@@ -3,7 +3,9 @@
 //   * fmlb_kernel_predict_f64: y_s[q] = sum_t k_s(Xq[q], Xt[t]) alpha_s[t] for
 //     every sigma, with the kernel matrix never written to memory (the user-side
 //     prediction K_test @ alpha, fused; reference pattern fget_prediction,
-//     fml/kernels/fkernels.f90:480-539).
+//     fml/kernels/fkernels.f90:480-539);
+//   * fmlb_gemv_f64: y = M x for a stored kernel matrix (the user-side
+//     K_test @ alpha when the test kernel was built separately, e.g. ARAD).
 // The prediction is split over the training set into fixed chunks whose
 // partial sums are reduced in a second pass in a fixed order (deterministic).
 #include <math.h>
@@ -127,8 +129,32 @@ __global__ void reduce_splits_kernel(const double *__restrict__ partial, int nsp
     y[s * ldy + q] = v;
 }
 
+// one warp per row, lanes stride the columns, fixed shuffle tree (deterministic)
+__global__ void gemv_rows_kernel(const double *__restrict__ M, long long ldm, int rows, int cols,
+                                 const double *__restrict__ x, double *__restrict__ y) {
+    const int warp = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (warp >= rows) return;
+    const double *m = M + (size_t)warp * ldm;
+    double v = 0.0;
+    for (int t = lane; t < cols; t += 32) v = fma(m[t], x[t], v);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) y[warp] = v;
+}
+
 }  // namespace
 }  // namespace fmlb
+
+extern "C" int fmlb_gemv_f64(const double *M, long long ldm, int rows, int cols, const double *x,
+                             double *y, void *stream) {
+    using namespace fmlb;
+    FMLB_REQUIRE(rows >= 0 && cols >= 0 && ldm >= cols, "fmlb_gemv_f64: bad sizes");
+    if (rows == 0) return FMLB_OK;
+    FMLB_REQUIRE(M && x && y, "fmlb_gemv_f64: null pointer");
+    gemv_rows_kernel<<<ceil_div(rows, 8), 256, 0, FMLB_STREAM(stream)>>>(M, ldm, rows, cols, x, y);
+    return launch_status("gemv_rows_kernel");
+}
 
 extern "C" int fmlb_add_diagonal_f64(double *A, long long lda, int n, double lam, void *stream) {
     using namespace fmlb;

@@ -178,6 +178,15 @@ def _arad(X1, X2, Z1, Z2, sigmas, width, cut_distance, r_width, c_width, symmetr
     return to_output(K, as_np)
 
 
+def arad_launches(symmetric, precision, amax, nsigma):
+    """Kernel launches of one ``fmlb_arad_kernels`` call (mirrors its host code)."""
+    fast = precision == "fp32" and amax <= 32
+    sets = 1 if symmetric else 2
+    if fast:  # prep, class scan, assign, self per set; class build; fast + gated generic pair
+        return 4 * sets + 1 + 2 * -(-nsigma // 8)
+    return sets + -(-nsigma // 16)
+
+
 def get_atomic_kernels_arad(X1, X2, Z1, Z2, sigmas, width=0.2, cut_distance=6.0, r_width=1.0,
                             c_width=0.5, precision="fp64"):
     """Kernels (nsigma, nm1, nm2) between two sets of ARAD descriptors."""

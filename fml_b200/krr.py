@@ -87,12 +87,22 @@ class KRRPipeline:
         per_sigma = 1 + potrf + potrs
         return 1 + 1 + self.nsig * per_sigma + (2 if self.n_test else 0)
 
+    def run_descriptors(self, X, y_train, stream=None):
+        """Like ``run`` with the descriptor rows (n_mol, d) given instead of molecules."""
+        self.X.copy_(X)
+        return self._solve_predict(y_train, stream)
+
     def run(self, charges, coords, offsets, y_train, stream=None):
         """Device tensors in; predictions (nsigma, n_test) on the device out."""
         s = _lib.stream_handle(stream)
         n, d = self.n_train, self.d
         _lib.call("fmlb_coulomb_matrices", _lib.ptr(charges), _lib.ptr(coords), _lib.ptr(offsets),
                   self.n_mol, self.size, _lib.ptr(self.X), d, None, 0, None, None, s)
+        return self._solve_predict(y_train, stream)
+
+    def _solve_predict(self, y_train, stream=None):
+        s = _lib.stream_handle(stream)
+        n, d = self.n_train, self.d
         fn = "fmlb_gaussian_kernel_f64" if self.kind == 0 else "fmlb_laplacian_kernel_f64"
         _lib.call(fn, _lib.ptr(self.X), n, d, _lib.ptr(self.X), n, d, d, self._sig_ptr, self.nsig,
                   _lib.ptr(self.K), n, n * n, 1, s)

@@ -165,7 +165,12 @@ int fmlb_syrk_lower_f64(double *C, long long ldc, int m, const double *P, long l
  *   fmlb_laplacian_kernel_f64). Replaces the user-side prediction
  *   gaussian_kernel(Xq, Xt, sigma) @ alpha (pattern of fget_prediction,
  *   fml/kernels/fkernels.f90:480-539). nsigma <= 8. Deterministic.
+ * fmlb_gemv_f64: y[r] = sum_c M[r, c] x[c] (row-major M, leading dimension
+ *   ldm); the user-side K_test @ alpha for a test kernel that was stored, e.g.
+ *   the ARAD kernel from fmlb_arad_kernels. Deterministic.
  * ---------------------------------------------------------------------- */
+int fmlb_gemv_f64(const double *M, long long ldm, int rows, int cols, const double *x, double *y,
+                  void *stream);
 int fmlb_add_diagonal_f64(double *A, long long lda, int n, double lambda, void *stream);
 size_t fmlb_kernel_predict_workspace_bytes(int nq, int nt, int nsigma);
 int fmlb_kernel_predict_f64(int kind, const double *Xq, int nq, int ldq, const double *Xt, int nt,

@@ -80,3 +80,46 @@ def test_batched_precomputed_kernels_and_failure_isolation(oracle_mod, problems)
     for p, pred in zip(problems[:4], bk.predictions()[:4]):
         ref, _ = _oracle_predict(oracle_mod, p.X_train, p.y, p.X_test, p.sigma, p.lam)
         np.testing.assert_allclose(pred, ref, rtol=1e-8, atol=1e-8 * np.abs(ref).max())
+
+
+@pytest.fixture(scope="module")
+def arad_set(oracle_mod):
+    b = synthetic.generate(110, nmax=12, seed=21)
+    X = oracle_mod.arad_descriptors(b.charges, b.coords, b.offsets, 12, 1e6)
+    Z = [b.molecule(i)[0] for i in range(b.nmol)]
+    return b, X, Z
+
+
+@pytest.mark.parametrize("precision,rtol", [("fp64", 1e-8), ("fp32", 1e-3)])
+def test_batched_arad_builds_in_pass(oracle_mod, problems, arad_set, precision, rtol):
+    """ARAD kernels built by the pass itself (side streams), one ARAD problem on
+    the multi-CTA path (stored test kernel, GEMV prediction), graph replay."""
+    from fml_b200.batched import AradProblem
+    b, X, Z = arad_set
+    splits = [(slice(0, 30), slice(30, 40), 0.7, 1e-3), (slice(40, 100), slice(100, 110), 2.0,
+                                                         1e-2)]
+    aps, refs = [], []
+    for tr, te, sig, lam in splits:
+        aps.append(AradProblem(X[tr], Z[tr], b.energies[tr], X[te], Z[te], sig, lam,
+                               precision=precision))
+        Ktr = oracle_mod.get_atomic_symmetric_kernels_arad(X[tr], Z[tr], [sig])[0]
+        Kte = oracle_mod.get_atomic_kernels_arad(X[te], X[tr], Z[te], Z[tr], [sig])[0]
+        alpha, info = oracle_mod.cho_solve(Ktr + lam * np.eye(len(Ktr)), b.energies[tr])
+        assert info == 0
+        refs.append(Kte @ alpha)
+    probs = [problems[0], aps[0], problems[2], aps[1]]
+    bk = BatchedKRR(probs, split_threshold=50, grid=0)
+    assert 3 in bk.big and 1 in bk.small
+    g = bk.capture()
+    bk.pred.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    assert (bk.infos() == 0).all()
+    preds = bk.predictions()
+    for k, ref in zip((1, 3), refs):
+        np.testing.assert_allclose(preds[k], ref, rtol=rtol, atol=rtol * np.abs(ref).max())
+    for k in (0, 2):
+        p = probs[k]
+        ref, _ = _oracle_predict(oracle_mod, p.X_train, p.y, p.X_test, p.sigma, p.lam)
+        np.testing.assert_allclose(preds[k], ref, rtol=1e-8, atol=1e-8 * np.abs(ref).max())
+    assert bk.launches_per_run() > 1
