@@ -61,6 +61,11 @@ def parse():
                    help="krr: the large-N KRR step (default, the headline line); batched: "
                         "256 uneven problems in one persistent launch; serving: the request loop")
     p.add_argument("--nprob", type=int, default=256)
+    p.add_argument("--serve-rates", default="200,1000,5000")
+    p.add_argument("--serve-requests", type=int, default=400,
+                   help="requests per arrival rate")
+    p.add_argument("--serve-max-train", type=int, default=32768)
+    p.add_argument("--serve-baseline-seconds", type=float, default=30.0)
     p.add_argument("--arad-nmol", type=int, default=4000,
                    help="molecules of the ARAD stage (the first 3/4 form the symmetric set)")
     return p.parse_args()
@@ -830,13 +835,180 @@ def run_batched(a):
         "gpu_launches_looped": loop.launches(), "cuda_graph": True}))
 
 
+def serving_models(max_train, size=29):
+    """16 models: 8 CM-Gaussian and 8 ARAD, training sizes log-spaced
+    2000..max_train, model m seeded 400+m."""
+    from fml_b200 import synthetic
+    ns = np.unique(np.round(np.geomspace(2000, max_train, 8)).astype(int))
+    ns = np.resize(ns, 8)
+    specs = []
+    for m in range(16):
+        kind = "cm" if m < 8 else "arad"
+        n = int(ns[m % 8])
+        b = synthetic.generate(n, nmax=size, seed=400 + m)
+        if kind == "cm":
+            sigma, lam = (100.0, 400.0, 1600.0)[m % 3], 1e-8
+        else:
+            sigma, lam = (0.5, 1.0, 2.0)[m % 3], 1e-6
+        specs.append((m, kind, b, sigma, lam))
+    return specs
+
+
+def serving_requests(nreq, rate, pool, nmodels, seed, train_sizes, retrain_frac=0.02):
+    """Poisson arrivals at ``rate``; each request names a model uniformly, holds
+    1..512 query molecules (a slice of the pool); ``retrain_frac`` of them append
+    10% of the model's training size."""
+    from fml_b200.serving import Request
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    out = []
+    for i in range(nreq):
+        m = int(rng.integers(0, nmodels))
+        retrain = rng.random() < retrain_frac
+        cnt = max(1, train_sizes[m] // 10) if retrain else int(rng.integers(1, 513))
+        lo = int(rng.integers(0, pool.nmol - cnt))
+        sub = pool.subset(np.arange(lo, lo + cnt))
+        out.append(Request(m, sub.charges, sub.coords, sub.offsets.astype(np.int64),
+                           float(t[i]), y=sub.energies if retrain else None, retrain=retrain))
+        out[-1].truth = sub.energies
+    return out
+
+
+def run_serving(a):
+    """Served KRR: resident models, Poisson request streams, continuous batching,
+    HBM-budget admission, retrains; p50/p99 latency and molecules/s, beside the
+    sequential plain FP64 prediction path."""
+    import ctypes
+
+    import torch
+
+    from fml_b200 import _lib, synthetic
+    from fml_b200.kernels import _ptp_arrays
+    from fml_b200.serving import ARAD_CUT, ARAD_PARAMS, KRRServer, latency_summary
+
+    torch.cuda.set_device(0)
+    size = 29
+    t_setup = time.perf_counter()
+    srv = KRRServer(hbm_budget=150e9, max_inflight=8, max_batch_molecules=1024)
+    specs = serving_models(a.serve_max_train, size)
+    for m, kind, b, sigma, lam in specs:
+        srv.add_model(m, kind, b.charges, b.coords, b.offsets, b.energies, sigma, lam, size=size)
+    setup_s = time.perf_counter() - t_setup
+    train_sizes = [b.nmol for _, _, b, _, _ in specs]
+    pool = synthetic.generate(20000, nmax=size, seed=4000)
+    # warm-up: one request per model
+    warm = serving_requests(16, 1e6, pool, 16, 3999, train_sizes, retrain_frac=0.0)
+    for k, r in enumerate(warm):
+        r.model = k
+    srv.serve(warm, realtime=False)
+    results = {}
+    launches0 = srv.launches
+    sampler = ClockSampler(0)
+    sampler.start()
+    all_reqs = []
+    for rate in [float(x) for x in a.serve_rates.split(",")]:
+        srv.stats.clear()
+        reqs = serving_requests(a.serve_requests, rate, pool, 16, 4000, train_sizes)
+        wall = srv.serve(reqs, realtime=True)
+        preds = [r for r in reqs if not r.retrain]
+        mols = sum(r.nmol for r in preds)
+        rt = [r.done - r.arrival for r in reqs if r.retrain]
+        res = latency_summary(reqs)
+        res.update({"offered_req_per_s": rate, "molecules_per_s": mols / wall,
+                    "requests_per_s": len(preds) / wall, "wall_s": wall,
+                    "arrival_span_s": reqs[-1].arrival,
+                    "batches": srv.stats["batches"], "retrains": len(rt),
+                    "retrain_latency_ms_max": float(max(rt) * 1e3) if rt else None,
+                    "budget_waits": srv.stats["budget_waits"],
+                    "p99_ms_cm": latency_summary([r for r in preds if r.model < 8]).get("p99_ms"),
+                    "p99_ms_arad": latency_summary([r for r in preds
+                                                    if r.model >= 8]).get("p99_ms")})
+        results["%g" % rate] = res
+        all_reqs += preds
+    clocks = sampler.stop()
+    launches = srv.launches - launches0
+    # sequential plain FP64 prediction, one request at a time, on a bounded sample
+    # of the same requests (fresh FP64 copies of each model's alpha / descriptors)
+    lib = _lib.load()
+    P = _lib.ptr
+    st = _lib.stream_handle()
+    sample = serving_requests(64, 200.0, pool, 16, 4001, train_sizes, retrain_frac=0.0)
+    seq_mols, seq_t, mae_srv, mae_seq = 0, 0.0, [], []
+    srv_preds = {}
+    srv.serve([r for r in sample], realtime=False)
+    for r in sample:
+        srv_preds[id(r)] = r.result
+    t_start = time.perf_counter()
+    done = 0
+    for r in sample:
+        if time.perf_counter() - t_start > a.serve_baseline_seconds and done >= 4:
+            break
+        mdl = srv.models[r.model]
+        v = mdl.version
+        nq = r.nmol
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        z = torch.from_numpy(r.charges).cuda()
+        c = torch.from_numpy(np.ascontiguousarray(r.coords)).cuda()
+        o = torch.from_numpy(r.offsets.astype(np.int32)).cuda()
+        out = torch.empty(nq, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        e0.record()
+        if mdl.kind == "cm":
+            X = torch.empty((nq, mdl.d), dtype=torch.float64, device="cuda")
+            _lib.call("fmlb_coulomb_matrices", P(z), P(c), P(o), nq, size, P(X), mdl.d, None, 0,
+                      None, None, st)
+            pw = torch.empty(lib.fmlb_kernel_predict_workspace_bytes(nq, v.n, 1),
+                             dtype=torch.uint8, device="cuda")
+            _lib.call("fmlb_kernel_predict_f64", 0, P(X), nq, mdl.d, P(v.X), v.n, mdl.d, mdl.d,
+                      mdl.sig_ptr, 1, P(v.alpha), v.n, P(out), nq, P(pw), pw.numel(), st)
+        else:
+            X = torch.empty((nq, size, 5, size), dtype=torch.float64, device="cuda")
+            _lib.call("fmlb_arad_descriptors", P(z), P(c), P(o), nq, size, ARAD_CUT, P(X), None,
+                      st)
+            Zs = [r.charges[r.offsets[i]:r.offsets[i + 1]] for i in range(nq)]
+            zp, n1 = _ptp_arrays(Zs, size)
+            Zd = torch.from_numpy(zp).cuda()
+            Nd = torch.from_numpy(n1).cuda()
+            Kt = torch.empty((nq, v.n), dtype=torch.float64, device="cuda")
+            ws = torch.empty(lib.fmlb_arad_workspace_bytes(nq, v.n, size, 0), dtype=torch.uint8,
+                             device="cuda")
+            _lib.call("fmlb_arad_kernels", P(X), P(Zd), P(Nd), nq, P(v.X), P(v.Z), P(v.N), v.n,
+                      size, mdl.sig_ptr, 1, *ARAD_PARAMS, 0, 0, P(Kt), P(ws), ws.numel(), st)
+            _lib.call("fmlb_gemv_f64", P(Kt), v.n, nq, v.n, P(v.alpha), P(out), st)
+        e1.record()
+        torch.cuda.synchronize()
+        seq_t += e0.elapsed_time(e1) * 1e-3
+        seq_mols += nq
+        done += 1
+        ref = out.cpu().numpy()
+        mae_seq.append(float(np.mean(np.abs(ref - r.truth))))
+        mae_srv.append(float(np.mean(np.abs(srv_preds[id(r)] - r.truth))))
+    rel = [abs(x - y) / y for x, y in zip(mae_srv, mae_seq)]
+    best = max(results.values(), key=lambda x: x["molecules_per_s"])
+    print(json.dumps({
+        "metric": METRIC,
+        "workload": "KRR serving: 16 resident models (8 CM-Gaussian, 8 ARAD, FP32 ARAD kernels), "
+                    "n_train log-spaced 2000..%d, molecules of 4..29 atoms, Poisson arrivals, "
+                    "1..512 query molecules per request, 2%% retrains (+10%% data), HBM budget "
+                    "150 GB, %d requests per rate" % (a.serve_max_train, a.serve_requests),
+        "value": best["molecules_per_s"], "unit": "molecules/s", "per_rate": results,
+        "setup_s": setup_s, "resident_gb": srv.resident_bytes() / 1e9,
+        "sequential_plain_fp64": {"molecules_per_s": seq_mols / seq_t if seq_t else None,
+                                  "requests": done, "device_s": seq_t},
+        "speedup_vs_sequential_fp64": best["molecules_per_s"] / (seq_mols / seq_t)
+        if seq_t else None,
+        "rel_mae_diff_vs_sequential_fp64": {"median": float(np.median(rel)),
+                                            "max": float(np.max(rel))} if rel else None,
+        "gpu_launches": launches, "clocks": clocks}))
+
+
 def main():
     a = parse()
     if a.workload == "batched":
         return run_batched(a)
     if a.workload == "serving":
-        from fml_b200 import serving
-        return serving.bench(a)
+        return run_serving(a)
     if a.stages:
         run_stages(a)
     elif a.impl == "reference":

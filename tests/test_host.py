@@ -82,3 +82,17 @@ def test_autotune_cache_roundtrip(tmp_path, monkeypatch):
     key = "batched_krr|%s|%s" % (autotune.shape_class(probs), autotune.gpu_key())
     autotune._store({key: {"split_threshold": 2048, "grid": 296}})
     assert autotune.batched_config(probs)["split_threshold"] == 2048
+
+
+def test_serving_ptp_packing_matches_reference_marshalling():
+    from fml_b200 import synthetic
+    from fml_b200.kernels import _ptp_arrays
+    from fml_b200.serving import _ptp_packed
+    b = synthetic.generate(40, nmax=17, seed=8)
+    Z = [b.molecule(i)[0] for i in range(b.nmol)]
+    ref, nref = _ptp_arrays(Z, 17)
+    got, n = _ptp_packed(b.charges, b.offsets, 17)
+    np.testing.assert_array_equal(got, ref)
+    np.testing.assert_array_equal(n, nref)
+    with pytest.raises(KeyError):
+        _ptp_packed(np.array([1.0, 200.0]), np.array([0, 2]), 4)
