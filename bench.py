@@ -893,6 +893,7 @@ def run_serving(a):
     specs = serving_models(a.serve_max_train, size)
     for m, kind, b, sigma, lam in specs:
         srv.add_model(m, kind, b.charges, b.coords, b.offsets, b.energies, sigma, lam, size=size)
+    srv.reserve()
     setup_s = time.perf_counter() - t_setup
     train_sizes = [b.nmol for _, _, b, _, _ in specs]
     pool = synthetic.generate(20000, nmax=size, seed=4000)

@@ -18,8 +18,8 @@ Design:
   one descriptor launch, one kernel/prediction pass, one device->host copy.
   Batches of different models run on different streams and overlap on the
   device; cheap batches (CM) go to high-priority streams;
-* a batch, or a retrain, is admitted only when the resident models, the
-  batches in flight and its own device memory fit the HBM budget;
+* a batch, or a retrain, is admitted only when the resident models, the slot
+  arenas, the retrains in flight and the memory it adds fit the HBM budget;
 * retrains (``+m`` molecules appended to a model's training set) run on a
   low-priority stream; the model switches to the new version when the
   retrain completes, batches already launched keep the old one;
@@ -81,6 +81,25 @@ def _ptp_packed(charges, offsets, amax):
     return ptp, counts
 
 
+def _aligned(nbytes):
+    return (int(nbytes) + 255) // 256 * 256
+
+
+def _layout_bytes(specs):
+    return sum(_aligned(int(np.prod(shape)) * torch.empty(0, dtype=dt).element_size())
+               for shape, dt in specs)
+
+
+def _carve(buf, specs):
+    """Typed views of a uint8 buffer, one per (shape, dtype), 256-byte aligned."""
+    out, off = [], 0
+    for shape, dt in specs:
+        nb = int(np.prod(shape)) * torch.empty(0, dtype=dt).element_size()
+        out.append(buf[off:off + nb].view(dt).view(shape))
+        off += _aligned(nb)
+    return out
+
+
 class _Version:
     """One trained state of a model (immutable once built)."""
 
@@ -120,16 +139,17 @@ class KRRServer:
             raise ValueError("max_inflight must be >= 1")
         # at least one slot takes ARAD batches
         high_priority_slots = min(high_priority_slots, max_inflight - 1)
-        lo, hi = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream,
-                                                               "priority_range") else (0, -1)
+        pr = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream,
+                                                          "priority_range") else (0, -1)
+        lo, hi = max(pr), min(pr)  # a lower number is a higher priority
         self.slots = []
         for k in range(max_inflight):
             pri = hi if k < high_priority_slots else lo
             st = torch.cuda.Stream(device=self.dev, priority=pri)
             self.slots.append({"stream": st, "high": k < high_priority_slots, "busy": None,
-                               "host": None})
+                               "dev": None, "pin": None})
         self.retrain_stream = torch.cuda.Stream(device=self.dev, priority=lo)
-        self.inflight_bytes = 0
+        self.inflight_bytes = 0  # retrains in flight
         self.launches = 0
         self.stats = collections.Counter()
 
@@ -141,20 +161,52 @@ class KRRServer:
                 total += m.version.nbytes()
         return total
 
-    def _fits(self, nbytes):
-        return self.resident_bytes() + self.inflight_bytes + nbytes <= self.budget
+    def arena_bytes(self):
+        return sum(sl["dev"].numel() for sl in self.slots if sl["dev"] is not None)
 
-    def _predict_bytes(self, m, nq, atoms):
-        v = m.version
-        host_in = atoms * 4 * 8 + (nq + 1) * 4
-        if m.kind == "cm":
-            lib = _lib.load()
-            return host_in + nq * m.d * 8 + nq * 8 + \
-                lib.fmlb_kernel_predict_workspace_bytes(nq, v.n, 1)
+    def _fits(self, nbytes):
+        return self.resident_bytes() + self.arena_bytes() + self.inflight_bytes + nbytes <= \
+            self.budget
+
+    def _predict_specs(self, m, nq, atoms):
+        """(pinned host, device) layouts of one prediction batch."""
         lib = _lib.load()
-        a = m.size
-        return host_in + nq * a * 5 * a * 8 + nq * a * 2 * 8 + nq * 4 + nq * v.n * 8 + nq * 8 + \
-            lib.fmlb_arad_workspace_bytes(nq, v.n, a, 0)
+        f64, i32, u8 = torch.float64, torch.int32, torch.uint8
+        n, a = m.version.n, m.size
+        pin = [((atoms,), f64), ((atoms, 3), f64), ((nq + 1,), i32), ((nq,), f64)]
+        dev = [((atoms,), f64), ((atoms, 3), f64), ((nq + 1,), i32), ((nq,), f64)]
+        if m.kind == "cm":
+            dev += [((nq, m.d), f64),
+                    ((lib.fmlb_kernel_predict_workspace_bytes(nq, n, 1),), u8)]
+        else:
+            pin += [((nq, a, 2), f64), ((nq,), i32)]
+            dev += [((nq, a, 5, a), f64), ((nq, a, 2), f64), ((nq,), i32), ((nq, n), f64),
+                    ((lib.fmlb_arad_workspace_bytes(nq, n, a, 0),), u8)]
+        return pin, dev
+
+    def reserve(self):
+        """Size every slot's arenas for a full batch (``max_batch_molecules`` of
+        the largest molecules) of any resident model the slot may serve."""
+        for slot in self.slots:
+            dev = pin = 0
+            for m in self.models.values():
+                if slot["high"] and m.kind == "arad":
+                    continue
+                p, d = self._predict_specs(m, self.max_batch, self.max_batch * m.size)
+                dev, pin = max(dev, _layout_bytes(d)), max(pin, _layout_bytes(p))
+            extra = dev - (slot["dev"].numel() if slot["dev"] is not None else 0)
+            if extra > 0:
+                if not self._fits(extra):
+                    raise MemoryError("slot arenas do not fit the HBM budget")
+                slot["dev"] = None
+                slot["dev"] = torch.empty(dev, dtype=torch.uint8, device=self.dev)
+            if slot["pin"] is None or slot["pin"].numel() < pin:
+                slot["pin"] = torch.empty(pin, dtype=torch.uint8, pin_memory=True)
+
+    def _slot_growth(self, slot, m, nq, atoms):
+        need = _layout_bytes(self._predict_specs(m, nq, atoms)[1])
+        have = slot["dev"].numel() if slot["dev"] is not None else 0
+        return max(0, need - have)
 
     def _train_bytes(self, m, n_new, m_add):
         lib = _lib.load()
@@ -320,51 +372,67 @@ class KRRServer:
         counts = np.concatenate([np.diff(r.offsets) for r in reqs])
         offsets = np.zeros(len(counts) + 1, np.int64)
         np.cumsum(counts, out=offsets[1:])
-        nq = len(counts)
+        nq, atoms = len(counts), len(charges)
+        if counts.max() > m.size:
+            raise ValueError("a molecule has %d atoms, more than the model size %d"
+                             % (int(counts.max()), m.size))
         v = m.version
-        nbytes = self._predict_bytes(m, nq, len(charges))
-        dev_in, pins = self._upload(charges, coords, offsets, stream)
-        D = self._describe(m, dev_in, nq, charges, offsets, stream)
+        pin_specs, dev_specs = self._predict_specs(m, nq, atoms)
+        # per-slot arenas, grown when a batch needs more (never inside the steady state)
+        need_dev, need_pin = _layout_bytes(dev_specs), _layout_bytes(pin_specs)
+        if slot["dev"] is None or slot["dev"].numel() < need_dev:
+            slot["dev"] = None
+            slot["dev"] = torch.empty(need_dev, dtype=torch.uint8, device=self.dev)
+        if slot["pin"] is None or slot["pin"].numel() < need_pin:
+            slot["pin"] = torch.empty(need_pin, dtype=torch.uint8, pin_memory=True)
+        hp = _carve(slot["pin"], pin_specs)
+        dv = _carve(slot["dev"], dev_specs)
+        hp[0].numpy()[:] = charges
+        hp[1].numpy()[:] = coords
+        hp[2].numpy()[:] = offsets
         P = _lib.ptr
         st = _lib.stream_handle(stream)
-        keep = [dev_in, pins, D]
+        a = m.size
         with torch.cuda.stream(stream):
-            pred = torch.empty(max(nq, 1), dtype=torch.float64, device=self.dev)
+            for k in range(3):
+                dv[k].copy_(hp[k], non_blocking=True)
+            zd, rd, od, pred = dv[:4]
             if m.kind == "cm":
-                lib = _lib.load()
-                pw = torch.empty(lib.fmlb_kernel_predict_workspace_bytes(nq, v.n, 1),
-                                 dtype=torch.uint8, device=self.dev)
-                _lib.call("fmlb_kernel_predict_f64", 0, P(D["X"]), nq, m.d, P(v.X), v.n, m.d,
-                          m.d, m.sig_ptr, 1, P(v.alpha), v.n, P(pred), nq, P(pw), pw.numel(), st)
-                self.launches += 2
-                keep.append(pw)
+                X, pw = dv[4:6]
+                _lib.call("fmlb_coulomb_matrices", P(zd), P(rd), P(od), nq, a, P(X), m.d, None,
+                          0, None, None, st)
+                _lib.call("fmlb_kernel_predict_f64", 0, P(X), nq, m.d, P(v.X), v.n, m.d, m.d,
+                          m.sig_ptr, 1, P(v.alpha), v.n, P(pred), nq, P(pw), pw.numel(), st)
+                self.launches += 3
             else:
-                Kt = torch.empty((nq, v.n), dtype=torch.float64, device=self.dev)
-                keep.append(self._arad_call(m, D, {"X": v.X, "Z": v.Z, "N": v.N}, Kt, stream,
-                                            False))
+                X, Z, N, Kt, ws = dv[4:9]
+                ptp, cnt = _ptp_packed(charges, offsets, a)
+                hp[4].numpy()[:] = ptp
+                hp[5].numpy()[:] = cnt
+                Z.copy_(hp[4], non_blocking=True)
+                N.copy_(hp[5], non_blocking=True)
+                _lib.call("fmlb_arad_descriptors", P(zd), P(rd), P(od), nq, a, ARAD_CUT, P(X),
+                          None, st)
+                _lib.call("fmlb_arad_kernels", P(X), P(Z), P(N), nq, P(v.X), P(v.Z), P(v.N), v.n,
+                          a, m.sig_ptr, 1, *ARAD_PARAMS, 0, PRECISIONS[m.precision], P(Kt), P(ws),
+                          ws.numel(), st)
                 _lib.call("fmlb_gemv_f64", P(Kt), v.n, nq, v.n, P(v.alpha), P(pred), st)
-                self.launches += 1
-                keep.append(Kt)
-            host = torch.empty(max(nq, 1), dtype=torch.float64, pin_memory=True)
-            host.copy_(pred, non_blocking=True)
+                self.launches += 2 + arad_launches(False, m.precision, a, 1)
+            hp[3].copy_(pred, non_blocking=True)
             ev = torch.cuda.Event()
             ev.record(stream)
-        keep += [pred, v]
-        self.inflight_bytes += nbytes
-        slot["busy"] = {"reqs": reqs, "event": ev, "host": host, "keep": keep, "bytes": nbytes,
-                        "counts": counts}
+        slot["busy"] = {"reqs": reqs, "event": ev, "out": hp[3], "version": v}
         self.stats["batches"] += 1
         self.stats["batched_requests"] += len(reqs)
 
     def _finish_predict(self, slot, now):
         b = slot["busy"]
-        out = b["host"].numpy()
+        out = b["out"].numpy()
         k = 0
         for r in b["reqs"]:
             r.result = out[k:k + r.nmol].copy()
             r.done = now
             k += r.nmol
-        self.inflight_bytes -= b["bytes"]
         slot["busy"] = None
 
     # ------------------------------------------------------------------ retraining
@@ -462,25 +530,26 @@ class KRRServer:
                 free.sort(key=lambda s: not s["high"])
                 if not free:
                     continue
+                slot = free[0]
                 take, mols, atoms = [], 0, 0
                 while q and q[0].nmol and (not take or mols + q[0].nmol <= self.max_batch):
                     mols += q[0].nmol
                     atoms += len(q[0].charges)
                     take.append(q.popleft())
-                while take and not self._fits(self._predict_bytes(m, mols, atoms)):
+                while take and not self._fits(self._slot_growth(slot, m, mols, atoms)):
                     r = take.pop()  # shrink the batch until it fits
                     q.appendleft(r)
                     mols -= r.nmol
                     atoms -= len(r.charges)
                 if not take:
-                    if self.inflight_bytes == 0:
+                    if self.inflight_bytes == 0 and all(sl["busy"] is None for sl in self.slots):
                         raise MemoryError("a request for model %r needs more device memory than "
                                           "the HBM budget leaves" % (mid,))
                     self.stats["budget_waits"] += 1
                     continue
                 for r in take:
                     r.admitted = now
-                self._launch_predict(free[0], m, take)
+                self._launch_predict(slot, m, take)
                 progressed = True
             # retrains: one at a time per model, when the budget allows
             for m in self.models.values():
@@ -490,7 +559,8 @@ class KRRServer:
                     if self._fits(need):
                         self._launch_retrain(m, now)
                         progressed = True
-                    elif self.inflight_bytes == 0:
+                    elif self.inflight_bytes == 0 and all(sl["busy"] is None
+                                                          for sl in self.slots):
                         raise MemoryError("retraining model %r needs more device memory than "
                                           "the HBM budget leaves" % (m.mid,))
             if not progressed and nxt == len(reqs) and self.inflight_bytes == 0 and \

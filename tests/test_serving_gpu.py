@@ -44,6 +44,8 @@ def server():
         srv.add_model(mid, kind, b.charges, b.coords, b.offsets, b.energies, sig, lam,
                       size=SIZE, precision=prec)
         train[mid] = (b, sig, lam)
+    srv.reserve()
+    assert srv.arena_bytes() > 0
     return srv, train
 
 
