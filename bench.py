@@ -410,7 +410,6 @@ def _time(torch, fn, reps=3, warmup=1):
 def run_stages(a):
     import torch
 
-    import oracle
     from fml_b200 import _lib, synthetic
     from fml_b200.kernels import _ptp_arrays
 
@@ -564,14 +563,14 @@ def run_stages(a):
 def run_arad_stage(a, torch, lib, st, P):
     """ARAD kernels: symmetric set of 3/4 of --arad-nmol molecules (3000 of the
     4000-molecule configuration), size 23, descriptor cut 1e6, 5 sigmas."""
-    import oracle
+    import fml_b200
     from fml_b200 import _lib, synthetic
     from fml_b200.kernels import _ptp_arrays
 
     out = []
     dev = torch.device("cuda", 0)
     ba = synthetic.generate(a.arad_nmol, nmax=23, seed=1)
-    Xa = oracle.arad_descriptors(ba.charges, ba.coords, ba.offsets, 23, 1e6)
+    Xa = fml_b200.generate_arad_descriptors(ba.charges, ba.coords, ba.offsets, size=23, cut=1e6)
     Z = [ba.molecule(i)[0] for i in range(ba.nmol)]
     ntr = (3 * a.arad_nmol) // 4
     asig = [0.1, 0.5, 1.0, 2.0, 5.0]
