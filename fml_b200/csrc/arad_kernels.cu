@@ -274,7 +274,7 @@ arad_pair_kernel(const double *__restrict__ X1, const double *__restrict__ Z1,
 // sigma. Self terms come from the same code (J = I), so l2 cancels exactly for
 // identical environments.
 // ---------------------------------------------------------------------------
-constexpr int FC_BM = 8, FC_WARPS = 4, FC_MAXREC = 1024, FC_MAXA = 32, FC_MAXSIG = 8;
+constexpr int FC_BM = 8, FC_WARPS = 8, FC_MAXREC = 1024, FC_MAXA = 32, FC_MAXSIG = 8;
 constexpr int FC_SST = FC_MAXC + 1;
 
 __device__ __forceinline__ int ptp_pos(double row, double col) {
@@ -350,17 +350,36 @@ __global__ void arad_class_assign_kernel(const double *__restrict__ X, const dou
     }
 }
 
+// Paired path (at most FC_PC element classes): the records of J are stored two
+// at a time, (r0, r1, xi0, xi1) and (xc0, xc1, xs0, xs1), so every lane
+// evaluates two neighbour pairs per step with packed FP32x2 arithmetic
+// (FADD2 / FMUL2 / FFMA2) and fetches both stoichiometric factors with one
+// load from a per-class pair table. An atom with an odd neighbour count gets
+// a padding record (r = 1e18, xi = 0) whose window test and exponential are 0.
+constexpr int FC_PC = 8;
+constexpr int FC_PTS = FC_PC * FC_PC + 1;  // pair-table row stride (float2): conflict-free rows
+
 struct FastSmem {
     float4 recI[FC_MAXREC];      // molecule I, dense by atom, 32 records per pass
-    int metaI[FC_MAXREC];        // atom | seg_start << 8 | active << 24 | tail << 25
+    int metaI[FC_MAXREC];        // atom | seg_start << 8 | cls << 16 | active << 24 | tail << 25
     float selfI[FC_MAXA];
     int aclsI[FC_MAXA];
-    float4 recJ[FC_MAXREC];      // molecule J, dense by atom
-    signed char clsJ[FC_MAXREC]; // element class of each record of J
-    int offJ[FC_MAXA + 1];
+    union {
+        struct {
+            float4 rec[FC_MAXREC];       // molecule J, dense by atom
+            signed char cls[FC_MAXREC];  // element class of each record of J
+        } s;
+        struct {
+            float4 a[FC_MAXREC / 2];     // (r0, r1, xi0, xi1) per record pair
+            float4 b[FC_MAXREC / 2];     // (xc0, xc1, xs0, xs1)
+            int k[FC_MAXREC / 2];        // cls0 * FC_PC + cls1: column of the pair table
+        } p;
+    } J;
+    int offJ[FC_MAXA + 1];       // record offsets (scalar path) or pair offsets (paired path)
     float selfJ[FC_MAXA];
     int aclsJ[FC_MAXA];
     float stoch[FC_MAXC * FC_SST];  // row stride 17: lanes of different classes hit distinct banks
+    float2 pt[FC_PC * FC_PTS];   // pt[c1][ca * FC_PC + cb] = (stoch(c1, ca), stoch(c1, cb))
     float S[FC_MAXA * FC_MAXA];  // S(i1, j1) of the current molecule pair
     float red[FC_WARPS][FC_MAXSIG];
     int npassI, nI, nJ;
@@ -437,14 +456,105 @@ __device__ void fast_load_J(FastSmem &sm, const SetWs &w, int J, int amax, int n
         if (k < sm.offJ[a + 1] - sm.offJ[a]) {
             const int d = sm.offJ[a] + k;
             const size_t src = ((size_t)J * amax + a) * amax + k;
-            sm.recJ[d] = w.pk[src];
-            sm.clsJ[d] = w.cls[src];
+            sm.J.s.rec[d] = w.pk[src];
+            sm.J.s.cls[d] = w.cls[src];
         }
     }
     for (int a = threadIdx.x; a < nJ; a += blockDim.x) {
         sm.selfJ[a] = use_self ? w.selff[(size_t)J * amax + a] : 0.0f;
         sm.aclsJ[a] = w.acls[(size_t)J * amax + a];
     }
+}
+
+// Molecule J in record pairs (paired path). Whole CTA; the caller synchronises
+// before the records are read.
+__device__ void fast_load_J_pairs(FastSmem &sm, const SetWs &w, int J, int amax, int nJ,
+                                  bool use_self) {
+    if (threadIdx.x < 32) {  // exclusive prefix of the padded pair counts (nJ <= 32)
+        const int a = threadIdx.x;
+        const int np = a < nJ ? (w.nnb[(size_t)J * amax + a] + 1) >> 1 : 0;
+        int incl = np;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int o = __shfl_up_sync(0xffffffffu, incl, d);
+            if (a >= d) incl += o;
+        }
+        sm.offJ[a] = incl - np;
+        if (a == 31) {
+            sm.offJ[32] = incl;
+            sm.nJ = nJ;
+        }
+    }
+    __syncthreads();
+    const int hp = (amax + 1) >> 1;
+    for (int t = threadIdx.x; t < nJ * hp; t += blockDim.x) {
+        const int a = t / hp, q = t - a * hp;
+        const int beg = sm.offJ[a];
+        if (q < sm.offJ[a + 1] - beg) {
+            const size_t base = (size_t)J * amax + a;
+            const int cnt = w.nnb[base];
+            const size_t src = base * amax + 2 * q;
+            const float4 r0 = w.pk[src];
+            const int c0 = w.cls[src];
+            float4 r1 = make_float4(1.0e18f, 0.0f, 0.0f, 0.0f);
+            int c1 = 0;
+            if (2 * q + 1 < cnt) {
+                r1 = w.pk[src + 1];
+                c1 = w.cls[src + 1];
+            }
+            sm.J.p.a[beg + q] = make_float4(r0.x, r1.x, r0.y, r1.y);
+            sm.J.p.b[beg + q] = make_float4(r0.z, r1.z, r0.w, r1.w);
+            sm.J.p.k[beg + q] = c0 * FC_PC + c1;
+        }
+    }
+    for (int a = threadIdx.x; a < nJ; a += blockDim.x) {
+        sm.selfJ[a] = use_self ? w.selff[(size_t)J * amax + a] : 0.0f;
+        sm.aclsJ[a] = w.acls[(size_t)J * amax + a];
+    }
+}
+
+__device__ __forceinline__ float set_lt(float a, float b) {  // 1.0f if a < b, else 0.0f
+    float r;
+    asm("set.lt.f32.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+
+// Paired work item: as fast_item, two records of j1 per step. Every term is
+// computed with the same operations as in fast_item; the even and odd
+// records accumulate separately and are added at the end.
+__device__ __forceinline__ void fast_item_pairs(FastSmem &sm, int p, int j1, float maxg2s) {
+    const int lane = threadIdx.x & 31;
+    const float4 u = sm.recI[p * 32 + lane];
+    const int meta = sm.metaI[p * 32 + lane];
+    const float2 *ptrow = sm.pt + ((meta >> 16) & 0xff) * FC_PTS;
+    const float2 nux = make_float2(-u.x, -u.x), uy = make_float2(u.y, u.y),
+                 uz = make_float2(u.z, u.z), uw = make_float2(u.w, u.w);
+    const int beg = sm.offJ[j1], end = sm.offJ[j1 + 1];
+    float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll 4
+    for (int m = beg; m < end; ++m) {
+        const float4 A = sm.J.p.a[m];
+        const float4 B = sm.J.p.b[m];
+        const float2 st = ptrow[sm.J.p.k[m]];
+        const float2 dr = __fadd2_rn(make_float2(A.x, A.y), nux);
+        const float2 t = __fmul2_rn(dr, dr);
+        float e0, e1;
+        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e0) : "f"(-t.x));
+        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e1) : "f"(-t.y));
+        const float2 g = __ffma2_rn(make_float2(B.z, B.w), uw,
+                                    __ffma2_rn(make_float2(B.x, B.y), uz,
+                                               __fmul2_rn(make_float2(A.z, A.w), uy)));
+        const float2 win = make_float2(set_lt(t.x, maxg2s), set_lt(t.y, maxg2s));
+        const float2 eg = __fmul2_rn(__fmul2_rn(make_float2(e0, e1), st), win);
+        acc = __ffma2_rn(eg, g, acc);
+    }
+    const int seg = (meta >> 8) & 0xff;
+    float v = acc.x + acc.y;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const float o = __shfl_up_sync(0xffffffffu, v, d);
+        if (lane - d >= seg) v += o;
+    }
+    if ((meta >> 25) & 1) atomicAdd(&sm.S[(meta & 0xff) * FC_MAXA + j1], v);
 }
 
 // Work item (pass p, atom j1): the segment sums of the pass against j1 are
@@ -460,13 +570,13 @@ __device__ __forceinline__ void fast_item(FastSmem &sm, int p, int j1, float max
     float acc = 0.0f;
 #pragma unroll 4
     for (int m2 = beg; m2 < end; ++m2) {
-        const float4 q = sm.recJ[m2];
+        const float4 q = sm.J.s.rec[m2];
         const float dr = q.x - u.x;
         const float t = dr * dr;
         float e;
         asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(-t));
         const float g = fmaf(u.w, q.w, fmaf(u.z, q.z, u.y * q.y));
-        const float eg = e * strow[sm.clsJ[m2]];
+        const float eg = e * strow[sm.J.s.cls[m2]];
         if (t < maxg2s) acc = fmaf(eg, g, acc);
     }
     const int seg = (meta >> 8) & 0xff;
@@ -480,13 +590,32 @@ __device__ __forceinline__ void fast_item(FastSmem &sm, int p, int j1, float max
 }
 
 // All work items of one molecule pair, S cleared first. Whole CTA.
-__device__ __forceinline__ void fast_pair_sums(FastSmem &sm, int nJ, float maxg2s) {
+__device__ __forceinline__ void fast_pair_sums(FastSmem &sm, int nJ, float maxg2s, bool paired) {
     for (int t = threadIdx.x; t < FC_MAXA * FC_MAXA; t += blockDim.x) sm.S[t] = 0.0f;
     __syncthreads();
     const int warp = threadIdx.x >> 5;
     const int items = sm.npassI * nJ;
-    for (int it = warp; it < items; it += FC_WARPS) fast_item(sm, it / nJ, it % nJ, maxg2s);
+    if (paired) {
+        for (int it = warp; it < items; it += FC_WARPS)
+            fast_item_pairs(sm, it / nJ, it % nJ, maxg2s);
+    } else {
+        for (int it = warp; it < items; it += FC_WARPS) fast_item(sm, it / nJ, it % nJ, maxg2s);
+    }
     __syncthreads();
+}
+
+// Class tables of the CTA: the stoichiometric table (row stride FC_SST) and,
+// for the paired path, the pair table.
+__device__ __forceinline__ void fast_load_tables(FastSmem &sm, const ClassInfo *ci, bool paired) {
+    for (int t = threadIdx.x; t < FC_MAXC * FC_MAXC; t += blockDim.x)
+        sm.stoch[(t / FC_MAXC) * FC_SST + t % FC_MAXC] = ci->stoch[t];
+    if (paired)
+        for (int t = threadIdx.x; t < FC_PC * FC_PC * FC_PC; t += blockDim.x) {
+            const int c1 = t / (FC_PC * FC_PC), k = t % (FC_PC * FC_PC);
+            const int ca = k / FC_PC, cb = k % FC_PC;
+            sm.pt[c1 * FC_PTS + k] =
+                make_float2(ci->stoch[c1 * FC_MAXC + ca], ci->stoch[c1 * FC_MAXC + cb]);
+        }
 }
 
 __device__ __forceinline__ void pair_block(long long t, int symmetric, int nbj, int &bi, int &bj) {
@@ -507,18 +636,22 @@ __device__ __forceinline__ void pair_block(long long t, int symmetric, int nbj, 
 __global__ void __launch_bounds__(FC_WARPS * 32)
 arad_fast_self_kernel(SetWs w, const int *__restrict__ N, int nm, int amax, AradParams P,
                       const ClassInfo *ci) {
-    __shared__ FastSmem sm;
+    extern __shared__ __align__(16) unsigned char fc_smem_raw[];
+    FastSmem &sm = *reinterpret_cast<FastSmem *>(fc_smem_raw);
     if (ci->flag) return;
     const int I = blockIdx.x;
     if (I >= nm) return;
-    for (int t = threadIdx.x; t < FC_MAXC * FC_MAXC; t += blockDim.x)
-        sm.stoch[(t / FC_MAXC) * FC_SST + t % FC_MAXC] = ci->stoch[t];
+    const bool paired = ci->ncls <= FC_PC;
+    fast_load_tables(sm, ci, paired);
     const int nI = min(max(N[I], 0), amax);
     fast_load_I(sm, w, I, amax, nI, false);
-    fast_load_J(sm, w, I, amax, nI, false);
+    if (paired)
+        fast_load_J_pairs(sm, w, I, amax, nI, false);
+    else
+        fast_load_J(sm, w, I, amax, nI, false);
     __syncthreads();
     const float maxg2s = (float)(P.maxg2 * fp32_scale(P) * fp32_scale(P));
-    fast_pair_sums(sm, nI, maxg2s);
+    fast_pair_sums(sm, nI, maxg2s, paired);
     for (int a = threadIdx.x; a < nI; a += blockDim.x)
         w.selff[(size_t)I * amax + a] = sm.S[a * FC_MAXA + a];
 }
@@ -528,13 +661,14 @@ arad_fast_pair_kernel(SetWs w1, const int *__restrict__ N1, int nm1, SetWs w2,
                       const int *__restrict__ N2, int nm2, int amax, AradParams P,
                       const ClassInfo *ci, SigmaTable sig, int nsig, int symmetric,
                       double *__restrict__ K) {
-    __shared__ FastSmem sm;
+    extern __shared__ __align__(16) unsigned char fc_smem_raw[];
+    FastSmem &sm = *reinterpret_cast<FastSmem *>(fc_smem_raw);
     if (ci->flag) return;
     const int nbj = (nm2 + FC_BM - 1) / FC_BM;
     int bi, bj;
     pair_block(blockIdx.x, symmetric, nbj, bi, bj);
-    for (int t = threadIdx.x; t < FC_MAXC * FC_MAXC; t += blockDim.x)
-        sm.stoch[(t / FC_MAXC) * FC_SST + t % FC_MAXC] = ci->stoch[t];
+    const bool paired = ci->ncls <= FC_PC;
+    fast_load_tables(sm, ci, paired);
     const float maxg2s = (float)(P.maxg2 * fp32_scale(P) * fp32_scale(P));
     const float eps = 5.0e-12f;
     float sc[FC_MAXSIG];
@@ -554,9 +688,12 @@ arad_fast_pair_kernel(SetWs w1, const int *__restrict__ N1, int nm1, SetWs w2,
             if (symmetric && J < I) continue;
             __syncthreads();
             const int nJ = min(max(N2[J], 0), amax);
-            fast_load_J(sm, w2, J, amax, nJ, true);
+            if (paired)
+                fast_load_J_pairs(sm, w2, J, amax, nJ, true);
+            else
+                fast_load_J(sm, w2, J, amax, nJ, true);
             __syncthreads();
-            fast_pair_sums(sm, nJ, maxg2s);
+            fast_pair_sums(sm, nJ, maxg2s, paired);
             // phase 2: l2 and the kernel exponentials of every atom pair
             float kacc[FC_MAXSIG];
 #pragma unroll
@@ -591,6 +728,25 @@ arad_fast_pair_kernel(SetWs w1, const int *__restrict__ N1, int nm1, SetWs w2,
             }
         }
     }
+}
+
+// The fast kernels' shared memory is dynamic (above the 48 KB static limit);
+// the attribute is set once per device.
+int fast_smem_attrs() {
+    static int attr_dev = -1;
+    int dev = 0;
+    FMLB_TRY(cuda_status(cudaGetDevice(&dev), "fmlb_arad_kernels: cudaGetDevice"));
+    if (attr_dev == dev) return FMLB_OK;
+    FMLB_TRY(cuda_status(cudaFuncSetAttribute(arad_fast_self_kernel,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)sizeof(FastSmem)),
+                         "fmlb_arad_kernels: self kernel smem attribute"));
+    FMLB_TRY(cuda_status(cudaFuncSetAttribute(arad_fast_pair_kernel,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)sizeof(FastSmem)),
+                         "fmlb_arad_kernels: pair kernel smem attribute"));
+    attr_dev = dev;
+    return FMLB_OK;
 }
 
 }  // namespace
@@ -665,8 +821,12 @@ extern "C" int fmlb_arad_kernels(const double *X1, const double *Z1, const int *
         if (!symmetric)
             arad_class_assign_kernel<<<ceil_div((long long)nm2 * amax, tpb), tpb, 0, st>>>(
                 X2, Z2, N2, nm2, amax, ci, w2);
-        arad_fast_self_kernel<<<nm1, FC_WARPS * 32, 0, st>>>(w1, N1, nm1, amax, P, ci);
-        if (!symmetric) arad_fast_self_kernel<<<nm2, FC_WARPS * 32, 0, st>>>(w2, N2, nm2, amax, P, ci);
+        FMLB_TRY(fast_smem_attrs());
+        arad_fast_self_kernel<<<nm1, FC_WARPS * 32, sizeof(FastSmem), st>>>(w1, N1, nm1, amax, P,
+                                                                            ci);
+        if (!symmetric)
+            arad_fast_self_kernel<<<nm2, FC_WARPS * 32, sizeof(FastSmem), st>>>(w2, N2, nm2, amax,
+                                                                                P, ci);
         FMLB_TRY(launch_status("arad fast-path preparation"));
     }
     const long long npairs = symmetric ? (long long)nm1 * (nm1 + 1) / 2 : (long long)nm1 * nm2;
@@ -686,7 +846,7 @@ extern "C" int fmlb_arad_kernels(const double *X1, const double *Z1, const int *
                 const long long nbi = ceil_div(nm1, FC_BM), nbj = ceil_div(nm2, FC_BM);
                 const long long nblk = symmetric ? nbi * (nbi + 1) / 2 : nbi * nbj;
                 FMLB_REQUIRE(nblk < (1LL << 31), "fmlb_arad_kernels: too many molecule blocks");
-                arad_fast_pair_kernel<<<(unsigned)nblk, FC_WARPS * 32, 0, st>>>(
+                arad_fast_pair_kernel<<<(unsigned)nblk, FC_WARPS * 32, sizeof(FastSmem), st>>>(
                     w1, N1, nm1, w2, N2, nm2, amax, P, ci, sig, ns, symmetric, Ks);
                 FMLB_TRY(launch_status("arad_fast_pair_kernel"));
             }
