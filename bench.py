@@ -326,6 +326,25 @@ def run_ours(a):
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(nsig * a.ntest * 8),
                "ms_per_step": ems, "api": "fml_b200.krr.KRRPipeline.run on host-pinned inputs"}
 
+    # relative residual ||y - (K + lambda I) alpha|| / ||y|| of every sigma, in FP64,
+    # with K rebuilt after the timed region (the factorisation overwrote it)
+    resid = {}
+    n_tr, d_cm = a.ntrain, pipe.d
+    Kr = torch.empty((n_tr, n_tr), dtype=torch.float64, device=dev)
+    Ka = torch.empty(n_tr, dtype=torch.float64, device=dev)
+    hs = _lib.stream_handle()
+    for k, s in enumerate(sigmas):
+        sp, keep = _lib.host_doubles([s])
+        _lib.call("fmlb_gaussian_kernel_f64", _lib.ptr(pipe.X), n_tr, d_cm, _lib.ptr(pipe.X), n_tr,
+                  d_cm, d_cm, sp, 1, _lib.ptr(Kr), n_tr, n_tr * n_tr, 1, hs)
+        _lib.call("fmlb_gemv_f64", _lib.ptr(Kr), n_tr, n_tr, n_tr, _lib.ptr(pipe.alpha[k]),
+                  _lib.ptr(Ka), hs)
+        alpha_h = pipe.alpha[k].cpu().numpy()
+        rvec = b.energies[:n_tr] - Ka.cpu().numpy() - a.lam * alpha_h
+        resid[str(s)] = float(np.linalg.norm(rvec) / np.linalg.norm(b.energies[:n_tr]))
+        del keep
+    del Kr, Ka
+
     # dominant kernel: FP64 trailing update of the factorisation
     flops, syrk_ms, nl = measure_syrk(pipe, torch, _lib.call, _lib.ptr, _lib.stream_handle())
     peak = measure_dgemm_peak(torch)
@@ -337,7 +356,8 @@ def run_ours(a):
             traffic = json.load(open(tpath)).get("bytes_per_launch")
         except (OSError, ValueError):
             traffic = None
-    roofline = {"bound": "fp64", "kernel": "syrk_dmma_kernel (FP64 trailing update)",
+    roofline = {"bound": "tensor", "pipe": "FP64 DMMA (mma.sync m8n8k4 f64)",
+                "kernel": "syrk_dmma_kernel (FP64 trailing update)",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json "
                                "holds no FP64 figure)",
@@ -370,6 +390,7 @@ def run_ours(a):
                              % (a.ntrain ** 2 * 8 / 1e9)},
             "solves_per_s": world * nsig / (ms * 1e-3),
             "mae": mae, "potrf_info": [int(v) for v in info],
+            "relative_residual": resid,
             "clocks": clocks, "e2e": e2e, "gpu_launches": pipe.launches_per_run() * a.steps,
             "roofline": roofline, "cpu_baseline": cpu,
         }))
@@ -389,6 +410,16 @@ def _measured_peaks():
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except (OSError, ValueError):
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def _max_abs_diff(torch, A, B):
+    """max |A - B| over (nsigma, n, n) stacks, one row block at a time (measurement only)."""
+    worst = 0.0
+    for k in range(A.shape[0]):
+        for r0 in range(0, A.shape[1], 2048):
+            d = (A[k, r0:r0 + 2048].double() - B[k, r0:r0 + 2048].double()).abs().max()
+            worst = max(worst, float(d.item()))
+    return worst
 
 
 def _time(torch, fn, reps=3, warmup=1):
@@ -468,7 +499,6 @@ def run_stages(a):
           "ms": ms, "entries_per_s": n * n * ns / (ms * 1e-3), "bound": "fp64",
           "achieved_tflops": fl / ms / 1e9, "peak_tflops": dgemm,
           "frac": fl / ms / 1e9 / dgemm, "peak_source": "cuBLAS DGEMM measured in this run"})
-    del K
     K32 = torch.empty((ns, n, n), dtype=torch.float32, device=dev)
     mu = torch.empty(L, dtype=torch.float64, device=dev)
     ws = torch.empty(lib.fmlb_tc_operand_bytes(n, L), dtype=torch.uint8, device=dev)
@@ -485,8 +515,8 @@ def run_stages(a):
           % (n, L, ns), "ms": ms, "entries_per_s": n * n * ns / (ms * 1e-3), "bound": "hbm",
           "achieved_gbs": wbytes / ms / 1e6, "peak_gbs": hbm, "frac": wbytes / ms / 1e6 / hbm,
           "tensor_tflops": tfl / ms / 1e9, "tensor_frac_of_bf16": tfl / ms / 1e9 / peaks["bf16_tflops"],
-          "status": int(status.item())})
-    del K32, ws
+          "max_abs_err_vs_fp64": _max_abs_diff(torch, K32, K), "status": int(status.item())})
+    del K32, ws, K
     nl = min(n, 16384)
     Kl = torch.empty((ns, nl, nl), dtype=torch.float64, device=dev)
     Xl = X[:nl]
@@ -496,7 +526,6 @@ def run_stages(a):
     emit({"stage": "laplacian_f64_symmetric", "config": "N=%d, d=%d, %d sigmas" % (nl, L, ns),
           "ms": ms, "entries_per_s": nl * nl * ns / (ms * 1e-3), "bound": "fp64",
           "achieved_tflops": fl / ms / 1e9, "peak_tflops": dgemm, "frac": fl / ms / 1e9 / dgemm})
-    del Kl
     Kl32 = torch.empty((ns, n, n), dtype=torch.float32, device=dev)
     ms = _time(torch, lambda: _lib.call("fmlb_laplacian_kernel_f32", P(Xt), n, L, P(Xt), n, L, L,
                                         sp, ns, P(Kl32), n, n * n, 1, st), reps=2)
@@ -505,8 +534,10 @@ def run_stages(a):
     emit({"stage": "laplacian_f32_symmetric", "config": "N=%d, d=%d, %d sigmas" % (n, L, ns),
           "ms": ms, "entries_per_s": n * n * ns / (ms * 1e-3), "bound": "fp32 issue",
           "achieved_fp32_tinst": fp32_tf, "peak_fp32_tinst": FP32_PEAK_TFLOPS / 2,
-          "frac": fp32_tf / (FP32_PEAK_TFLOPS / 2)})
-    del Kl32
+          "frac": fp32_tf / (FP32_PEAK_TFLOPS / 2),
+          "max_abs_err_vs_fp64": _max_abs_diff(torch, Kl32[:, :nl, :nl], Kl),
+          "error_sample": "leading %d x %d block" % (nl, nl)})
+    del Kl32, Kl
 
     # --- Cholesky, solve, prediction ------------------------------------------
     K1 = torch.empty((n, n), dtype=torch.float64, device=dev)

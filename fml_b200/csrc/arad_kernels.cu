@@ -358,6 +358,8 @@ __global__ void arad_class_assign_kernel(const double *__restrict__ X, const dou
 // a padding record (r = 1e18, xi = 0) whose window test and exponential are 0.
 constexpr int FC_PC = 8;
 constexpr int FC_PTS = FC_PC * FC_PC + 1;  // pair-table row stride (float2): conflict-free rows
+constexpr int FC_SS = FC_MAXA + 1;         // S row stride: lanes adding to different atoms i1
+                                           // of one column j1 hit different banks
 
 struct FastSmem {
     float4 recI[FC_MAXREC];      // molecule I, dense by atom, 32 records per pass
@@ -380,7 +382,7 @@ struct FastSmem {
     int aclsJ[FC_MAXA];
     float stoch[FC_MAXC * FC_SST];  // row stride 17: lanes of different classes hit distinct banks
     float2 pt[FC_PC * FC_PTS];   // pt[c1][ca * FC_PC + cb] = (stoch(c1, ca), stoch(c1, cb))
-    float S[FC_MAXA * FC_MAXA];  // S(i1, j1) of the current molecule pair
+    float S[FC_MAXA * FC_SS];    // S(i1, j1) of the current molecule pair, row stride FC_SS
     float red[FC_WARPS][FC_MAXSIG];
     int npassI, nI, nJ;
 };
@@ -554,7 +556,7 @@ __device__ __forceinline__ void fast_item_pairs(FastSmem &sm, int p, int j1, flo
         const float o = __shfl_up_sync(0xffffffffu, v, d);
         if (lane - d >= seg) v += o;
     }
-    if ((meta >> 25) & 1) atomicAdd(&sm.S[(meta & 0xff) * FC_MAXA + j1], v);
+    if ((meta >> 25) & 1) atomicAdd(&sm.S[(meta & 0xff) * FC_SS + j1], v);
 }
 
 // Work item (pass p, atom j1): the segment sums of the pass against j1 are
@@ -586,12 +588,12 @@ __device__ __forceinline__ void fast_item(FastSmem &sm, int p, int j1, float max
         const float o = __shfl_up_sync(0xffffffffu, v, d);
         if (lane - d >= seg) v += o;
     }
-    if ((meta >> 25) & 1) atomicAdd(&sm.S[(meta & 0xff) * FC_MAXA + j1], v);
+    if ((meta >> 25) & 1) atomicAdd(&sm.S[(meta & 0xff) * FC_SS + j1], v);
 }
 
 // All work items of one molecule pair, S cleared first. Whole CTA.
 __device__ __forceinline__ void fast_pair_sums(FastSmem &sm, int nJ, float maxg2s, bool paired) {
-    for (int t = threadIdx.x; t < FC_MAXA * FC_MAXA; t += blockDim.x) sm.S[t] = 0.0f;
+    for (int t = threadIdx.x; t < FC_MAXA * FC_SS; t += blockDim.x) sm.S[t] = 0.0f;
     __syncthreads();
     const int warp = threadIdx.x >> 5;
     const int items = sm.npassI * nJ;
@@ -653,7 +655,7 @@ arad_fast_self_kernel(SetWs w, const int *__restrict__ N, int nm, int amax, Arad
     const float maxg2s = (float)(P.maxg2 * fp32_scale(P) * fp32_scale(P));
     fast_pair_sums(sm, nI, maxg2s, paired);
     for (int a = threadIdx.x; a < nI; a += blockDim.x)
-        w.selff[(size_t)I * amax + a] = sm.S[a * FC_MAXA + a];
+        w.selff[(size_t)I * amax + a] = sm.S[a * FC_SS + a];
 }
 
 __global__ void __launch_bounds__(FC_WARPS * 32)
@@ -701,7 +703,7 @@ arad_fast_pair_kernel(SetWs w1, const int *__restrict__ N1, int nm1, SetWs w2,
             for (int t = threadIdx.x; t < nI * nJ; t += blockDim.x) {
                 const int a = t / nJ, j1 = t - a * nJ;
                 const float stz = sm.stoch[sm.aclsI[a] * FC_SST + sm.aclsJ[j1]];
-                float l2 = sm.selfI[a] + sm.selfJ[j1] - 2.0f * sm.S[a * FC_MAXA + j1] * stz;
+                float l2 = sm.selfI[a] + sm.selfJ[j1] - 2.0f * sm.S[a * FC_SS + j1] * stz;
                 if (fabsf(l2) < eps) l2 = 0.0f;  // farad_kernels.f90:594
 #pragma unroll
                 for (int s = 0; s < FC_MAXSIG; ++s) {

@@ -545,8 +545,11 @@ static int factor_outer_panel(double *A, long long lda, int n, int K0, int width
 }
 
 // Outer panel width: wide panels give the trailing update a long k-loop
-// (k = 512: ~28 TFLOP/s against ~17 at k = 128 on B200).
-static int outer_width(int n) { return n >= 8192 ? 4 * fmlb::NB : 2 * fmlb::NB; }
+// (k = 512: ~28 TFLOP/s against ~17 at k = 128 on B200) and fewer steps.
+// Measured at n = 32768 on B200: 455 ms (512), 436 ms (768), 429 ms (1024).
+static int outer_width(int n) {
+    return n >= 16384 ? 8 * fmlb::NB : n >= 8192 ? 4 * fmlb::NB : 2 * fmlb::NB;
+}
 
 // Two-level blocked factorisation with a lookahead of depth one. For outer
 // panel K (factored), with outer block K+1 the next:

@@ -28,7 +28,7 @@ PANEL = 128  # inner panel width of the FP64 factorisation (NB in cholesky_f64.c
 
 def outer_panel(n):
     """Outer panel width of the FP64 factorisation (outer_width in cholesky_f64.cu)."""
-    return 4 * PANEL if n >= 8192 else 2 * PANEL
+    return 8 * PANEL if n >= 16384 else 4 * PANEL if n >= 8192 else 2 * PANEL
 
 
 def potrf_launches(n):

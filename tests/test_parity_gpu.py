@@ -291,6 +291,20 @@ def test_cho_solve_multi_panel(oracle_mod, n):
     np.testing.assert_allclose(x, ref, rtol=1e-9, atol=1e-10 * np.abs(ref).max())
 
 
+def test_cho_solve_wide_outer_panels(oracle_mod):
+    """n >= 16384 factors with 1024-column outer panels (16 full panels and a
+    partial one here)."""
+    n = 16500
+    rng = np.random.default_rng(n)
+    M = rng.standard_normal((n, 64))
+    A = M @ M.T / 64 + 0.5 * np.eye(n)
+    y = rng.standard_normal(n)
+    x = fml_b200.cho_solve(A, y)
+    ref, info = oracle_mod.cho_solve(A, y)
+    assert info == 0
+    np.testing.assert_allclose(x, ref, rtol=1e-9, atol=1e-10 * np.abs(ref).max())
+
+
 @pytest.mark.parametrize("bad", [1, 33, 300, 1000])
 def test_cho_solve_failure_column_matches_lapack(oracle_mod, bad):
     n = 1031
