@@ -66,6 +66,7 @@ def parse():
                    help="requests per arrival rate")
     p.add_argument("--serve-max-train", type=int, default=32768)
     p.add_argument("--serve-baseline-seconds", type=float, default=30.0)
+    p.add_argument("--serve-retrain-frac", type=float, default=0.02)
     p.add_argument("--arad-nmol", type=int, default=4000,
                    help="molecules of the ARAD stage (the first 3/4 form the symmetric set)")
     return p.parse_args()
@@ -236,6 +237,19 @@ def measure_dgemm_peak(torch):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def max_over_ranks(torch, dist, value, device):
+    """The slowest rank's time: every replica's step is timed on its own device,
+    the job's time is the maximum (barrier before and after the timed region)."""
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seed(seed, rank):
+    """Each replica solves its own problem (independent molecules per rank)."""
+    return seed + 1000 * rank
+
+
 def run_ours(a):
     import torch
     import torch.distributed as dist
@@ -254,7 +268,7 @@ def run_ours(a):
     sigmas = [float(s) for s in a.sigmas.split(",")]
     nsig = len(sigmas)
     n_mol = a.ntrain + a.ntest
-    b = synthetic.generate(n_mol, nmax=a.nmax, seed=a.seed + 1000 * rank)
+    b = synthetic.generate(n_mol, nmax=a.nmax, seed=replica_seed(a.seed, rank))
     dev = torch.device("cuda", local)
     z = torch.from_numpy(b.charges).to(dev)
     r = torch.from_numpy(b.coords).to(dev)
@@ -289,9 +303,7 @@ def run_ours(a):
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1) / a.steps
     if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(torch, dist, ms, dev)
     per_step = entries_per_step(a.ntrain, a.ntest, nsig)
     value = world * per_step / (ms * 1e-3)
 
@@ -319,9 +331,7 @@ def run_ours(a):
         torch.cuda.synchronize()
         ems = s0.elapsed_time(s1) / a.steps
         if world > 1:
-            t = torch.tensor([ems], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+            ems = max_over_ranks(torch, dist, ems, dev)
         e2e = {"value": world * per_step / (ems * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(nsig * a.ntest * 8),
                "ms_per_step": ems, "api": "fml_b200.krr.KRRPipeline.run on host-pinned inputs"}
@@ -939,7 +949,9 @@ def run_serving(a):
     all_reqs = []
     for rate in [float(x) for x in a.serve_rates.split(",")]:
         srv.stats.clear()
-        reqs = serving_requests(a.serve_requests, rate, pool, 16, 4000, train_sizes)
+        srv.batch_log.clear()
+        reqs = serving_requests(a.serve_requests, rate, pool, 16, 4000, train_sizes,
+                                retrain_frac=a.serve_retrain_frac)
         wall = srv.serve(reqs, realtime=True)
         preds = [r for r in reqs if not r.retrain]
         mols = sum(r.nmol for r in preds)
@@ -951,9 +963,14 @@ def run_serving(a):
                     "batches": srv.stats["batches"], "retrains": len(rt),
                     "retrain_latency_ms_max": float(max(rt) * 1e3) if rt else None,
                     "budget_waits": srv.stats["budget_waits"],
-                    "p99_ms_cm": latency_summary([r for r in preds if r.model < 8]).get("p99_ms"),
-                    "p99_ms_arad": latency_summary([r for r in preds
-                                                    if r.model >= 8]).get("p99_ms")})
+                    "batch_device_ms_p50": {k: float(np.median([b[2] for b in srv.batch_log
+                                                                  if b[0] == k]) * 1e3)
+                                            for k in ("cm", "arad")
+                                            if any(b[0] == k for b in srv.batch_log)},
+                    "batch_host_launch_ms_max": float(max(b[1] for b in srv.batch_log) * 1e3)
+                    if srv.batch_log else None,
+                    "cm": latency_summary([r for r in preds if r.model < 8]),
+                    "arad": latency_summary([r for r in preds if r.model >= 8])})
         results["%g" % rate] = res
         all_reqs += preds
     clocks = sampler.stop()

@@ -152,6 +152,7 @@ class KRRServer:
         self.inflight_bytes = 0  # retrains in flight
         self.launches = 0
         self.stats = collections.Counter()
+        self.batch_log = []  # (kind, host launch seconds, device seconds, requests)
 
     # ------------------------------------------------------------------ memory
     def resident_bytes(self):
@@ -366,6 +367,7 @@ class KRRServer:
 
     # ------------------------------------------------------------------ prediction
     def _launch_predict(self, slot, m, reqs):
+        t_host = time.perf_counter()
         stream = slot["stream"]
         charges = np.concatenate([r.charges for r in reqs])
         coords = np.concatenate([np.asarray(r.coords).reshape(-1, 3) for r in reqs])
@@ -394,6 +396,8 @@ class KRRServer:
         st = _lib.stream_handle(stream)
         a = m.size
         with torch.cuda.stream(stream):
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
             for k in range(3):
                 dv[k].copy_(hp[k], non_blocking=True)
             zd, rd, od, pred = dv[:4]
@@ -419,14 +423,18 @@ class KRRServer:
                 _lib.call("fmlb_gemv_f64", P(Kt), v.n, nq, v.n, P(v.alpha), P(pred), st)
                 self.launches += 2 + arad_launches(False, m.precision, a, 1)
             hp[3].copy_(pred, non_blocking=True)
-            ev = torch.cuda.Event()
+            ev = torch.cuda.Event(enable_timing=True)
             ev.record(stream)
-        slot["busy"] = {"reqs": reqs, "event": ev, "out": hp[3], "version": v}
+        slot["busy"] = {"reqs": reqs, "event": ev, "start": ev0, "out": hp[3], "version": v,
+                        "kind": m.kind, "host_s": time.perf_counter() - t_host}
         self.stats["batches"] += 1
         self.stats["batched_requests"] += len(reqs)
 
     def _finish_predict(self, slot, now):
         b = slot["busy"]
+        # per-batch record: host time to launch, device time from first copy to last
+        self.batch_log.append((b["kind"], b["host_s"], b["start"].elapsed_time(b["event"]) * 1e-3,
+                               len(b["reqs"])))
         out = b["out"].numpy()
         k = 0
         for r in b["reqs"]:
@@ -588,6 +596,10 @@ def latency_summary(requests):
     lat = np.array([r.done - r.arrival for r in requests if not r.retrain])
     if not len(lat):
         return {}
+    wait = np.array([r.admitted - r.arrival for r in requests if not r.retrain])
+    service = np.array([r.done - r.admitted for r in requests if not r.retrain])
     return {"p50_ms": float(np.percentile(lat, 50) * 1e3),
             "p99_ms": float(np.percentile(lat, 99) * 1e3),
-            "mean_ms": float(lat.mean() * 1e3), "n": int(len(lat))}
+            "mean_ms": float(lat.mean() * 1e3), "n": int(len(lat)),
+            "queue_wait_p50_ms": float(np.percentile(wait, 50) * 1e3),
+            "service_p50_ms": float(np.percentile(service, 50) * 1e3)}
