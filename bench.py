@@ -31,6 +31,10 @@ sys.path.insert(0, ROOT)
 _CORES = len(os.sched_getaffinity(0))
 os.environ.setdefault("OMP_NUM_THREADS", str(_CORES))
 os.environ.setdefault("OPENBLAS_NUM_THREADS", str(_CORES))
+# independent hardware work queues for the serving slots and the batched side
+# streams (the default of 8 makes unrelated streams wait behind each other);
+# read when the CUDA context is created
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 import numpy as np  # noqa: E402
 

@@ -25,11 +25,18 @@ Design:
   retrain completes, batches already launched keep the old one;
 * each prediction is computed row by row with the same kernels whatever the
   batch it is in, so a request's result is the same alone and in the mix.
+
+The slots only overlap if the CUDA driver gives their streams separate
+hardware work queues: set ``CUDA_DEVICE_MAX_CONNECTIONS`` (default 8) to at
+least ``max_inflight + 4`` before the process creates its CUDA context, or a
+short CM batch can wait behind a long ARAD batch that shares its queue.
 """
 
 import collections
 import ctypes
+import os
 import time
+import warnings
 from dataclasses import dataclass
 
 import numpy as np
@@ -137,6 +144,11 @@ class KRRServer:
         self.models = {}
         if max_inflight < 1:
             raise ValueError("max_inflight must be >= 1")
+        conn = int(os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS", "8"))
+        if conn < max_inflight + 4:
+            warnings.warn("CUDA_DEVICE_MAX_CONNECTIONS=%d: streams of the %d slots share hardware "
+                          "queues, so batches can wait behind unrelated ones; set it to >= %d "
+                          "before CUDA initialises" % (conn, max_inflight, max_inflight + 4))
         # at least one slot takes ARAD batches
         high_priority_slots = min(high_priority_slots, max_inflight - 1)
         pr = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream,

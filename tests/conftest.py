@@ -4,6 +4,10 @@ import sys
 import numpy as np
 import pytest
 
+# separate hardware work queues for the serving and batched streams (read when
+# the CUDA context is created)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
