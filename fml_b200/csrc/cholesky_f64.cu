@@ -11,12 +11,12 @@
 //      non-positive pivot records the LAPACK info (1-based column) and every
 //      later kernel of the factorisation returns at once;
 //   2. panel solve L21 = A21 L11^-T as a product with the stored inverse;
-// outer panels of 256 or 512 columns (four inner panels at large n):
+// outer panels of 256, 512 or 1024 columns (wider at larger n):
 //   3. trailing update A22 -= L21 L21^T with k = the outer width, on the FP64
 //      tensor cores (mma.sync m8n8k4 f64), 128x64 tiles on or below the
 //      diagonal, operands streamed through a 3-stage cp.async pipeline;
 // with the next outer panel factored on a second stream under step 3.
-// The inverted diagonal blocks stay in the workspace for the solve.
+// The inverted diagonal blocks stay in the workspace for the solve (section 4).
 #include <math.h>
 #include <stdint.h>
 
@@ -408,52 +408,177 @@ int launch_syrk(double *C, long long ldc, int m, const double *P, long long ldp,
     return launch_syrk_impl<false>(C, ldc, m, P, ldp, k, strip_cols, info, st);
 }
 
-// ---- solve ------------------------------------------------------------------
-// forward step: y_k = Linv_k * x_k; x_j -= L[j, k-block] y_k for rows j after the block
-constexpr int SOLVE_ROWS = 256;
-__global__ void __launch_bounds__(TPB)
-forward_step_kernel(const double *__restrict__ L, long long lda, int n, int k0, int kn,
-                    const double *__restrict__ Linv, double *__restrict__ x,
-                    double *__restrict__ y) {
-    __shared__ double yk[NB];
-    const int tid = threadIdx.x;
-    if (tid < NB) {
-        double s = 0.0;
-        if (tid < kn)
-            for (int c = 0; c <= tid; ++c) s = fma(Linv[tid * NB + c], x[k0 + c], s);
-        yk[tid] = s;
-    }
-    __syncthreads();
-    if (blockIdx.x == 0 && tid < kn) y[k0 + tid] = yk[tid];
-    const int r = k0 + kn + blockIdx.x * SOLVE_ROWS + tid;
-    if (r < n) {
-        const double *row = L + (size_t)r * lda + k0;
-        double s = 0.0;
-        for (int c = 0; c < kn; ++c) s = fma(row[c], yk[c], s);
-        x[r] -= s;
+// ---- 4. triangular solves with the factor (potrs) ---------------------------
+// Right-looking, one launch per 128-block column and direction. Every thread
+// block reads its rows (forward) or columns (backward) of the factor once,
+// coalesced; the block that owns the next diagonal block also applies that
+// block's stored inverse, so the next launch starts from a finished
+// sub-vector. All reductions run in a fixed order (deterministic).
+constexpr int SOLVE_WARPS = TPB / 32;
+constexpr int FWD_ROWS = 32;   // rows per thread block past the next diagonal block
+constexpr int BWD_COLS = 32;   // columns per thread block before the previous one
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// out[t] = sum_{c <= t} Linv[t][c] in[c], t < kn (lower-triangular block
+// inverse, row-major 128 x 128); warp per row, four rows in flight per warp.
+__device__ __forceinline__ void tri_lower_apply(const double *__restrict__ Linv,
+                                                const double *in, double *out, int kn) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int t0 = warp; t0 < kn; t0 += 4 * SOLVE_WARPS) {
+        double s[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int t = t0 + q * SOLVE_WARPS;
+            s[q] = 0.0;
+#pragma unroll
+            for (int i = 0; i < NB / 32; ++i) {
+                const int c = lane + 32 * i;
+                if (t < kn && c <= t) s[q] = fma(Linv[t * NB + c], in[c], s[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const double v = warp_sum(s[q]);
+            const int t = t0 + q * SOLVE_WARPS;
+            if (lane == 0 && t < kn) out[t] = v;
+        }
     }
 }
 
-// backward step: x_k = Linv_k^T y_k; y_j -= sum_r L[k0+r, j] x_k[r] for j < k0
+// out[t] = sum_{r >= t} Linv[r][t] in[r], t < kn (the transposed inverse);
+// thread t with 2 row halves reduced through shared memory.
+__device__ __forceinline__ void tri_upper_apply(const double *__restrict__ Linv,
+                                                const double *in, double *out, int kn,
+                                                double *red) {
+    const int t = threadIdx.x & (NB - 1), h = threadIdx.x >> 7;  // TPB = 2 NB
+    double s = 0.0;
+    if (t < kn) {
+        const int r1 = min(kn, (h + 1) * (NB / 2));
+#pragma unroll 16
+        for (int r = h * (NB / 2); r < r1; ++r)
+            if (r >= t) s = fma(Linv[r * NB + t], in[r], s);
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    if (h == 0 && t < kn) out[t] = red[t] + red[t + NB];
+}
+
+// y[0..kn) = Linv_0 x[0..kn)
 __global__ void __launch_bounds__(TPB)
-backward_step_kernel(const double *__restrict__ L, long long lda, int n, int k0, int kn,
-                     const double *__restrict__ Linv, double *__restrict__ y,
+solve_first_forward_kernel(const double *__restrict__ Linv0, const double *__restrict__ x,
+                           double *__restrict__ y, int kn) {
+    tri_lower_apply(Linv0, x, y, kn);
+}
+
+// x[k0..k0+kn) = Linv_k^T y[k0..k0+kn)
+__global__ void __launch_bounds__(TPB)
+solve_first_backward_kernel(const double *__restrict__ Linvk, const double *__restrict__ y,
+                            double *__restrict__ x, int kn) {
+    __shared__ double red[TPB];
+    tri_upper_apply(Linvk, y, x, kn, red);
+}
+
+// Forward step for block column k (y_k final): x[r] -= L[r, k0:k0+kn] y_k for
+// r >= k0 + kn. Thread block 0 owns the next diagonal block and then writes
+// y_{k+1} = Linv_{k+1} x_{k+1}. Each warp keeps four rows' loads in flight.
+__global__ void __launch_bounds__(TPB)
+forward_step_kernel(const double *__restrict__ L, long long lda, int n, int k0, int kn,
+                    const double *__restrict__ LinvNext, double *__restrict__ x,
+                    double *__restrict__ y) {
+    __shared__ double yk[NB];
+    __shared__ double xn[NB];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid < NB) yk[tid] = tid < kn ? y[k0 + tid] : 0.0;
+    __syncthreads();
+    const int nb0 = k0 + kn;
+    int rb, re;
+    if (blockIdx.x == 0) {
+        rb = nb0;
+        re = min(n, nb0 + NB);
+    } else {
+        rb = nb0 + NB + (blockIdx.x - 1) * FWD_ROWS;
+        re = min(n, rb + FWD_ROWS);
+    }
+    for (int r0 = rb + warp; r0 < re; r0 += 4 * SOLVE_WARPS) {
+        double s[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = r0 + q * SOLVE_WARPS;
+            s[q] = 0.0;
+            const double *row = L + (size_t)min(r, n - 1) * lda + k0;
+#pragma unroll
+            for (int i = 0; i < NB / 32; ++i) {
+                const int c = lane + 32 * i;
+                if (r < re && c < kn) s[q] = fma(row[c], yk[c], s[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const double sq = warp_sum(s[q]);
+            const int r = r0 + q * SOLVE_WARPS;
+            if (lane == 0 && r < re) {
+                const double v = x[r] - sq;
+                x[r] = v;
+                if (blockIdx.x == 0) xn[r - nb0] = v;
+            }
+        }
+    }
+    if (blockIdx.x == 0 && LinvNext != nullptr) {
+        __syncthreads();
+        tri_lower_apply(LinvNext, xn, y + nb0, re - rb);
+    }
+}
+
+// Backward step for block column k (x_k final): y[j] -= sum_r L[k0 + r, j]
+// x_k[r] for j < k0. Thread block 0 owns the previous diagonal block's 128
+// columns (2 row halves per column) and then writes x_{k-1} = Linv_{k-1}^T
+// y_{k-1}; the others own 32 columns each (8 row groups per column). Partial
+// sums are added in a fixed order.
+__global__ void __launch_bounds__(TPB)
+backward_step_kernel(const double *__restrict__ L, long long lda, int k0, int kn,
+                     const double *__restrict__ LinvPrev, double *__restrict__ y,
                      double *__restrict__ x) {
     __shared__ double xk[NB];
+    __shared__ double yp[NB];
+    __shared__ double red[TPB];
     const int tid = threadIdx.x;
-    if (tid < NB) {
-        double s = 0.0;
-        if (tid < kn)
-            for (int r = tid; r < kn; ++r) s = fma(Linv[r * NB + tid], y[k0 + r], s);
-        xk[tid] = s;
-    }
+    if (tid < NB) xk[tid] = tid < kn ? x[k0 + tid] : 0.0;
     __syncthreads();
-    if (blockIdx.x == 0 && tid < kn) x[k0 + tid] = xk[tid];
-    const int j = blockIdx.x * SOLVE_ROWS + tid;
-    if (j < k0) {
-        double s = 0.0;
-        for (int r = 0; r < kn; ++r) s = fma(L[(size_t)(k0 + r) * lda + j], xk[r], s);
-        y[j] -= s;
+    const int pb = k0 - NB;  // first column of the previous diagonal block (k0 >= NB here)
+    const bool owner = blockIdx.x == 0;
+    const int W = owner ? NB : BWD_COLS;          // columns of this thread block
+    const int G = TPB / W;                        // row groups per column
+    const int rows_per = NB / G;
+    const int cb = owner ? pb : (blockIdx.x - 1) * BWD_COLS;
+    const int ce = owner ? k0 : min(pb, cb + BWD_COLS);
+    const int col = tid % W, g = tid / W;
+    const int j = cb + col;
+    double s = 0.0;
+    if (j < ce) {
+        const int rbeg = g * rows_per;
+#pragma unroll 16
+        for (int rr = 0; rr < rows_per; ++rr) {
+            const int r = rbeg + rr;
+            if (r < kn) s = fma(L[(size_t)(k0 + r) * lda + j], xk[r], s);
+        }
+    }
+    red[tid] = s;
+    __syncthreads();
+    if (g == 0 && j < ce) {
+        double t = 0.0;
+        for (int q = 0; q < G; ++q) t += red[q * W + col];
+        const double v = y[j] - t;
+        y[j] = v;
+        if (owner) yp[col] = v;
+    }
+    if (owner) {
+        __syncthreads();
+        tri_upper_apply(LinvPrev, yp, x + pb, NB, red);
     }
 }
 
@@ -610,19 +735,26 @@ extern "C" int fmlb_potrs_f64(const double *L, long long lda, int n, const void 
     const size_t nblk = (size_t)(n + NB - 1) / NB;
     // y lives after the inverted blocks in the workspace (written by potrs only)
     double *y = const_cast<double *>(Linv + nblk * NB * NB);
-    for (int k0 = 0, kb = 0; k0 < n; k0 += NB, ++kb) {
-        const int kn = std::min(NB, n - k0);
-        const int rest = n - k0 - kn;
-        const int grid = std::max(1, ceil_div(rest, SOLVE_ROWS));
-        forward_step_kernel<<<grid, TPB, 0, st>>>(L, lda, n, k0, kn, Linv + (size_t)kb * NB * NB,
-                                                  x, y);
+    solve_first_forward_kernel<<<1, TPB, 0, st>>>(Linv, x, y, std::min(NB, n));
+    FMLB_TRY(launch_status("solve_first_forward_kernel"));
+    for (int k0 = 0, kb = 0; k0 + NB < n; k0 += NB, ++kb) {
+        const int rest = n - k0 - NB;  // rows past this block column
+        const int grid = 1 + ceil_div(std::max(0, rest - NB), FWD_ROWS);
+        forward_step_kernel<<<grid, TPB, 0, st>>>(L, lda, n, k0, NB,
+                                                  Linv + (size_t)(kb + 1) * NB * NB, x, y);
         FMLB_TRY(launch_status("forward_step_kernel"));
     }
-    for (int kb = (int)nblk - 1; kb >= 0; --kb) {
+    {
+        const int kb = (int)nblk - 1, k0 = kb * NB;
+        solve_first_backward_kernel<<<1, TPB, 0, st>>>(Linv + (size_t)kb * NB * NB, y + k0,
+                                                       x + k0, n - k0);
+        FMLB_TRY(launch_status("solve_first_backward_kernel"));
+    }
+    for (int kb = (int)nblk - 1; kb >= 1; --kb) {
         const int k0 = kb * NB, kn = std::min(NB, n - k0);
-        const int grid = std::max(1, ceil_div(k0, SOLVE_ROWS));
-        backward_step_kernel<<<grid, TPB, 0, st>>>(L, lda, n, k0, kn, Linv + (size_t)kb * NB * NB,
-                                                   y, x);
+        const int grid = 1 + ceil_div(k0 - NB, BWD_COLS);
+        backward_step_kernel<<<grid, TPB, 0, st>>>(L, lda, k0, kn,
+                                                   Linv + (size_t)(kb - 1) * NB * NB, y, x);
         FMLB_TRY(launch_status("backward_step_kernel"));
     }
     return FMLB_OK;
