@@ -71,6 +71,8 @@ def parse():
     p.add_argument("--serve-max-train", type=int, default=32768)
     p.add_argument("--serve-baseline-seconds", type=float, default=30.0)
     p.add_argument("--serve-retrain-frac", type=float, default=0.02)
+    p.add_argument("--serve-trace", default=None,
+                   help="write every request's model, arrival, admission and completion (JSON)")
     p.add_argument("--arad-nmol", type=int, default=4000,
                    help="molecules of the ARAD stage (the first 3/4 form the symmetric set)")
     return p.parse_args()
@@ -954,6 +956,9 @@ def run_serving(a):
     for rate in [float(x) for x in a.serve_rates.split(",")]:
         srv.stats.clear()
         srv.batch_log.clear()
+        srv.retrain_host_s.clear()
+        srv.phase_max.clear()
+        retries0 = torch.cuda.memory_stats().get("num_alloc_retries", 0)
         reqs = serving_requests(a.serve_requests, rate, pool, 16, 4000, train_sizes,
                                 retrain_frac=a.serve_retrain_frac)
         wall = srv.serve(reqs, realtime=True)
@@ -973,10 +978,21 @@ def run_serving(a):
                                             if any(b[0] == k for b in srv.batch_log)},
                     "batch_host_launch_ms_max": float(max(b[1] for b in srv.batch_log) * 1e3)
                     if srv.batch_log else None,
+                    "retrain_host_launch_ms_max": float(max(srv.retrain_host_s) * 1e3)
+                    if srv.retrain_host_s else None,
+                    "loop_max_ms": {k: v * 1e3 for k, v in srv.phase_max.items()},
+                    "allocator_retries": int(torch.cuda.memory_stats().get("num_alloc_retries", 0)
+                                             - retries0),
                     "cm": latency_summary([r for r in preds if r.model < 8]),
                     "arad": latency_summary([r for r in preds if r.model >= 8])})
+        res["stats"] = dict(srv.stats)
         results["%g" % rate] = res
         all_reqs += preds
+        if a.serve_trace:
+            with open("%s.%g.json" % (a.serve_trace, rate), "w") as f:
+                json.dump({"requests": [[r.model, r.nmol, r.retrain, r.arrival, r.admitted,
+                                          r.done] for r in reqs],
+                           "batches": srv.batch_log}, f)
     clocks = sampler.stop()
     launches = srv.launches - launches0
     # sequential plain FP64 prediction, one request at a time, on a bounded sample

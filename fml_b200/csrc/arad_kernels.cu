@@ -44,6 +44,9 @@ struct SetWs {
     signed char *cls;     // (nm, amax, amax) element class of each neighbour (fast path)
     signed char *acls;    // (nm, amax)       element class of each atom (fast path)
     float *selff;         // (nm, amax)       self terms (fast path)
+    float4 *spk;          // (nm, amax, amax) records of each molecule sorted by r (paired path)
+    int *smeta;           // (nm, amax, amax) atom | class << 16 | 1 << 24 of each sorted record
+    int *nrec;            // (nm)             records per molecule
 };
 
 // Element classes (distinct periodic-table positions) of the fast FP32 path:
@@ -65,7 +68,8 @@ size_t set_ws_bytes(int nm, int amax) {
     return align256(a1 * sizeof(int)) + align256(a2 * sizeof(double)) +
            align256(a1 * sizeof(double)) + align256(a2 * sizeof(float4)) +
            align256(a2 * sizeof(float2)) + align256(a1 * sizeof(float)) + align256(a2) +
-           align256(a1) + align256(a1 * sizeof(float));
+           align256(a1) + align256(a1 * sizeof(float)) + align256(a2 * sizeof(float4)) +
+           align256(a2 * sizeof(int)) + align256((size_t)nm * sizeof(int));
 }
 
 SetWs carve(char *&p, int nm, int amax) {
@@ -80,6 +84,9 @@ SetWs carve(char *&p, int nm, int amax) {
     w.cls = reinterpret_cast<signed char *>(p); p += align256(a2);
     w.acls = reinterpret_cast<signed char *>(p); p += align256(a1);
     w.selff = reinterpret_cast<float *>(p); p += align256(a1 * sizeof(float));
+    w.spk = reinterpret_cast<float4 *>(p); p += align256(a2 * sizeof(float4));
+    w.smeta = reinterpret_cast<int *>(p); p += align256(a2 * sizeof(int));
+    w.nrec = reinterpret_cast<int *>(p); p += align256((size_t)nm * sizeof(int));
     return w;
 }
 
@@ -382,7 +389,11 @@ struct FastSmem {
     int aclsJ[FC_MAXA];
     float stoch[FC_MAXC * FC_SST];  // row stride 17: lanes of different classes hit distinct banks
     float2 pt[FC_PC * FC_PTS];   // pt[c1][ca * FC_PC + cb] = (stoch(c1, ca), stoch(c1, cb))
-    float S[FC_MAXA * FC_SS];    // S(i1, j1) of the current molecule pair, row stride FC_SS
+    union {
+        float f[FC_MAXA * FC_SS];      // scalar path: S(i1, j1), row stride FC_SS
+        long long q[FC_MAXA * FC_SS];  // paired path: S(i1, j1) in fixed point (2^-32 units)
+    } S;
+    float passLo[FC_MAXREC / 32], passHi[FC_MAXREC / 32];  // r band of each I pass (paired)
     float red[FC_WARPS][FC_MAXSIG];
     int npassI, nI, nJ;
 };
@@ -520,10 +531,16 @@ __device__ __forceinline__ float set_lt(float a, float b) {  // 1.0f if a < b, e
     return r;
 }
 
-// Paired work item: as fast_item, two records of j1 per step. Every term is
-// computed with the same operations as in fast_item; the even and odd
-// records accumulate separately and are added at the end.
-__device__ __forceinline__ void fast_item_pairs(FastSmem &sm, int p, int j1, float maxg2s) {
+// Paired work item over molecule I in radius bands: lane = one record of I
+// (records sorted by r, 32 per pass), loop over the record pairs of atom j1
+// of J, two records per step with packed FP32x2 arithmetic. Every term is
+// computed with the same operations as in fast_item. Records of j1 that lie
+// outside the (8w)^2 window of every lane of the pass (j1's records are
+// sorted by r) are skipped: their terms are exactly zero. The lane's sum is
+// added to S(i1, j1) in 2^-32 fixed point, so the result does not depend on
+// the order of the additions.
+__device__ __forceinline__ void fast_item_band(FastSmem &sm, int p, int j1, float maxg2s,
+                                               float wd) {
     const int lane = threadIdx.x & 31;
     const float4 u = sm.recI[p * 32 + lane];
     const int meta = sm.metaI[p * 32 + lane];
@@ -531,9 +548,20 @@ __device__ __forceinline__ void fast_item_pairs(FastSmem &sm, int p, int j1, flo
     const float2 nux = make_float2(-u.x, -u.x), uy = make_float2(u.y, u.y),
                  uz = make_float2(u.z, u.z), uw = make_float2(u.w, u.w);
     const int beg = sm.offJ[j1], end = sm.offJ[j1 + 1];
+    // window sub-range: pairs whose records are all <= lo, and pairs from the
+    // first one whose first record is >= hi (at most 16 pairs: one per lane)
+    const float lo = sm.passLo[p] - wd, hi = sm.passHi[p] + wd;
+    bool below = false, before = false;
+    if (beg + lane < end) {
+        const float4 A = sm.J.p.a[beg + lane];
+        below = !(A.y > lo);
+        before = A.x < hi;
+    }
+    const int mb = beg + __popc(__ballot_sync(0xffffffffu, below));
+    const int me = beg + __popc(__ballot_sync(0xffffffffu, before));
     float2 acc = make_float2(0.0f, 0.0f);
 #pragma unroll 4
-    for (int m = beg; m < end; ++m) {
+    for (int m = mb; m < me; ++m) {
         const float4 A = sm.J.p.a[m];
         const float4 B = sm.J.p.b[m];
         const float2 st = ptrow[sm.J.p.k[m]];
@@ -549,14 +577,12 @@ __device__ __forceinline__ void fast_item_pairs(FastSmem &sm, int p, int j1, flo
         const float2 eg = __fmul2_rn(__fmul2_rn(make_float2(e0, e1), st), win);
         acc = __ffma2_rn(eg, g, acc);
     }
-    const int seg = (meta >> 8) & 0xff;
-    float v = acc.x + acc.y;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const float o = __shfl_up_sync(0xffffffffu, v, d);
-        if (lane - d >= seg) v += o;
+    if ((meta >> 24) & 1) {
+        const long long f = __float2ll_rn((acc.x + acc.y) * 4294967296.0f);
+        if (f)
+            atomicAdd(reinterpret_cast<unsigned long long *>(&sm.S.q[(meta & 0xff) * FC_SS + j1]),
+                      (unsigned long long)f);
     }
-    if ((meta >> 25) & 1) atomicAdd(&sm.S[(meta & 0xff) * FC_SS + j1], v);
 }
 
 // Work item (pass p, atom j1): the segment sums of the pass against j1 are
@@ -588,22 +614,64 @@ __device__ __forceinline__ void fast_item(FastSmem &sm, int p, int j1, float max
         const float o = __shfl_up_sync(0xffffffffu, v, d);
         if (lane - d >= seg) v += o;
     }
-    if ((meta >> 25) & 1) atomicAdd(&sm.S[(meta & 0xff) * FC_SS + j1], v);
+    if ((meta >> 25) & 1) atomicAdd(&sm.S.f[(meta & 0xff) * FC_SS + j1], v);
 }
 
 // All work items of one molecule pair, S cleared first. Whole CTA.
 __device__ __forceinline__ void fast_pair_sums(FastSmem &sm, int nJ, float maxg2s, bool paired) {
-    for (int t = threadIdx.x; t < FC_MAXA * FC_SS; t += blockDim.x) sm.S[t] = 0.0f;
+    if (paired) {
+        for (int t = threadIdx.x; t < FC_MAXA * FC_SS; t += blockDim.x) sm.S.q[t] = 0;
+    } else {
+        for (int t = threadIdx.x; t < FC_MAXA * FC_SS; t += blockDim.x) sm.S.f[t] = 0.0f;
+    }
     __syncthreads();
     const int warp = threadIdx.x >> 5;
     const int items = sm.npassI * nJ;
     if (paired) {
+        // skip margin slightly wider than the window: only records whose every
+        // term is masked are skipped
+        const float wd = sqrtf(maxg2s) * 1.0001f;
         for (int it = warp; it < items; it += FC_WARPS)
-            fast_item_pairs(sm, it / nJ, it % nJ, maxg2s);
+            fast_item_band(sm, it / nJ, it % nJ, maxg2s, wd);
     } else {
         for (int it = warp; it < items; it += FC_WARPS) fast_item(sm, it / nJ, it % nJ, maxg2s);
     }
     __syncthreads();
+}
+
+__device__ __forceinline__ float s_value(const FastSmem &sm, int idx, bool paired) {
+    return paired ? (float)((double)sm.S.q[idx] * 2.3283064365386963e-10) : sm.S.f[idx];
+}
+
+// Molecule I for the paired path: its records sorted by r (prepared once per
+// set by arad_sort_records_kernel), 32 per pass, with the r band of each
+// pass. Whole CTA; the caller synchronises before the records are read.
+__device__ void fast_load_I_band(FastSmem &sm, const SetWs &w, int I, int amax, int nI,
+                                 bool use_self) {
+    const int nrec = w.nrec[I];
+    const int npass = (nrec + 31) / 32;
+    const size_t base = (size_t)I * amax * amax;
+    for (int slot = threadIdx.x; slot < npass * 32; slot += blockDim.x) {
+        if (slot < nrec) {
+            sm.recI[slot] = w.spk[base + slot];
+            sm.metaI[slot] = w.smeta[base + slot];
+        } else {
+            sm.recI[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+            sm.metaI[slot] = 0;  // inactive
+        }
+    }
+    for (int p = threadIdx.x; p < npass; p += blockDim.x) {
+        sm.passLo[p] = w.spk[base + 32 * p].x;
+        sm.passHi[p] = w.spk[base + min(32 * p + 31, nrec - 1)].x;
+    }
+    for (int a = threadIdx.x; a < nI; a += blockDim.x) {
+        sm.selfI[a] = use_self ? w.selff[(size_t)I * amax + a] : 0.0f;
+        sm.aclsI[a] = w.acls[(size_t)I * amax + a];
+    }
+    if (threadIdx.x == 0) {
+        sm.npassI = npass;
+        sm.nI = nI;
+    }
 }
 
 // Class tables of the CTA: the stoichiometric table (row stride FC_SST) and,
@@ -633,6 +701,69 @@ __device__ __forceinline__ void pair_block(long long t, int symmetric, int nbj, 
     }
 }
 
+// Records of one molecule sorted by r (ties by atom, then neighbour index):
+// the I-side layout of the paired path. One CTA per molecule, bitonic sort
+// of 64-bit keys (r bits << 32 | atom * 32 + k) in shared memory.
+__global__ void __launch_bounds__(FC_WARPS * 32)
+arad_sort_records_kernel(SetWs w, const int *__restrict__ N, int nm, int amax,
+                         const ClassInfo *ci) {
+    __shared__ unsigned long long key[FC_MAXREC];
+    __shared__ int off[FC_MAXA + 1];
+    if (ci->flag || ci->ncls > FC_PC) return;
+    const int I = blockIdx.x;
+    if (I >= nm) return;
+    const int nI = min(max(N[I], 0), amax);
+    if (threadIdx.x < 32) {
+        const int a = threadIdx.x;
+        const int cnt = a < nI ? w.nnb[(size_t)I * amax + a] : 0;
+        int incl = cnt;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int o = __shfl_up_sync(0xffffffffu, incl, d);
+            if (a >= d) incl += o;
+        }
+        off[a] = incl - cnt;
+        if (a == 31) off[32] = incl;
+    }
+    __syncthreads();
+    const int nrec = off[32];
+    int len = 1;
+    while (len < nrec) len <<= 1;
+    for (int t = threadIdx.x; t < len; t += blockDim.x) key[t] = ~0ull;
+    __syncthreads();
+    for (int t = threadIdx.x; t < nI * amax; t += blockDim.x) {
+        const int a = t / amax, k = t % amax;
+        if (k < off[a + 1] - off[a]) {
+            const float r = w.pk[((size_t)I * amax + a) * amax + k].x;
+            key[off[a] + k] = ((unsigned long long)__float_as_uint(r) << 32) |
+                              (unsigned)(a * FC_MAXA + k);
+        }
+    }
+    __syncthreads();
+    for (int size = 2; size <= len; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = threadIdx.x; t < len; t += blockDim.x) {
+                const int partner = t ^ stride;
+                if (partner > t) {
+                    const bool up = (t & size) == 0;
+                    const unsigned long long x = key[t], y = key[partner];
+                    if ((x > y) == up) {
+                        key[t] = y;
+                        key[partner] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    const size_t base = (size_t)I * amax * amax;
+    for (int t = threadIdx.x; t < nrec; t += blockDim.x) {
+        const int idx = (int)(key[t] & 0xffffffffu), a = idx / FC_MAXA, k = idx % FC_MAXA;
+        const size_t src = ((size_t)I * amax + a) * amax + k;
+        w.spk[base + t] = w.pk[src];
+        w.smeta[base + t] = a | ((int)w.cls[src] << 16) | (1 << 24);
+    }
+    if (threadIdx.x == 0) w.nrec[I] = nrec;
+}
+
 // Self terms S(a, a) through the same passes, scan and partial sums as the
 // pair kernel, so that l2 = s + s - 2 S cancels exactly for an atom with itself.
 __global__ void __launch_bounds__(FC_WARPS * 32)
@@ -646,16 +777,18 @@ arad_fast_self_kernel(SetWs w, const int *__restrict__ N, int nm, int amax, Arad
     const bool paired = ci->ncls <= FC_PC;
     fast_load_tables(sm, ci, paired);
     const int nI = min(max(N[I], 0), amax);
-    fast_load_I(sm, w, I, amax, nI, false);
-    if (paired)
+    if (paired) {
+        fast_load_I_band(sm, w, I, amax, nI, false);
         fast_load_J_pairs(sm, w, I, amax, nI, false);
-    else
+    } else {
+        fast_load_I(sm, w, I, amax, nI, false);
         fast_load_J(sm, w, I, amax, nI, false);
+    }
     __syncthreads();
     const float maxg2s = (float)(P.maxg2 * fp32_scale(P) * fp32_scale(P));
     fast_pair_sums(sm, nI, maxg2s, paired);
     for (int a = threadIdx.x; a < nI; a += blockDim.x)
-        w.selff[(size_t)I * amax + a] = sm.S[a * FC_SS + a];
+        w.selff[(size_t)I * amax + a] = s_value(sm, a * FC_SS + a, paired);
 }
 
 __global__ void __launch_bounds__(FC_WARPS * 32)
@@ -683,7 +816,10 @@ arad_fast_pair_kernel(SetWs w1, const int *__restrict__ N1, int nm1, SetWs w2,
         if (I >= nm1) break;
         __syncthreads();
         const int nI = min(max(N1[I], 0), amax);
-        fast_load_I(sm, w1, I, amax, nI, true);
+        if (paired)
+            fast_load_I_band(sm, w1, I, amax, nI, true);
+        else
+            fast_load_I(sm, w1, I, amax, nI, true);
         for (int jl = 0; jl < FC_BM; ++jl) {
             const int J = bj * FC_BM + jl;
             if (J >= nm2) break;
@@ -703,7 +839,8 @@ arad_fast_pair_kernel(SetWs w1, const int *__restrict__ N1, int nm1, SetWs w2,
             for (int t = threadIdx.x; t < nI * nJ; t += blockDim.x) {
                 const int a = t / nJ, j1 = t - a * nJ;
                 const float stz = sm.stoch[sm.aclsI[a] * FC_SST + sm.aclsJ[j1]];
-                float l2 = sm.selfI[a] + sm.selfJ[j1] - 2.0f * sm.S[a * FC_SS + j1] * stz;
+                float l2 = sm.selfI[a] + sm.selfJ[j1] -
+                           2.0f * s_value(sm, a * FC_SS + j1, paired) * stz;
                 if (fabsf(l2) < eps) l2 = 0.0f;  // farad_kernels.f90:594
 #pragma unroll
                 for (int s = 0; s < FC_MAXSIG; ++s) {
@@ -824,6 +961,9 @@ extern "C" int fmlb_arad_kernels(const double *X1, const double *Z1, const int *
             arad_class_assign_kernel<<<ceil_div((long long)nm2 * amax, tpb), tpb, 0, st>>>(
                 X2, Z2, N2, nm2, amax, ci, w2);
         FMLB_TRY(fast_smem_attrs());
+        arad_sort_records_kernel<<<nm1, FC_WARPS * 32, 0, st>>>(w1, N1, nm1, amax, ci);
+        if (!symmetric)
+            arad_sort_records_kernel<<<nm2, FC_WARPS * 32, 0, st>>>(w2, N2, nm2, amax, ci);
         arad_fast_self_kernel<<<nm1, FC_WARPS * 32, sizeof(FastSmem), st>>>(w1, N1, nm1, amax, P,
                                                                             ci);
         if (!symmetric)

@@ -182,8 +182,8 @@ def arad_launches(symmetric, precision, amax, nsigma):
     """Kernel launches of one ``fmlb_arad_kernels`` call (mirrors its host code)."""
     fast = precision == "fp32" and amax <= 32
     sets = 1 if symmetric else 2
-    if fast:  # prep, class scan, assign, self per set; class build; fast + gated generic pair
-        return 4 * sets + 1 + 2 * -(-nsigma // 8)
+    if fast:  # prep, class scan, assign, record sort, self per set; class build; fast + gated
+        return 5 * sets + 1 + 2 * -(-nsigma // 8)  # generic pair per sigma chunk
     return sets + -(-nsigma // 16)
 
 

@@ -17,12 +17,15 @@ Design:
   ``max_batch_molecules`` are merged into ONE batch: one host->device copy,
   one descriptor launch, one kernel/prediction pass, one device->host copy.
   Batches of different models run on different streams and overlap on the
-  device; cheap batches (CM) go to high-priority streams;
+  device; cheap batches (CM) run only on the high-priority streams;
 * a batch, or a retrain, is admitted only when the resident models, the slot
   arenas, the retrains in flight and the memory it adds fit the HBM budget;
 * retrains (``+m`` molecules appended to a model's training set) run on a
-  low-priority stream; the model switches to the new version when the
-  retrain completes, batches already launched keep the old one;
+  stream between the CM and ARAD priorities and are launched from a worker
+  thread (a retrain
+  enqueues thousands of kernels, and a launch into a full queue blocks); the
+  model switches to the new version when the retrain completes, batches
+  already launched keep the old one;
 * each prediction is computed row by row with the same kernels whatever the
   batch it is in, so a request's result is the same alone and in the mix.
 
@@ -33,8 +36,10 @@ short CM batch can wait behind a long ARAD batch that shares its queue.
 """
 
 import collections
+import concurrent.futures
 import ctypes
 import os
+import threading
 import time
 import warnings
 from dataclasses import dataclass
@@ -136,7 +141,7 @@ class Model:
 
 class KRRServer:
     def __init__(self, hbm_budget=150e9, max_inflight=8, max_batch_molecules=1024,
-                 high_priority_slots=2):
+                 high_priority_slots=3):
         _lib.load()
         self.dev = device()
         self.budget = float(hbm_budget)
@@ -160,11 +165,43 @@ class KRRServer:
             st = torch.cuda.Stream(device=self.dev, priority=pri)
             self.slots.append({"stream": st, "high": k < high_priority_slots, "busy": None,
                                "dev": None, "pin": None})
-        self.retrain_stream = torch.cuda.Stream(device=self.dev, priority=lo)
+        # retrains above the ARAD slots: their thousands of small kernels would
+        # otherwise wait behind whole ARAD grids and back up the launch queue
+        self._have_high = high_priority_slots > 0
+        self.retrain_stream = torch.cuda.Stream(device=self.dev, priority=(lo + hi) // 2
+                                                if lo - hi >= 2 else hi)
         self.inflight_bytes = 0  # retrains in flight
         self.launches = 0
+        self._count_lock = threading.Lock()
+        # retrains are launched from one worker thread: a retrain enqueues
+        # thousands of kernels, and a launch blocks while the stream's queue
+        # is full, which must not stall the admission of prediction batches
+        self._retrain_pool = concurrent.futures.ThreadPoolExecutor(
+            max_workers=1, thread_name_prefix="fmlb-retrain")
+        self._retrain_pool.submit(self._warm_worker).result()
         self.stats = collections.Counter()
-        self.batch_log = []  # (kind, host launch seconds, device seconds, requests)
+        # (kind, host launch s, device s, requests, admitted at, completion seen at)
+        self.batch_log = []
+        self.retrain_host_s = []  # host seconds spent launching each retrain
+        self.phase_max = collections.Counter()  # longest loop iteration / phase (seconds)
+
+    def _warm_worker(self):
+        """A 1 x 1 factorisation on the worker thread, outside any capture: it
+        creates the library's per-thread lookahead stream and events."""
+        torch.cuda.set_device(self.dev)
+        lib = _lib.load()
+        with torch.cuda.stream(self.retrain_stream):
+            A = torch.ones((1, 1), dtype=torch.float64, device=self.dev)
+            work = torch.empty(lib.fmlb_potrf_workspace_bytes(1), dtype=torch.uint8,
+                               device=self.dev)
+            info = torch.zeros(1, dtype=torch.int32, device=self.dev)
+            _lib.call("fmlb_potrf_f64", _lib.ptr(A), 1, 1, _lib.ptr(work), _lib.ptr(info),
+                      _lib.stream_handle(self.retrain_stream))
+        self.retrain_stream.synchronize()
+
+    def _count(self, k):
+        with self._count_lock:
+            self.launches += k
 
     # ------------------------------------------------------------------ memory
     def resident_bytes(self):
@@ -258,7 +295,7 @@ class KRRServer:
                 X = torch.empty((nmol, m.d), dtype=torch.float64, device=self.dev)
                 _lib.call("fmlb_coulomb_matrices", P(zd), P(rd), P(od), nmol, m.size, P(X), m.d,
                           None, 0, None, None, st)
-                self.launches += 1
+                self._count(1)
                 return {"X": X}
             a = m.size
             X = torch.empty((nmol, a, 5, a), dtype=torch.float64, device=self.dev)
@@ -267,7 +304,7 @@ class KRRServer:
             ptp, cnt = _ptp_packed(charges, offsets, a)
             Z = torch.from_numpy(ptp).pin_memory().to(self.dev, non_blocking=True)
             N = torch.from_numpy(cnt).pin_memory().to(self.dev, non_blocking=True)
-            self.launches += 1
+            self._count(1)
             return {"X": X, "Z": Z, "N": N}
 
     # ------------------------------------------------------------------ training
@@ -285,14 +322,18 @@ class KRRServer:
         _lib.call("fmlb_arad_kernels", P(A["X"]), P(A["Z"]), P(A["N"]), nA, P(B["X"]), P(B["Z"]),
                   P(B["N"]), nB, a, m.sig_ptr, 1, *ARAD_PARAMS, 1 if symmetric else 0,
                   PRECISIONS[m.precision], P(out), P(ws), ws.numel(), _lib.stream_handle(stream))
-        self.launches += arad_launches(symmetric, m.precision, a, 1)
+        self._count(arad_launches(symmetric, m.precision, a, 1))
         return ws
 
-    def _factor(self, m, K, y, stream, keep_K):
-        """L = chol(K + lam I) (a copy when K is kept), alpha = solve; returns tensors."""
+    def _factor(self, m, K, y, stream, keep_K, graphs=None):
+        """L = chol(K + lam I) (a copy when K is kept), alpha = solve; returns tensors.
+
+        With ``graphs`` (a list) the factorisation and solve are captured into
+        one CUDA graph and replayed, so that their thousands of kernels reach
+        the GPU as one submission; the graph is appended to ``graphs``.
+        """
         lib = _lib.load()
         P = _lib.ptr
-        st = _lib.stream_handle(stream)
         n = K.shape[0]
         with torch.cuda.stream(stream):
             L = K.clone() if keep_K else K
@@ -301,13 +342,34 @@ class KRRServer:
             info = torch.zeros(1, dtype=torch.int32, device=self.dev)
             alpha = torch.from_numpy(np.ascontiguousarray(y, np.float64)).pin_memory().to(
                 self.dev, non_blocking=True)
+
+        def launches():
+            st = _lib.stream_handle(stream)
             _lib.call("fmlb_add_diagonal_f64", P(L), n, n, m.lam, st)
             _lib.call("fmlb_potrf_f64", P(L), n, n, P(work), P(info), st)
             _lib.call("fmlb_potrs_f64", P(L), n, n, P(work), P(alpha), st)
-        self.launches += 1 + potrf_launches(n) + 2 * -(-n // 128)
+
+        if graphs is None:
+            with torch.cuda.stream(stream):
+                launches()
+        else:
+            # capture_begin/end directly: the torch.cuda.graph context manager
+            # synchronises the device and empties the allocator caches, which
+            # would stall the serving loop
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(stream):
+                g.capture_begin(capture_error_mode="thread_local")
+                try:
+                    launches()
+                finally:
+                    g.capture_end()
+                g.replay()
+            graphs.append(g)
+        self._count(1 + potrf_launches(n) + 2 * -(-n // 128))
         return L, work, info, alpha
 
-    def _build_version(self, m, charges, coords, offsets, y, stream, old=None, old_nmol=0):
+    def _build_version(self, m, charges, coords, offsets, y, stream, old=None, old_nmol=0,
+                       graphs=None):
         """Train on the given molecules; with ``old`` (ARAD) only the kernel rows
         of the appended molecules are computed and the old K is reused."""
         n = len(offsets) - 1
@@ -321,8 +383,8 @@ class KRRServer:
                 K = torch.empty((n, n), dtype=torch.float64, device=self.dev)
                 _lib.call("fmlb_gaussian_kernel_f64", P(D["X"]), n, m.d, P(D["X"]), n, m.d, m.d,
                           m.sig_ptr, 1, P(K), n, n * n, 1, st)
-            self.launches += 1
-            L, work, info, alpha = self._factor(m, K, y, stream, keep_K=False)
+            self._count(1)
+            L, work, info, alpha = self._factor(m, K, y, stream, keep_K=False, graphs=graphs)
             keep += [dev_in, pins]
             return _Version(n=n, X=D["X"], L=L, work=work, info=info, alpha=alpha), keep
         if old is None:
@@ -353,7 +415,7 @@ class KRRServer:
                 D = {"X": torch.cat([old.X, Dn["X"]]), "Z": torch.cat([old.Z, Dn["Z"]]),
                      "N": torch.cat([old.N, Dn["N"]])}
             keep += [dev_in, pins, C, Dm, Dn]
-        L, work, info, alpha = self._factor(m, K, y, stream, keep_K=True)
+        L, work, info, alpha = self._factor(m, K, y, stream, keep_K=True, graphs=graphs)
         return _Version(n=n, X=D["X"], Z=D["Z"], N=D["N"], K=K, L=L, work=work, info=info,
                         alpha=alpha), keep
 
@@ -419,7 +481,7 @@ class KRRServer:
                           0, None, None, st)
                 _lib.call("fmlb_kernel_predict_f64", 0, P(X), nq, m.d, P(v.X), v.n, m.d, m.d,
                           m.sig_ptr, 1, P(v.alpha), v.n, P(pred), nq, P(pw), pw.numel(), st)
-                self.launches += 3
+                self._count(3)
             else:
                 X, Z, N, Kt, ws = dv[4:9]
                 ptp, cnt = _ptp_packed(charges, offsets, a)
@@ -433,12 +495,13 @@ class KRRServer:
                           a, m.sig_ptr, 1, *ARAD_PARAMS, 0, PRECISIONS[m.precision], P(Kt), P(ws),
                           ws.numel(), st)
                 _lib.call("fmlb_gemv_f64", P(Kt), v.n, nq, v.n, P(v.alpha), P(pred), st)
-                self.launches += 2 + arad_launches(False, m.precision, a, 1)
+                self._count(2 + arad_launches(False, m.precision, a, 1))
             hp[3].copy_(pred, non_blocking=True)
             ev = torch.cuda.Event(enable_timing=True)
             ev.record(stream)
         slot["busy"] = {"reqs": reqs, "event": ev, "start": ev0, "out": hp[3], "version": v,
-                        "kind": m.kind, "host_s": time.perf_counter() - t_host}
+                        "kind": m.kind, "host_s": time.perf_counter() - t_host,
+                        "t_admit": reqs[0].admitted}
         self.stats["batches"] += 1
         self.stats["batched_requests"] += len(reqs)
 
@@ -446,7 +509,7 @@ class KRRServer:
         b = slot["busy"]
         # per-batch record: host time to launch, device time from first copy to last
         self.batch_log.append((b["kind"], b["host_s"], b["start"].elapsed_time(b["event"]) * 1e-3,
-                               len(b["reqs"])))
+                               len(b["reqs"]), b["t_admit"], now))
         out = b["out"].numpy()
         k = 0
         for r in b["reqs"]:
@@ -457,6 +520,7 @@ class KRRServer:
 
     # ------------------------------------------------------------------ retraining
     def _launch_retrain(self, m, now):
+        t_host = time.perf_counter()
         reqs = m.retrain_pending
         m.retrain_pending = []
         z0, r0, o0, y0 = m.host
@@ -473,18 +537,40 @@ class KRRServer:
         np.cumsum(counts, out=offsets[1:])
         host = (np.concatenate(zs), np.concatenate(rs), offsets, np.concatenate(ys))
         nbytes = self._train_bytes(m, len(counts), len(counts) - n0)
-        v, keep = self._build_version(m, *host, self.retrain_stream,
-                                      old=m.version if m.kind == "arad" else None, old_nmol=n0)
-        ev = torch.cuda.Event()
-        ev.record(self.retrain_stream)
+        old = m.version if m.kind == "arad" else None
+        dev = self.dev
+
+        def job():
+            torch.cuda.set_device(dev)
+            graphs = []
+            v, keep = self._build_version(m, *host, self.retrain_stream, old=old, old_nmol=n0,
+                                          graphs=graphs)
+            keep.append(graphs)
+            with torch.cuda.stream(self.retrain_stream):
+                info_host = torch.empty(1, dtype=torch.int32, pin_memory=True)
+                info_host.copy_(v.info, non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(self.retrain_stream)
+            return v, keep, info_host, ev
+
         self.inflight_bytes += nbytes
-        m.retrain_active = {"reqs": reqs, "event": ev, "version": v, "host": host, "keep": keep,
-                            "bytes": nbytes}
+        m.retrain_active = {"reqs": reqs, "future": self._retrain_pool.submit(job),
+                            "host": host, "bytes": nbytes}
         self.stats["retrains"] += 1
+        self.retrain_host_s.append(time.perf_counter() - t_host)
+
+    def _retrain_done(self, m):
+        """True once the retrain's launches were issued and its work finished."""
+        a = m.retrain_active
+        if "event" not in a:
+            if not a["future"].done():
+                return False
+            a["version"], a["keep"], a["info"], a["event"] = a["future"].result()
+        return a["event"].query()
 
     def _finish_retrain(self, m, now):
         a = m.retrain_active
-        info = int(a["version"].info.item())
+        info = int(a["info"][0])
         self.inflight_bytes -= a["bytes"]
         m.retrain_active = None
         for r in a["reqs"]:
@@ -510,8 +596,12 @@ class KRRServer:
         queues = collections.defaultdict(collections.deque)
         nxt, remaining = 0, len(reqs)
         t0 = time.perf_counter()
+        t_prev = time.perf_counter()
         while remaining:
-            now = time.perf_counter() - t0
+            t_now = time.perf_counter()
+            self.phase_max["iteration"] = max(self.phase_max["iteration"], t_now - t_prev)
+            t_prev = t_now
+            now = t_now - t0
             progressed = False
             while nxt < len(reqs) and (not realtime or reqs[nxt].arrival <= now):
                 r = reqs[nxt]
@@ -521,6 +611,7 @@ class KRRServer:
                 else:
                     queues[r.model].append(r)
                 progressed = True
+            t_ph = time.perf_counter()
             # completions
             for slot in self.slots:
                 if slot["busy"] is not None and slot["busy"]["event"].query():
@@ -528,10 +619,12 @@ class KRRServer:
                     self._finish_predict(slot, time.perf_counter() - t0)
                     progressed = True
             for m in self.models.values():
-                if m.retrain_active is not None and m.retrain_active["event"].query():
+                if m.retrain_active is not None and self._retrain_done(m):
                     remaining -= len(m.retrain_active["reqs"])
                     self._finish_retrain(m, time.perf_counter() - t0)
                     progressed = True
+            t_adm = time.perf_counter()
+            self.phase_max["completions"] = max(self.phase_max["completions"], t_adm - t_ph)
             # admission of prediction batches: the model with the oldest waiting
             # request first; CM batches prefer the high-priority slots, ARAD
             # batches use the others
@@ -545,10 +638,12 @@ class KRRServer:
                     progressed = True
                 if not q:
                     continue
+                # a CM batch in a low-priority slot would wait behind whole ARAD
+                # grids, so CM batches use only the high-priority slots
                 free = [s for s in self.slots if s["busy"] is None and
-                        (m.kind == "cm" or not s["high"])]
-                free.sort(key=lambda s: not s["high"])
+                        (s["high"] == (m.kind == "cm") or not self._have_high)]
                 if not free:
+                    self.stats["no_free_slot_" + m.kind] += 1
                     continue
                 slot = free[0]
                 take, mols, atoms = [], 0, 0
@@ -571,6 +666,8 @@ class KRRServer:
                     r.admitted = now
                 self._launch_predict(slot, m, take)
                 progressed = True
+            t_rt = time.perf_counter()
+            self.phase_max["admission"] = max(self.phase_max["admission"], t_rt - t_adm)
             # retrains: one at a time per model, when the budget allows
             for m in self.models.values():
                 if m.retrain_pending and m.retrain_active is None:
