@@ -36,6 +36,9 @@ SIGNATURES = {
     "fmlb_potrf_f64": (_i, [_vp, _ll, _i, _vp, _vp, _vp]),
     "fmlb_potrs_f64": (_i, [_vp, _ll, _i, _vp, _vp, _vp]),
     "fmlb_syrk_lower_f64": (_i, [_vp, _ll, _i, _vp, _ll, _i, _i, _vp, _vp]),
+    "fmlb_krr_refine_scratch_doubles": (_sz, [_i]),
+    "fmlb_symmetrize_lower_f64": (_i, [_vp, _ll, _i, _vp]),
+    "fmlb_krr_refine_f64": (_i, [_vp, _ll, _i, _d, _vp, _ll, _vp, _vp, _vp, _i, _vp, _vp, _vp]),
     "fmlb_add_diagonal_f64": (_i, [_vp, _ll, _i, _d, _vp]),
     "fmlb_gemv_f64": (_i, [_vp, _ll, _i, _i, _vp, _vp, _vp]),
     "fmlb_kernel_predict_workspace_bytes": (_sz, [_i, _i, _i]),

@@ -51,16 +51,31 @@ def potrs(Ad, n, work, x):
               _lib.stream_handle())
 
 
-def cho_solve(A, y, strict=False):
-    """Solve A x = y for symmetric positive-definite A."""
+def cho_solve(A, y, strict=False, refine=0, return_residuals=False):
+    """Solve A x = y for symmetric positive-definite A.
+
+    ``refine`` > 0 adds that many FP64 iterative-refinement steps on the
+    device (r = y - A x with A kept unfactored, x += solve(r));
+    ``return_residuals`` also returns ||y - A x||_2 before each step and
+    after the last (``refine`` + 1 values; the plain solve's residual for
+    ``refine=0``). Both are extensions: the reference solves once.
+    """
     if len(A.shape) != 2 or A.shape[0] != A.shape[1]:
         raise ValueError('expected square matrix')
     if len(y.shape) != 1 or y.shape[0] != A.shape[1]:
         raise ValueError('expected matrix and vector of same stride size')
     n = A.shape[0]
+    if refine < 0:
+        raise ValueError("refine must be >= 0")
     Ad, as_np = _upper_as_rowmajor_lower(A)
     x, _ = to_device(y, torch.float64)
     x = x.clone()
+    keep = refine > 0 or return_residuals
+    if keep:  # the unfactored matrix, both triangles, for the FP64 residual
+        yd = x.clone()
+        Kf = Ad.clone()
+        _lib.call("fmlb_symmetrize_lower_f64", _lib.ptr(Kf), Kf.stride(0), n,
+                  _lib.stream_handle())
     work, info = potrf(Ad, n)
     code = int(info.item())
     if code > 0:
@@ -69,4 +84,16 @@ def cho_solve(A, y, strict=False):
             raise np.linalg.LinAlgError(msg)
         warnings.warn(msg, CholeskyWarning, stacklevel=2)
     potrs(Ad, n, work, x)
-    return to_output(x, as_np or not is_torch(y))
+    if not keep:
+        return to_output(x, as_np or not is_torch(y))
+    lib = _lib.load()
+    scratch = torch.empty(lib.fmlb_krr_refine_scratch_doubles(n), dtype=torch.float64,
+                          device=Ad.device)
+    resid = torch.empty(refine + 1, dtype=torch.float64, device=Ad.device)
+    _lib.call("fmlb_krr_refine_f64", _lib.ptr(Kf), Kf.stride(0), n, 0.0, _lib.ptr(Ad),
+              Ad.stride(0), _lib.ptr(work), _lib.ptr(yd), _lib.ptr(x), int(refine),
+              _lib.ptr(resid), _lib.ptr(scratch), _lib.stream_handle())
+    out = to_output(x, as_np or not is_torch(y))
+    if return_residuals:
+        return out, resid.cpu().numpy()
+    return out

@@ -155,6 +155,21 @@ int fmlb_potrs_f64(const double *L, long long lda, int n, const void *work, doub
 int fmlb_syrk_lower_f64(double *C, long long ldc, int m, const double *P, long long ldp, int k,
                         int strip_cols, const int *info, void *stream);
 
+/* FP64 residual and iterative refinement after fmlb_potrf_f64 (the reference
+ * solves once, fml/math/fcho_solve.f90:35-42, and leaves the residual to the
+ * user). For (K + lambda I) x = y with K full and symmetric (row-major, both
+ * triangles; fmlb_symmetrize_lower_f64 mirrors the lower triangle into the
+ * upper one) and L / work its factor:
+ *   per step: r = y - (K + lambda I) x in FP64, x += solve(L, r);
+ *   resid (device, iters + 1 doubles, may be NULL): ||r||_2 before every step
+ *   and after the last one (iters = 0 computes the residual only).
+ * scratch: fmlb_krr_refine_scratch_doubles(n) device doubles. Deterministic. */
+size_t fmlb_krr_refine_scratch_doubles(int n);
+int fmlb_symmetrize_lower_f64(double *A, long long lda, int n, void *stream);
+int fmlb_krr_refine_f64(const double *K, long long ldk, int n, double lambda, const double *L,
+                        long long ldl, const void *work, const double *y, double *x, int iters,
+                        double *resid, double *scratch, void *stream);
+
 /* ------------------------------------------------------------------------
  * KRR helpers, FP64.
  * fmlb_add_diagonal_f64: A[i, i] += lambda (the user-side K + lambda I that

@@ -450,3 +450,62 @@ def test_laplacian_fp32_symmetric(cm_large):
     for k in range(2):
         np.testing.assert_array_equal(K[k], K[k].T)
         np.testing.assert_array_equal(np.diag(K[k]), 1.0)
+
+
+# ---------------------------------------------------------------------------
+# FP64 residual and iterative refinement (extension; the reference solves once)
+# Tolerances: the residual itself 1e-12 relative to numpy when it is far from
+# the rounding floor; refined x against LAPACK to 1e-5 relative at cond 1e9.
+# ---------------------------------------------------------------------------
+def test_residual_kernel_matches_numpy():
+    from fml_b200 import _lib
+    rng = np.random.default_rng(21)
+    n, lam = 777, 0.37
+    M = rng.standard_normal((n, n))
+    K = M + M.T
+    y = rng.standard_normal(n)
+    x = rng.standard_normal(n)
+    dev = torch.device("cuda")
+    Kd = torch.from_numpy(K).to(dev)
+    yd, xd = torch.from_numpy(y).to(dev), torch.from_numpy(x).to(dev)
+    lib = _lib.load()
+    scratch = torch.empty(lib.fmlb_krr_refine_scratch_doubles(n), dtype=torch.float64, device=dev)
+    resid = torch.empty(1, dtype=torch.float64, device=dev)
+    work = torch.empty(256, dtype=torch.uint8, device=dev)
+    _lib.call("fmlb_krr_refine_f64", _lib.ptr(Kd), n, n, lam, _lib.ptr(Kd), n, _lib.ptr(work),
+              _lib.ptr(yd), _lib.ptr(xd), 0, _lib.ptr(resid), _lib.ptr(scratch),
+              _lib.stream_handle())
+    r = y - K @ x - lam * x
+    np.testing.assert_allclose(scratch[:n].cpu().numpy(), r, rtol=1e-12, atol=1e-12 * np.abs(r).max())
+    np.testing.assert_allclose(resid.item(), np.linalg.norm(r), rtol=1e-12)
+    np.testing.assert_array_equal(xd.cpu().numpy(), x)  # iters = 0 leaves x alone
+
+
+def test_symmetrize_lower():
+    from fml_b200 import _lib
+    rng = np.random.default_rng(22)
+    n = 130
+    A = rng.standard_normal((n, n))
+    Ad = torch.from_numpy(A).cuda()
+    _lib.call("fmlb_symmetrize_lower_f64", _lib.ptr(Ad), n, n, _lib.stream_handle())
+    L = np.tril(A)
+    np.testing.assert_array_equal(Ad.cpu().numpy(), L + np.tril(A, -1).T)
+
+
+def test_cho_solve_refinement(oracle_mod):
+    n = 600
+    rng = np.random.default_rng(11)
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    A = (Q * np.logspace(0, -9, n)) @ Q.T  # condition number 1e9
+    A = (A + A.T) / 2
+    y = rng.standard_normal(n)
+    B = A.copy()
+    B[np.tril_indices(n, -1)] = 7.0  # only the upper triangle is read, refinement included
+    x0, r0 = fml_b200.cho_solve(B, y, return_residuals=True)
+    x2, r2 = fml_b200.cho_solve(B, y, refine=2, return_residuals=True)
+    assert r0.shape == (1,) and r2.shape == (3,)
+    np.testing.assert_array_equal(x0, fml_b200.cho_solve(B, y))
+    assert r2[-1] <= 1.5 * r2[0]
+    ref, info = oracle_mod.cho_solve(A, y)
+    assert info == 0
+    np.testing.assert_allclose(x2, ref, rtol=1e-5, atol=1e-5 * np.abs(ref).max())
