@@ -123,3 +123,31 @@ def test_batched_arad_builds_in_pass(oracle_mod, problems, arad_set, precision, 
         ref, _ = _oracle_predict(oracle_mod, p.X_train, p.y, p.X_test, p.sigma, p.lam)
         np.testing.assert_allclose(preds[k], ref, rtol=1e-8, atol=1e-8 * np.abs(ref).max())
     assert bk.launches_per_run() > 1
+
+
+def test_autotuner_times_candidates_and_caches(tmp_path, monkeypatch, problems, arad_set):
+    """The tuner times every (split threshold, grid) candidate on the solve pass
+    (ARAD kernels restored, not rebuilt), keeps the fastest, caches it, and the
+    tuned batch gives the same predictions as an untuned one."""
+    from fml_b200 import autotune
+    from fml_b200.batched import AradProblem
+    monkeypatch.setenv("FMLB_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
+    b, X, Z = arad_set
+    probs = problems[:5] + [AradProblem(X[:40], Z[:40], b.energies[:40], X[40:50], Z[40:50],
+                                        1.0, 1e-3)]
+    bk = BatchedKRR(probs, split_threshold=autotune.DEFAULT["split_threshold"],
+                    grid=autotune.DEFAULT["grid"])
+    bk.run()
+    torch.cuda.synchronize()
+    ref = [p.copy() for p in bk.predictions()]
+    cfg = autotune.batched_config(probs, tune=True, batch=bk)
+    n_cand = len(autotune.CANDIDATE_THRESHOLDS) * len(autotune.CANDIDATE_GRID_MULT)
+    assert len(cfg["candidates"]) == n_cand
+    assert cfg["ms"] == min(c[2] for c in cfg["candidates"])
+    assert autotune.batched_config(probs) == cfg  # served from the cache now
+    tuned = BatchedKRR(probs)
+    assert (tuned.split_threshold, tuned.grid) == (cfg["split_threshold"], cfg["grid"])
+    tuned.run()
+    torch.cuda.synchronize()
+    for a, c in zip(ref, tuned.predictions()):
+        np.testing.assert_allclose(c, a, rtol=1e-9, atol=1e-9 * np.abs(a).max())
