@@ -61,7 +61,8 @@ def parse():
     p.add_argument("--stages", nargs="?", const="all", default=None,
                    help="time each hot-path kernel on its own (one JSON line per stage); "
                         "'arad' times only the ARAD kernels")
-    p.add_argument("--workload", default="krr", choices=["krr", "batched", "serving"],
+    p.add_argument("--workload", default="krr",
+                   choices=["krr", "batched", "serving", "small", "arad"],
                    help="krr: the large-N KRR step (default, the headline line); batched: "
                         "256 uneven problems in one persistent launch; serving: the request loop")
     p.add_argument("--nprob", type=int, default=256)
@@ -1079,8 +1080,127 @@ def run_serving(a):
         "gpu_launches": launches, "clocks": clocks}))
 
 
+def run_small(a):
+    """The reference's CPU-runnable configuration, end to end: 2000 molecules
+    (n <= 23, seed 0), sorted CM, 1000 train / 1000 test, sigma 724, lambda
+    1e-8, FP64; the oracle port runs the same configuration in full beside it."""
+    import torch
+
+    import fml_b200
+    import oracle
+    from fml_b200 import synthetic
+
+    torch.cuda.set_device(0)
+    b = synthetic.generate(2000, nmax=23, seed=0)
+    ytr, yte = b.energies[:1000], b.energies[1000:]
+
+    def ours():
+        X = fml_b200.generate_coulomb_matrices(b.charges, b.coords, b.offsets, size=23)
+        K = fml_b200.gaussian_kernel(X[:1000].T, X[:1000].T, 724.0)
+        K[np.diag_indices_from(K)] += 1e-8
+        alpha = fml_b200.cho_solve(K, ytr)
+        return fml_b200.gaussian_kernel(X[1000:].T, X[:1000].T, 724.0) @ alpha
+
+    def cpu():
+        X = oracle.coulomb_matrices(b.charges, b.coords, b.offsets, 23)
+        K = oracle.gaussian_kernel(X[:1000].T, X[:1000].T, 724.0)
+        K[np.diag_indices_from(K)] += 1e-8
+        alpha, _ = oracle.cho_solve(K, ytr)
+        return oracle.gaussian_kernel(X[1000:].T, X[:1000].T, 724.0) @ alpha
+
+    for _ in range(max(a.warmup, 1)):
+        p_ours = ours()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        p_ours = ours()
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) / a.steps * 1e3
+    oracle.build()
+    p_cpu = cpu()
+    t0 = time.perf_counter()
+    p_cpu = cpu()
+    ms_cpu = (time.perf_counter() - t0) * 1e3
+    entries = 1000 * 1000 + 1000 * 1000
+    print(json.dumps({
+        "metric": METRIC, "workload": "plain FP64 Gaussian KRR on sorted CMs: 2000 molecules "
+        "(n <= 23, seed 0), 1000 train / 1000 test, sigma 724, lambda 1e-8, through the "
+        "drop-in API (numpy in, numpy out)", "value": entries / (ms * 1e-3), "unit": UNIT,
+        "ms_per_step": ms, "mae": float(np.abs(p_ours - yte).mean()),
+        "cpu_baseline": {"value": entries / (ms_cpu * 1e-3), "unit": UNIT, "cores": _CORES,
+                         "kind": "port", "sample": "the full configuration, one run",
+                         "ms": ms_cpu, "mae": float(np.abs(p_cpu - yte).mean())},
+        "max_rel_pred_diff_vs_cpu_port": float(np.max(np.abs(p_ours - p_cpu) /
+                                                      np.maximum(np.abs(p_cpu), 1e-300))),
+        "note": "wall-clock per call including host<->device copies of the numpy API"}))
+
+
+def run_arad(a):
+    """ARAD KRR, plain FP64 against FP32 kernels: 4000 molecules (n <= 23, seed 1),
+    ARAD descriptors (size 23, cut 1e6), 3000 train / 1000 test, sigmas {0.1, 0.5,
+    1, 2, 5}, lambda 1e-9; FP64 Cholesky and prediction in both cases."""
+    import torch
+
+    import fml_b200
+    from fml_b200 import _lib, synthetic
+
+    torch.cuda.set_device(0)
+    b = synthetic.generate(4000, nmax=23, seed=1)
+    X = fml_b200.generate_arad_descriptors(torch.from_numpy(b.charges).cuda(),
+                                           torch.from_numpy(b.coords).cuda(),
+                                           torch.from_numpy(b.offsets).cuda(), size=23, cut=1e6)
+    Z = [b.charges[b.offsets[i]:b.offsets[i + 1]] for i in range(4000)]
+    sig = [0.1, 0.5, 1.0, 2.0, 5.0]
+    ytr = torch.from_numpy(b.energies[:3000]).cuda()
+    yte = b.energies[3000:]
+    out = {}
+    for prec in ("fp64", "fp32"):
+        def step():
+            Ktr = fml_b200.get_atomic_symmetric_kernels_arad(X[:3000], Z[:3000], sig,
+                                                             precision=prec)
+            Kte = fml_b200.get_atomic_kernels_arad(X[3000:], X[:3000], Z[3000:], Z[:3000], sig,
+                                                   precision=prec)
+            preds = torch.empty((len(sig), 1000), dtype=torch.float64, device="cuda")
+            for k in range(len(sig)):
+                K = Ktr[k].clone()
+                _lib.call("fmlb_add_diagonal_f64", _lib.ptr(K), 3000, 3000, 1e-9,
+                          _lib.stream_handle())
+                alpha = fml_b200.cho_solve(K, ytr)
+                _lib.call("fmlb_gemv_f64", _lib.ptr(Kte[k]), 3000, 1000, 3000, _lib.ptr(alpha),
+                          _lib.ptr(preds[k]), _lib.stream_handle())
+            return Ktr, Kte, preds
+        step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        Ktr, Kte, P = step()
+        torch.cuda.synchronize()
+        out[prec] = (time.perf_counter() - t0, Ktr, Kte, P.cpu().numpy())
+    t64, K64, T64, P64 = out["fp64"]
+    t32, K32, T32, P32 = out["fp32"]
+    mae64 = np.abs(P64 - yte).mean(axis=1)
+    mae32 = np.abs(P32 - yte).mean(axis=1)
+    print(json.dumps({
+        "metric": METRIC, "workload": "ARAD KRR: 4000 molecules (n <= 23, seed 1), ARAD size 23 "
+        "cut 1e6, 3000 train / 1000 test, sigmas 0.1,0.5,1,2,5, lambda 1e-9; FP64 against FP32 "
+        "ARAD kernels, FP64 Cholesky and prediction",
+        "value": 3000 * 3000 * 5 / t32, "unit": "kernel entries/s (train kernel, FP32 step)",
+        "step_s": {"fp64": t64, "fp32": t32}, "speedup_fp32_vs_fp64": t64 / t32,
+        "max_abs_kernel_err_fp32": {"train": float((K32 - K64).abs().max()),
+                                    "test": float((T32 - T64).abs().max())},
+        "max_rel_kernel_err_fp32_where_K_gt_1e-8_max": float(max(
+            ((K32[k] - K64[k]).abs() / K64[k].abs())[K64[k].abs() > 1e-8 * K64[k].abs().max()]
+            .max() for k in range(len(sig)))),
+        "mae": {"fp64": dict(zip(map(str, sig), map(float, mae64))),
+                "fp32": dict(zip(map(str, sig), map(float, mae32)))},
+        "note": "wall-clock per step through the drop-in API (device tensors in and out)"}))
+
+
 def main():
     a = parse()
+    if a.workload == "small":
+        return run_small(a)
+    if a.workload == "arad":
+        return run_arad(a)
     if a.workload == "batched":
         return run_batched(a)
     if a.workload == "serving":
