@@ -459,7 +459,7 @@ __device__ __forceinline__ void tri_upper_apply(const double *__restrict__ Linv,
     double s = 0.0;
     if (t < kn) {
         const int r1 = min(kn, (h + 1) * (NB / 2));
-#pragma unroll 16
+#pragma unroll 32
         for (int r = h * (NB / 2); r < r1; ++r)
             if (r >= t) s = fma(Linv[r * NB + t], in[r], s);
     }
@@ -483,52 +483,69 @@ solve_first_backward_kernel(const double *__restrict__ Linvk, const double *__re
     tri_upper_apply(Linvk, y, x, kn, red);
 }
 
+// L2 prefetch of a 128 x 128 block (the next diagonal block's inverse), so
+// that the owner block's final step reads it from L2
+__device__ __forceinline__ void prefetch_block_l2(const double *p) {
+    for (int t = threadIdx.x; t < NB * NB / 16; t += blockDim.x)  // one 128-byte line each
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(p + (size_t)t * 16));
+}
+
 // Forward step for block column k (y_k final): x[r] -= L[r, k0:k0+kn] y_k for
 // r >= k0 + kn. Thread block 0 owns the next diagonal block and then writes
-// y_{k+1} = Linv_{k+1} x_{k+1}. Each warp keeps four rows' loads in flight.
+// y_{k+1} = Linv_{k+1} x_{k+1}. Every lane reads its four entries of y_k
+// directly, so a warp's row loads, y_k loads and x loads all go out together;
+// each warp keeps eight rows in flight.
 __global__ void __launch_bounds__(TPB)
 forward_step_kernel(const double *__restrict__ L, long long lda, int n, int k0, int kn,
                     const double *__restrict__ LinvNext, double *__restrict__ x,
                     double *__restrict__ y) {
-    __shared__ double yk[NB];
     __shared__ double xn[NB];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (tid < NB) yk[tid] = tid < kn ? y[k0 + tid] : 0.0;
-    __syncthreads();
+    const bool owner = blockIdx.x == 0;
+    if (owner && LinvNext != nullptr) prefetch_block_l2(LinvNext);
+    double ykr[NB / 32];
+#pragma unroll
+    for (int i = 0; i < NB / 32; ++i) {
+        const int c = lane + 32 * i;
+        ykr[i] = c < kn ? y[k0 + c] : 0.0;
+    }
     const int nb0 = k0 + kn;
     int rb, re;
-    if (blockIdx.x == 0) {
+    if (owner) {
         rb = nb0;
         re = min(n, nb0 + NB);
     } else {
         rb = nb0 + NB + (blockIdx.x - 1) * FWD_ROWS;
         re = min(n, rb + FWD_ROWS);
     }
-    for (int r0 = rb + warp; r0 < re; r0 += 4 * SOLVE_WARPS) {
-        double s[4];
+    constexpr int G = 8;  // rows per warp in flight
+    for (int r0 = rb + warp; r0 < re; r0 += G * SOLVE_WARPS) {
+        double s[G], xr[G];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < G; ++q) {
             const int r = r0 + q * SOLVE_WARPS;
-            s[q] = 0.0;
+            const bool ok = r < re;
             const double *row = L + (size_t)min(r, n - 1) * lda + k0;
+            s[q] = 0.0;
+            xr[q] = (ok && lane == 0) ? x[r] : 0.0;
 #pragma unroll
             for (int i = 0; i < NB / 32; ++i) {
                 const int c = lane + 32 * i;
-                if (r < re && c < kn) s[q] = fma(row[c], yk[c], s[q]);
+                if (ok && c < kn) s[q] = fma(row[c], ykr[i], s[q]);
             }
         }
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < G; ++q) {
             const double sq = warp_sum(s[q]);
             const int r = r0 + q * SOLVE_WARPS;
             if (lane == 0 && r < re) {
-                const double v = x[r] - sq;
+                const double v = xr[q] - sq;
                 x[r] = v;
-                if (blockIdx.x == 0) xn[r - nb0] = v;
+                if (owner) xn[r - nb0] = v;
             }
         }
     }
-    if (blockIdx.x == 0 && LinvNext != nullptr) {
+    if (owner && LinvNext != nullptr) {
         __syncthreads();
         tri_lower_apply(LinvNext, xn, y + nb0, re - rb);
     }
@@ -547,10 +564,11 @@ backward_step_kernel(const double *__restrict__ L, long long lda, int k0, int kn
     __shared__ double yp[NB];
     __shared__ double red[TPB];
     const int tid = threadIdx.x;
+    const bool owner = blockIdx.x == 0;
+    if (owner) prefetch_block_l2(LinvPrev);
     if (tid < NB) xk[tid] = tid < kn ? x[k0 + tid] : 0.0;
     __syncthreads();
     const int pb = k0 - NB;  // first column of the previous diagonal block (k0 >= NB here)
-    const bool owner = blockIdx.x == 0;
     const int W = owner ? NB : BWD_COLS;          // columns of this thread block
     const int G = TPB / W;                        // row groups per column
     const int rows_per = NB / G;
@@ -561,7 +579,7 @@ backward_step_kernel(const double *__restrict__ L, long long lda, int k0, int kn
     double s = 0.0;
     if (j < ce) {
         const int rbeg = g * rows_per;
-#pragma unroll 16
+#pragma unroll 32
         for (int rr = 0; rr < rows_per; ++rr) {
             const int r = rbeg + rr;
             if (r < kn) s = fma(L[(size_t)(k0 + r) * lda + j], xk[r], s);
