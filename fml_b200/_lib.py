@@ -32,6 +32,9 @@ SIGNATURES = {
     "fmlb_arad_workspace_bytes": (_sz, [_i, _i, _i, _i]),
     "fmlb_arad_kernels": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp, _i, _i, _dp, _i, _d, _d, _d, _d,
                                _i, _i, _vp, _vp, _sz, _vp]),
+    "fmlb_arad_atomic_workspace_bytes": (_sz, [_i, _i, _i]),
+    "fmlb_arad_atomic_kernels": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp, _i, _i, _dp, _i, _d, _d,
+                                      _d, _d, _vp, _vp, _sz, _vp]),
     "fmlb_potrf_workspace_bytes": (_sz, [_i]),
     "fmlb_potrf_f64": (_i, [_vp, _ll, _i, _vp, _vp, _vp]),
     "fmlb_potrs_f64": (_i, [_vp, _ll, _i, _vp, _vp, _vp]),

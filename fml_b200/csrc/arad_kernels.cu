@@ -888,8 +888,114 @@ int fast_smem_attrs() {
     return FMLB_OK;
 }
 
+// ---- atom-level ARAD kernel (fget_atomic_kernels_arad, farad_kernels.f90:757-899)
+// Every atom is its own environment: descriptor (5, amax), neighbour count n.
+// Per atom: the prefix length of the neighbour list (the exit at r > cut of
+// atomic_distl2, :68 / :72), the sine factors 1 - sin(r inv_cut) for every
+// listed neighbour (:836-850, unconditional) and the self term (:855-868).
+__global__ void arad_atom_prep_kernel(const double *__restrict__ Q, const int *__restrict__ N,
+                                      int na, int amax, AradParams P, int *__restrict__ nnb,
+                                      double *__restrict__ sines, double *__restrict__ self) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= na) return;
+    const double *q = Q + (size_t)i * 5 * amax;
+    const int n = min(max(N[i], 0), amax);
+    double *si = sines + (size_t)i * amax;
+    int pre = 0;
+    while (pre < n && !(q[pre] > P.cut)) ++pre;
+    for (int m = 0; m < amax; ++m) si[m] = m < n ? 1.0 - sin(__dmul_rn(q[m], P.inv_cut)) : 0.0;
+    nnb[i] = pre;
+    self[i] = distl2_f64(q, si, pre, q, si, pre, amax, P);
+}
+
+// K[s, i, j] = exp(l2(i, j) inv_sigma2[s]), l2 = self_i + self_j - 2 d(i, j) stoch
+// (:873-891); thread per atom pair, j fastest (coalesced rows of K)
+__global__ void __launch_bounds__(128)
+arad_atom_pair_kernel(const double *__restrict__ Q1, const double *__restrict__ Z1,
+                      const int *__restrict__ nnb1, const double *__restrict__ S1,
+                      const double *__restrict__ self1, int na1,
+                      const double *__restrict__ Q2, const double *__restrict__ Z2,
+                      const int *__restrict__ nnb2, const double *__restrict__ S2,
+                      const double *__restrict__ self2, int na2, int amax, AradParams P,
+                      SigmaTable sig, int nsig, double *__restrict__ K) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const double eps = (double)5.0e-12f;  // :823, a single-precision literal in the source
+    for (int i = blockIdx.y; i < na1; i += gridDim.y) {
+        if (j >= na2) continue;
+        double l2 = distl2_f64(Q1 + (size_t)i * 5 * amax, S1 + (size_t)i * amax, nnb1[i],
+                               Q2 + (size_t)j * 5 * amax, S2 + (size_t)j * amax, nnb2[j], amax,
+                               P);
+        const double dz1 = __dsub_rn(Z1[2 * i], Z2[2 * j]);
+        const double dz2 = __dsub_rn(Z1[2 * i + 1], Z2[2 * j + 1]);
+        const double st = __ddiv_rn(
+            __dmul_rn(__ddiv_rn(P.rw2, __dadd_rn(P.rw2, __dmul_rn(dz1, dz1))), P.cw2),
+            __dadd_rn(P.cw2, __dmul_rn(dz2, dz2)));
+        l2 = __dsub_rn(__dadd_rn(self1[i], self2[j]), __dmul_rn(__dmul_rn(2.0, l2), st));
+        if (fabs(l2) < eps) l2 = 0.0;
+        for (int s = 0; s < nsig; ++s)
+            K[((size_t)s * na1 + i) * na2 + j] = exp(__dmul_rn(l2, sig.inv_sigma2[s]));
+    }
+}
+
+size_t atom_ws_bytes(int na, int amax) {
+    return align256((size_t)na * sizeof(int)) + align256((size_t)na * amax * sizeof(double)) +
+           align256((size_t)na * sizeof(double));
+}
+
 }  // namespace
 }  // namespace fmlb
+
+extern "C" size_t fmlb_arad_atomic_workspace_bytes(int na1, int na2, int amax) {
+    if (na1 < 0 || na2 < 0 || amax < 1) return 0;
+    return fmlb::atom_ws_bytes(na1, amax) + fmlb::atom_ws_bytes(na2, amax);
+}
+
+extern "C" int fmlb_arad_atomic_kernels(const double *Q1, const double *Z1, const int *N1, int na1,
+                                        const double *Q2, const double *Z2, const int *N2, int na2,
+                                        int amax, const double *sigmas_host, int nsigma,
+                                        double width, double cut_distance, double r_width,
+                                        double c_width, double *K, void *workspace,
+                                        size_t ws_bytes, void *stream) {
+    using namespace fmlb;
+    cudaStream_t st = FMLB_STREAM(stream);
+    FMLB_REQUIRE(na1 >= 0 && na2 >= 0 && amax >= 1, "fmlb_arad_atomic_kernels: bad sizes");
+    FMLB_REQUIRE(nsigma >= 1 && nsigma <= MAXSIG && sigmas_host,
+                 "fmlb_arad_atomic_kernels: nsigma must be 1..%d", MAXSIG);
+    const size_t need = fmlb_arad_atomic_workspace_bytes(na1, na2, amax);
+    if (ws_bytes < need || (need && !workspace)) {
+        set_error("fmlb_arad_atomic_kernels: workspace %zu bytes < required %zu", ws_bytes, need);
+        return FMLB_ENOMEM;
+    }
+    if (na1 == 0 || na2 == 0) return FMLB_OK;
+    FMLB_REQUIRE(Q1 && Z1 && N1 && Q2 && Z2 && N2 && K, "fmlb_arad_atomic_kernels: null pointer");
+    AradParams P;
+    P.width = width;
+    P.cut = cut_distance;
+    P.rw2 = r_width * r_width;
+    P.cw2 = c_width * c_width;
+    P.inv_width = -1.0 / (4.0 * width * width);      // :58
+    P.maxg2 = (8.0 * width) * (8.0 * width);          // :60
+    P.inv_cut = (4.0 * atan(1.0)) / (2.0 * cut_distance);  // :828
+    SigmaTable sig;
+    for (int s = 0; s < nsigma; ++s) sig.inv_sigma2[s] = -1.0 / (sigmas_host[s] * sigmas_host[s]);
+    char *p = static_cast<char *>(workspace);
+    int *nnb1 = reinterpret_cast<int *>(p); p += align256((size_t)na1 * sizeof(int));
+    double *S1 = reinterpret_cast<double *>(p); p += align256((size_t)na1 * amax * sizeof(double));
+    double *self1 = reinterpret_cast<double *>(p); p += align256((size_t)na1 * sizeof(double));
+    int *nnb2 = reinterpret_cast<int *>(p); p += align256((size_t)na2 * sizeof(int));
+    double *S2 = reinterpret_cast<double *>(p); p += align256((size_t)na2 * amax * sizeof(double));
+    double *self2 = reinterpret_cast<double *>(p);
+    arad_atom_prep_kernel<<<ceil_div(na1, 128), 128, 0, st>>>(Q1, N1, na1, amax, P, nnb1, S1,
+                                                               self1);
+    FMLB_TRY(launch_status("arad_atom_prep_kernel"));
+    arad_atom_prep_kernel<<<ceil_div(na2, 128), 128, 0, st>>>(Q2, N2, na2, amax, P, nnb2, S2,
+                                                               self2);
+    FMLB_TRY(launch_status("arad_atom_prep_kernel"));
+    const dim3 grid(ceil_div(na2, 128), std::min(na1, 65535));
+    arad_atom_pair_kernel<<<grid, 128, 0, st>>>(Q1, Z1, nnb1, S1, self1, na1, Q2, Z2, nnb2, S2,
+                                                self2, na2, amax, P, sig, nsigma, K);
+    return launch_status("arad_atom_pair_kernel");
+}
 
 extern "C" size_t fmlb_arad_workspace_bytes(int nm1, int nm2, int amax, int symmetric) {
     if (nm1 < 0 || nm2 < 0 || amax < 1) return 0;

@@ -4,6 +4,8 @@
 * ``laplacian_kernel(A, B, sigma)`` -> flaplacian_kernel (fkernels.f90:351-377)
 * ``get_atomic_kernels_arad`` / ``get_atomic_symmetric_kernels_arad``
   -> fget_kernels_arad / fget_symmetric_kernels_arad (farad_kernels.f90:439-755)
+* ``fget_atomic_kernels_arad`` -> the atom-level routine of the same name
+  (farad_kernels.f90:757-899), which fml.kernels exports directly
 
 Signatures follow the reference: ``A`` is (d, na) and ``B`` is (d, nb) with
 descriptors as columns; the result is (na, nb). Extension: ``sigma`` may be a
@@ -185,6 +187,52 @@ def arad_launches(symmetric, precision, amax, nsigma):
     if fast:  # prep, class scan, assign, record sort, self per set; class build; fast + gated
         return 5 * sets + 1 + 2 * -(-nsigma // 8)  # generic pair per sigma chunk
     return sets + -(-nsigma // 16)
+
+
+def fget_atomic_kernels_arad(q1, q2, z1, z2, n1, n2, sigmas, na1, na2, nsigmas, width,
+                             cut_distance, r_width, c_width):
+    """Atom-level ARAD kernel, the routine fml.kernels exports from its Fortran
+    (farad_kernels.f90:757-899; the f2py argument order is kept).
+
+    q1 (na1, 5, m1) / q2 (na2, 5, m2): per-atom ARAD descriptors; z1 (na1, 2) /
+    z2 (na2, 2): period row and group column of each atom; n1 / n2: neighbour
+    counts. Returns (nsigmas, na1, na2), FP64 in the reference's order.
+    Difference: the reference prints its inv_cut value to stdout; this does not.
+    """
+    q1a = q1 if is_torch(q1) else np.asarray(q1, dtype=np.float64)
+    q2a = q2 if is_torch(q2) else np.asarray(q2, dtype=np.float64)
+    if q1a.shape[0] != na1 or q2a.shape[0] != na2 or len(n1) != na1 or len(n2) != na2:
+        raise ValueError("na1 / na2 do not match the descriptor and count arrays")
+    sig, _ = _sigma_list(sigmas)
+    if len(sig) != nsigmas:
+        raise ValueError("nsigmas does not match sigmas")
+    amax = max(q1a.shape[2], q2a.shape[2])
+    dev = device()
+
+    def padded(q):
+        t, _ = to_device(q, torch.float64)
+        if t.shape[2] == amax:
+            return t.contiguous()
+        out = torch.zeros((t.shape[0], 5, amax), dtype=torch.float64, device=dev)
+        out[:, :, :t.shape[2]] = t
+        return out
+
+    Q1, Q2 = padded(q1a), padded(q2a)
+    Z1d, _ = to_device(np.asarray(z1, np.float64).reshape(-1, 2) if not is_torch(z1) else z1,
+                       torch.float64)
+    Z2d, _ = to_device(np.asarray(z2, np.float64).reshape(-1, 2) if not is_torch(z2) else z2,
+                       torch.float64)
+    N1d, _ = to_device(np.asarray(n1, np.int32) if not is_torch(n1) else n1, torch.int32)
+    N2d, _ = to_device(np.asarray(n2, np.int32) if not is_torch(n2) else n2, torch.int32)
+    K = torch.empty((nsigmas, na1, na2), dtype=torch.float64, device=dev)
+    ws = workspace(_lib.load().fmlb_arad_atomic_workspace_bytes(na1, na2, amax))
+    sp, keep = _lib.host_doubles(sig)
+    _lib.call("fmlb_arad_atomic_kernels", _lib.ptr(Q1), _lib.ptr(Z1d), _lib.ptr(N1d), na1,
+              _lib.ptr(Q2), _lib.ptr(Z2d), _lib.ptr(N2d), na2, amax, sp, nsigmas, float(width),
+              float(cut_distance), float(r_width), float(c_width), _lib.ptr(K), _lib.ptr(ws),
+              ws.numel(), _lib.stream_handle())
+    del keep
+    return to_output(K, not is_torch(q1))
 
 
 def get_atomic_kernels_arad(X1, X2, Z1, Z2, sigmas, width=0.2, cut_distance=6.0, r_width=1.0,

@@ -118,6 +118,22 @@ int fmlb_laplacian_kernel_f64(const double *A, int na, int lda, const double *B,
  * Errors: FMLB_ENOTSUP if amax > 64; FMLB_ENOMEM if ws_bytes is too small.
  * ---------------------------------------------------------------------- */
 size_t fmlb_arad_workspace_bytes(int nm1, int nm2, int amax, int symmetric);
+
+/* Atom-level ARAD kernel, fget_atomic_kernels_arad
+ * (fml/kernels/farad_kernels.f90:757-899), FP64 in the reference's order:
+ *   K[s, i, j] = exp(l2(i, j) * -1/sigma_s^2) for every atom i of set 1 and j
+ *   of set 2, l2 = self_i + self_j - 2 atomic_distl2(i, j) stoch(z_i, z_j),
+ *   |l2| < 5e-12 -> 0.
+ *   Q1 (na1, 5, amax) per-atom ARAD descriptors, Z1 (na1, 2) PTP row/column,
+ *   N1 (na1,) neighbour counts; the same for set 2 (same amax).
+ *   K (nsigma, na1, na2) row-major; nsigma <= 16.
+ *   workspace: fmlb_arad_atomic_workspace_bytes(na1, na2, amax) bytes. */
+size_t fmlb_arad_atomic_workspace_bytes(int na1, int na2, int amax);
+int fmlb_arad_atomic_kernels(const double *Q1, const double *Z1, const int *N1, int na1,
+                             const double *Q2, const double *Z2, const int *N2, int na2, int amax,
+                             const double *sigmas_host, int nsigma, double width,
+                             double cut_distance, double r_width, double c_width, double *K,
+                             void *workspace, size_t ws_bytes, void *stream);
 int fmlb_arad_kernels(const double *X1, const double *Z1, const int *N1, int nm1,
                       const double *X2, const double *Z2, const int *N2, int nm2, int amax,
                       const double *sigmas_host, int nsigma, double width, double cut_distance,

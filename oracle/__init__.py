@@ -168,6 +168,24 @@ def get_atomic_symmetric_kernels_arad(X1, Z1, sigmas, width=0.2, cut_distance=6.
     return K
 
 
+def fget_atomic_kernels_arad(q1, q2, z1, z2, n1, n2, sigmas, na1, na2, nsigmas, width,
+                             cut_distance, r_width, c_width):
+    """farad_kernels.f90:757-899 (the f2py routine fml.kernels exports).
+    q (na, 5, m) per-atom descriptors, z (na, 2), n (na,) neighbour counts."""
+    amax = max(np.shape(q1)[2], np.shape(q2)[2])
+    Q1, Q2 = (np.zeros((q.shape[0], 5, amax)) for q in (np.asarray(q1), np.asarray(q2)))
+    Q1[:, :, :np.shape(q1)[2]] = q1
+    Q2[:, :, :np.shape(q2)[2]] = q2
+    K = np.zeros((nsigmas, na1, na2))
+    _lib().orc_arad_atomic_kernels(
+        _p(Q1), _p(Q2), _p(np.ascontiguousarray(z1, np.float64)),
+        _p(np.ascontiguousarray(z2, np.float64)), _p(np.ascontiguousarray(n1, np.int32), _ip),
+        _p(np.ascontiguousarray(n2, np.int32), _ip), _p(np.ascontiguousarray(sigmas, np.float64)),
+        na1, na2, nsigmas, amax, ctypes.c_double(width), ctypes.c_double(cut_distance),
+        ctypes.c_double(r_width), ctypes.c_double(c_width), _p(K))
+    return K
+
+
 # --------------------------------------------------------------------------
 # solve
 # --------------------------------------------------------------------------

@@ -257,6 +257,51 @@ static double orc_arad_pair(const double *Q1, const double *Z1, const int *N1, c
     return 0.0;
 }
 
+/* fget_atomic_kernels_arad: farad_kernels.f90:757-899. Q (na, 5, amax) per-atom
+ * descriptors, Z (na, 2), N (na,) neighbour counts; K (nsig, na1, na2). */
+void orc_arad_atomic_kernels(const double *Q1, const double *Q2, const double *Z1,
+                             const double *Z2, const int *N1, const int *N2,
+                             const double *sigmas, int na1, int na2, int nsig, int amax,
+                             double width, double cut, double rw, double cw, double *K)
+{
+    const double pi = 4.0 * atan(1.0);
+    const double inv_cut = pi / (2.0 * cut); /* :828 */
+    const double eps = 5.0e-12f;            /* :823 */
+    const double rw2 = rw * rw, cw2 = cw * cw;
+    double *s1 = (double *)calloc((size_t)na1 * amax, sizeof(double));
+    double *s2 = (double *)calloc((size_t)na2 * amax, sizeof(double));
+    double *self1 = (double *)calloc((size_t)na1, sizeof(double));
+    double *self2 = (double *)calloc((size_t)na2, sizeof(double));
+    for (int i = 0; i < na1; ++i) /* :836-842 */
+        for (int m = 0; m < N1[i]; ++m)
+            s1[(size_t)i * amax + m] = 1.0 - sin(Q1[((size_t)i * 5) * amax + m] * inv_cut);
+    for (int i = 0; i < na2; ++i) /* :844-850 */
+        for (int m = 0; m < N2[i]; ++m)
+            s2[(size_t)i * amax + m] = 1.0 - sin(Q2[((size_t)i * 5) * amax + m] * inv_cut);
+    for (int i = 0; i < na1; ++i) { /* :855-860 */
+        const double *x = Q1 + (size_t)i * 5 * amax, *s = s1 + (size_t)i * amax;
+        self1[i] = orc_atomic_distl2(x, x, N1[i], N1[i], s, s, amax, width, cut, rw, cw);
+    }
+    for (int i = 0; i < na2; ++i) { /* :862-868 */
+        const double *x = Q2 + (size_t)i * 5 * amax, *s = s2 + (size_t)i * amax;
+        self2[i] = orc_atomic_distl2(x, x, N2[i], N2[i], s, s, amax, width, cut, rw, cw);
+    }
+#pragma omp parallel for schedule(dynamic)
+    for (int j = 0; j < na2; ++j) /* :873-891 */
+        for (int i = 0; i < na1; ++i) {
+            double l2 = orc_atomic_distl2(Q1 + (size_t)i * 5 * amax, Q2 + (size_t)j * 5 * amax,
+                                          N1[i], N2[j], s1 + (size_t)i * amax,
+                                          s2 + (size_t)j * amax, amax, width, cut, rw, cw);
+            const double dz1 = Z1[2 * i] - Z2[2 * j], dz2 = Z1[2 * i + 1] - Z2[2 * j + 1];
+            l2 = self1[i] + self2[j] -
+                 2.0 * l2 * (rw2 / (rw2 + dz1 * dz1) * cw2 / (cw2 + dz2 * dz2));
+            if (fabs(l2) < eps) l2 = 0.0;
+            for (int k = 0; k < nsig; ++k)
+                K[((size_t)k * na1 + i) * na2 + j] = exp(l2 * (-1.0 / (sigmas[k] * sigmas[k])));
+        }
+    free(s1); free(s2); free(self1); free(self2);
+}
+
 /* fget_kernels_arad: farad_kernels.f90:439-616. K (nsig, nm1, nm2). */
 void orc_arad_kernels(const double *Q1, const double *Q2, const double *Z1, const double *Z2,
                       const int *N1, const int *N2, const double *sigmas, int nm1, int nm2,

@@ -509,3 +509,30 @@ def test_cho_solve_refinement(oracle_mod):
     ref, info = oracle_mod.cho_solve(A, y)
     assert info == 0
     np.testing.assert_allclose(x2, ref, rtol=1e-5, atol=1e-5 * np.abs(ref).max())
+
+
+# ---------------------------------------------------------------------------
+# atom-level ARAD kernel (fget_atomic_kernels_arad) against the oracle, FP64,
+# 1e-12 relative; different descriptor widths for the two sets, a cut that
+# ends some neighbour lists early
+# ---------------------------------------------------------------------------
+def test_atomic_kernels_arad_vs_oracle(oracle_mod):
+    from tests.test_arad_atomic_cpu import atoms_of
+    b = synthetic.generate(14, nmax=12, seed=12)
+    X = oracle_mod.arad_descriptors(b.charges, b.coords, b.offsets, 12, 1e6)
+    Z = [b.molecule(i)[0] for i in range(b.nmol)]
+    q, z, n, _ = atoms_of(X, Z)
+    q1, z1, n1 = q[:70], z[:70], n[:70]
+    q2, z2, n2 = q[50:, :, :10], z[50:], np.minimum(n[50:], 10)
+    sig = [0.3, 1.0, 4.0]
+    for cut in (6.0, 3.0):
+        got = fml_b200.fget_atomic_kernels_arad(q1, q2, z1, z2, n1, n2, sig, len(q1), len(q2),
+                                                len(sig), 0.2, cut, 1.0, 0.5)
+        ref = oracle_mod.fget_atomic_kernels_arad(q1, q2, z1, z2, n1, n2, sig, len(q1), len(q2),
+                                                  len(sig), 0.2, cut, 1.0, 0.5)
+        assert got.shape == (3, 70, len(q2))
+        np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-300)
+    same = fml_b200.fget_atomic_kernels_arad(q1, q1, z1, z1, n1, n1, sig, 70, 70, 3, 0.2, 6.0,
+                                             1.0, 0.5)
+    for k in range(3):
+        np.testing.assert_array_equal(np.diag(same[k]), 1.0)
