@@ -6,7 +6,8 @@ Drop-in names (same signatures and error behaviour as the reference):
   ``generate_arad_descriptor`` (fml/fml.py)
 * ``gaussian_kernel``, ``laplacian_kernel``, ``get_atomic_kernels_arad``,
   ``get_atomic_symmetric_kernels_arad`` (fml/kernels/kernels.py) and the
-  atom-level ``fget_atomic_kernels_arad`` (fml/kernels/farad_kernels.f90)
+  atom-level ``fget_atomic_kernels_arad`` / ``fget_atomic_distance_arad``
+  (fml/kernels/farad_kernels.f90)
 * ``cho_solve`` (fml/math/cho_solve.py)
 
 Batched forms: ``generate_coulomb_matrices``, ``generate_arad_descriptors``.
@@ -19,13 +20,15 @@ fallback: without the built library or a CUDA device the calls raise.
 from .cho_solve import CholeskyWarning, cho_solve
 from .data import NUCLEAR_CHARGE, PTP
 from .descriptors import generate_arad_descriptors, generate_coulomb_matrices
-from .kernels import (fget_atomic_kernels_arad, gaussian_kernel, get_atomic_kernels_arad,
-                      get_atomic_symmetric_kernels_arad, laplacian_kernel)
+from .kernels import (fget_atomic_distance_arad, fget_atomic_kernels_arad, gaussian_kernel,
+                      get_atomic_kernels_arad, get_atomic_symmetric_kernels_arad,
+                      laplacian_kernel)
 from .molecule import Molecule
 
 __all__ = [
     "Molecule", "gaussian_kernel", "laplacian_kernel", "get_atomic_kernels_arad",
-    "get_atomic_symmetric_kernels_arad", "fget_atomic_kernels_arad", "cho_solve",
+    "get_atomic_symmetric_kernels_arad", "fget_atomic_kernels_arad",
+    "fget_atomic_distance_arad", "cho_solve",
     "CholeskyWarning",
     "generate_coulomb_matrices", "generate_arad_descriptors", "NUCLEAR_CHARGE", "PTP",
 ]

@@ -33,6 +33,8 @@ SIGNATURES = {
     "fmlb_arad_kernels": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp, _i, _i, _dp, _i, _d, _d, _d, _d,
                                _i, _i, _vp, _vp, _sz, _vp]),
     "fmlb_arad_atomic_workspace_bytes": (_sz, [_i, _i, _i]),
+    "fmlb_arad_atomic_distances": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp, _i, _i, _d, _d, _d, _d,
+                                        _vp, _vp, _sz, _vp]),
     "fmlb_arad_atomic_kernels": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp, _i, _i, _dp, _i, _d, _d,
                                       _d, _d, _vp, _vp, _sz, _vp]),
     "fmlb_potrf_workspace_bytes": (_sz, [_i]),

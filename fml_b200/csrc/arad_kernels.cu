@@ -909,7 +909,10 @@ __global__ void arad_atom_prep_kernel(const double *__restrict__ Q, const int *_
 }
 
 // K[s, i, j] = exp(l2(i, j) inv_sigma2[s]), l2 = self_i + self_j - 2 d(i, j) stoch
-// (:873-891); thread per atom pair, j fastest (coalesced rows of K)
+// (:873-891); thread per atom pair, j fastest (coalesced rows of K). With
+// kDistance the l2 itself is stored, K[i, j] = l2(i, j) (the distances of
+// fget_atomic_distance_arad, :902-1030).
+template <bool kDistance>
 __global__ void __launch_bounds__(128)
 arad_atom_pair_kernel(const double *__restrict__ Q1, const double *__restrict__ Z1,
                       const int *__restrict__ nnb1, const double *__restrict__ S1,
@@ -932,8 +935,12 @@ arad_atom_pair_kernel(const double *__restrict__ Q1, const double *__restrict__ 
             __dadd_rn(P.cw2, __dmul_rn(dz2, dz2)));
         l2 = __dsub_rn(__dadd_rn(self1[i], self2[j]), __dmul_rn(__dmul_rn(2.0, l2), st));
         if (fabs(l2) < eps) l2 = 0.0;
-        for (int s = 0; s < nsig; ++s)
-            K[((size_t)s * na1 + i) * na2 + j] = exp(__dmul_rn(l2, sig.inv_sigma2[s]));
+        if (kDistance) {
+            K[(size_t)i * na2 + j] = l2;
+        } else {
+            for (int s = 0; s < nsig; ++s)
+                K[((size_t)s * na1 + i) * na2 + j] = exp(__dmul_rn(l2, sig.inv_sigma2[s]));
+        }
     }
 }
 
@@ -950,24 +957,24 @@ extern "C" size_t fmlb_arad_atomic_workspace_bytes(int na1, int na2, int amax) {
     return fmlb::atom_ws_bytes(na1, amax) + fmlb::atom_ws_bytes(na2, amax);
 }
 
-extern "C" int fmlb_arad_atomic_kernels(const double *Q1, const double *Z1, const int *N1, int na1,
-                                        const double *Q2, const double *Z2, const int *N2, int na2,
-                                        int amax, const double *sigmas_host, int nsigma,
-                                        double width, double cut_distance, double r_width,
-                                        double c_width, double *K, void *workspace,
-                                        size_t ws_bytes, void *stream) {
+static int arad_atomic_impl(const double *Q1, const double *Z1, const int *N1, int na1,
+                            const double *Q2, const double *Z2, const int *N2, int na2, int amax,
+                            const double *sigmas_host, int nsigma, double width,
+                            double cut_distance, double r_width, double c_width, double *K,
+                            void *workspace, size_t ws_bytes, bool distance, cudaStream_t st) {
     using namespace fmlb;
-    cudaStream_t st = FMLB_STREAM(stream);
-    FMLB_REQUIRE(na1 >= 0 && na2 >= 0 && amax >= 1, "fmlb_arad_atomic_kernels: bad sizes");
-    FMLB_REQUIRE(nsigma >= 1 && nsigma <= MAXSIG && sigmas_host,
-                 "fmlb_arad_atomic_kernels: nsigma must be 1..%d", MAXSIG);
+    const char *what = distance ? "fmlb_arad_atomic_distances" : "fmlb_arad_atomic_kernels";
+    FMLB_REQUIRE(na1 >= 0 && na2 >= 0 && amax >= 1, "%s: bad sizes", what);
+    if (!distance)
+        FMLB_REQUIRE(nsigma >= 1 && nsigma <= MAXSIG && sigmas_host,
+                     "%s: nsigma must be 1..%d", what, MAXSIG);
     const size_t need = fmlb_arad_atomic_workspace_bytes(na1, na2, amax);
     if (ws_bytes < need || (need && !workspace)) {
-        set_error("fmlb_arad_atomic_kernels: workspace %zu bytes < required %zu", ws_bytes, need);
+        set_error("%s: workspace %zu bytes < required %zu", what, ws_bytes, need);
         return FMLB_ENOMEM;
     }
     if (na1 == 0 || na2 == 0) return FMLB_OK;
-    FMLB_REQUIRE(Q1 && Z1 && N1 && Q2 && Z2 && N2 && K, "fmlb_arad_atomic_kernels: null pointer");
+    FMLB_REQUIRE(Q1 && Z1 && N1 && Q2 && Z2 && N2 && K, "%s: null pointer", what);
     AradParams P;
     P.width = width;
     P.cut = cut_distance;
@@ -977,7 +984,8 @@ extern "C" int fmlb_arad_atomic_kernels(const double *Q1, const double *Z1, cons
     P.maxg2 = (8.0 * width) * (8.0 * width);          // :60
     P.inv_cut = (4.0 * atan(1.0)) / (2.0 * cut_distance);  // :828
     SigmaTable sig;
-    for (int s = 0; s < nsigma; ++s) sig.inv_sigma2[s] = -1.0 / (sigmas_host[s] * sigmas_host[s]);
+    for (int s = 0; s < (distance ? 0 : nsigma); ++s)
+        sig.inv_sigma2[s] = -1.0 / (sigmas_host[s] * sigmas_host[s]);
     char *p = static_cast<char *>(workspace);
     int *nnb1 = reinterpret_cast<int *>(p); p += align256((size_t)na1 * sizeof(int));
     double *S1 = reinterpret_cast<double *>(p); p += align256((size_t)na1 * amax * sizeof(double));
@@ -992,9 +1000,37 @@ extern "C" int fmlb_arad_atomic_kernels(const double *Q1, const double *Z1, cons
                                                                self2);
     FMLB_TRY(launch_status("arad_atom_prep_kernel"));
     const dim3 grid(ceil_div(na2, 128), std::min(na1, 65535));
-    arad_atom_pair_kernel<<<grid, 128, 0, st>>>(Q1, Z1, nnb1, S1, self1, na1, Q2, Z2, nnb2, S2,
-                                                self2, na2, amax, P, sig, nsigma, K);
+    if (distance)
+        arad_atom_pair_kernel<true><<<grid, 128, 0, st>>>(Q1, Z1, nnb1, S1, self1, na1, Q2, Z2,
+                                                          nnb2, S2, self2, na2, amax, P, sig, 0,
+                                                          K);
+    else
+        arad_atom_pair_kernel<false><<<grid, 128, 0, st>>>(Q1, Z1, nnb1, S1, self1, na1, Q2, Z2,
+                                                           nnb2, S2, self2, na2, amax, P, sig,
+                                                           nsigma, K);
     return launch_status("arad_atom_pair_kernel");
+}
+
+extern "C" int fmlb_arad_atomic_kernels(const double *Q1, const double *Z1, const int *N1, int na1,
+                                        const double *Q2, const double *Z2, const int *N2, int na2,
+                                        int amax, const double *sigmas_host, int nsigma,
+                                        double width, double cut_distance, double r_width,
+                                        double c_width, double *K, void *workspace,
+                                        size_t ws_bytes, void *stream) {
+    return arad_atomic_impl(Q1, Z1, N1, na1, Q2, Z2, N2, na2, amax, sigmas_host, nsigma, width,
+                            cut_distance, r_width, c_width, K, workspace, ws_bytes, false,
+                            FMLB_STREAM(stream));
+}
+
+extern "C" int fmlb_arad_atomic_distances(const double *Q1, const double *Z1, const int *N1,
+                                          int na1, const double *Q2, const double *Z2,
+                                          const int *N2, int na2, int amax, double width,
+                                          double cut_distance, double r_width, double c_width,
+                                          double *D, void *workspace, size_t ws_bytes,
+                                          void *stream) {
+    return arad_atomic_impl(Q1, Z1, N1, na1, Q2, Z2, N2, na2, amax, nullptr, 0, width,
+                            cut_distance, r_width, c_width, D, workspace, ws_bytes, true,
+                            FMLB_STREAM(stream));
 }
 
 extern "C" size_t fmlb_arad_workspace_bytes(int nm1, int nm2, int amax, int symmetric) {

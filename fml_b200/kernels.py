@@ -4,8 +4,9 @@
 * ``laplacian_kernel(A, B, sigma)`` -> flaplacian_kernel (fkernels.f90:351-377)
 * ``get_atomic_kernels_arad`` / ``get_atomic_symmetric_kernels_arad``
   -> fget_kernels_arad / fget_symmetric_kernels_arad (farad_kernels.f90:439-755)
-* ``fget_atomic_kernels_arad`` -> the atom-level routine of the same name
-  (farad_kernels.f90:757-899), which fml.kernels exports directly
+* ``fget_atomic_kernels_arad`` / ``fget_atomic_distance_arad`` -> the
+  atom-level routines of the same names (farad_kernels.f90:757-1030), which
+  fml.kernels exports directly
 
 Signatures follow the reference: ``A`` is (d, na) and ``B`` is (d, nb) with
 descriptors as columns; the result is (na, nb). Extension: ``sigma`` may be a
@@ -189,6 +190,29 @@ def arad_launches(symmetric, precision, amax, nsigma):
     return sets + -(-nsigma // 16)
 
 
+def _atomic_inputs(q1a, q2a, z1, z2, n1, n2):
+    """Per-atom descriptors on the device, padded to one width, with PTP and counts."""
+    amax = max(q1a.shape[2], q2a.shape[2])
+    dev = device()
+
+    def padded(q):
+        t, _ = to_device(q, torch.float64)
+        if t.shape[2] == amax:
+            return t.contiguous()
+        out = torch.zeros((t.shape[0], 5, amax), dtype=torch.float64, device=dev)
+        out[:, :, :t.shape[2]] = t
+        return out
+
+    def rows(z):
+        return to_device(z if is_torch(z) else np.asarray(z, np.float64).reshape(-1, 2),
+                         torch.float64)[0]
+
+    def counts(n):
+        return to_device(n if is_torch(n) else np.asarray(n, np.int32), torch.int32)[0]
+
+    return padded(q1a), padded(q2a), rows(z1), rows(z2), counts(n1), counts(n2), amax
+
+
 def fget_atomic_kernels_arad(q1, q2, z1, z2, n1, n2, sigmas, na1, na2, nsigmas, width,
                              cut_distance, r_width, c_width):
     """Atom-level ARAD kernel, the routine fml.kernels exports from its Fortran
@@ -206,24 +230,8 @@ def fget_atomic_kernels_arad(q1, q2, z1, z2, n1, n2, sigmas, na1, na2, nsigmas, 
     sig, _ = _sigma_list(sigmas)
     if len(sig) != nsigmas:
         raise ValueError("nsigmas does not match sigmas")
-    amax = max(q1a.shape[2], q2a.shape[2])
+    Q1, Q2, Z1d, Z2d, N1d, N2d, amax = _atomic_inputs(q1a, q2a, z1, z2, n1, n2)
     dev = device()
-
-    def padded(q):
-        t, _ = to_device(q, torch.float64)
-        if t.shape[2] == amax:
-            return t.contiguous()
-        out = torch.zeros((t.shape[0], 5, amax), dtype=torch.float64, device=dev)
-        out[:, :, :t.shape[2]] = t
-        return out
-
-    Q1, Q2 = padded(q1a), padded(q2a)
-    Z1d, _ = to_device(np.asarray(z1, np.float64).reshape(-1, 2) if not is_torch(z1) else z1,
-                       torch.float64)
-    Z2d, _ = to_device(np.asarray(z2, np.float64).reshape(-1, 2) if not is_torch(z2) else z2,
-                       torch.float64)
-    N1d, _ = to_device(np.asarray(n1, np.int32) if not is_torch(n1) else n1, torch.int32)
-    N2d, _ = to_device(np.asarray(n2, np.int32) if not is_torch(n2) else n2, torch.int32)
     K = torch.empty((nsigmas, na1, na2), dtype=torch.float64, device=dev)
     ws = workspace(_lib.load().fmlb_arad_atomic_workspace_bytes(na1, na2, amax))
     sp, keep = _lib.host_doubles(sig)
@@ -233,6 +241,33 @@ def fget_atomic_kernels_arad(q1, q2, z1, z2, n1, n2, sigmas, na1, na2, nsigmas, 
               ws.numel(), _lib.stream_handle())
     del keep
     return to_output(K, not is_torch(q1))
+
+
+def fget_atomic_distance_arad(q1, q2, z1, z2, n1, n2, na1, na2, width, cut_distance, r_width,
+                              c_width):
+    """Atom-pair l2 distances, the routine fml.kernels exports from its Fortran
+    (farad_kernels.f90:902-1030; the f2py argument order is kept).
+
+    The reference stores l2(i, j) at kernel(j, i) of an (na1, na2) array
+    (:1019): the result is the transpose of the distance matrix, and only
+    na1 == na2 stays inside the array. That result is reproduced for
+    na1 == na2; other shapes raise ValueError.
+    """
+    if na1 != na2:
+        raise ValueError("fget_atomic_distance_arad writes kernel(j, i) into an (na1, na2) "
+                         "array: only na1 == na2 is defined")
+    q1a = q1 if is_torch(q1) else np.asarray(q1, dtype=np.float64)
+    q2a = q2 if is_torch(q2) else np.asarray(q2, dtype=np.float64)
+    if q1a.shape[0] != na1 or q2a.shape[0] != na2 or len(n1) != na1 or len(n2) != na2:
+        raise ValueError("na1 / na2 do not match the descriptor and count arrays")
+    Q1, Q2, Z1d, Z2d, N1d, N2d, amax = _atomic_inputs(q1a, q2a, z1, z2, n1, n2)
+    D = torch.empty((na1, na2), dtype=torch.float64, device=device())
+    ws = workspace(_lib.load().fmlb_arad_atomic_workspace_bytes(na1, na2, amax))
+    _lib.call("fmlb_arad_atomic_distances", _lib.ptr(Q1), _lib.ptr(Z1d), _lib.ptr(N1d), na1,
+              _lib.ptr(Q2), _lib.ptr(Z2d), _lib.ptr(N2d), na2, amax, float(width),
+              float(cut_distance), float(r_width), float(c_width), _lib.ptr(D), _lib.ptr(ws),
+              ws.numel(), _lib.stream_handle())
+    return to_output(D.t().contiguous(), not is_torch(q1))
 
 
 def get_atomic_kernels_arad(X1, X2, Z1, Z2, sigmas, width=0.2, cut_distance=6.0, r_width=1.0,

@@ -129,6 +129,14 @@ size_t fmlb_arad_workspace_bytes(int nm1, int nm2, int amax, int symmetric);
  *   K (nsigma, na1, na2) row-major; nsigma <= 16.
  *   workspace: fmlb_arad_atomic_workspace_bytes(na1, na2, amax) bytes. */
 size_t fmlb_arad_atomic_workspace_bytes(int na1, int na2, int amax);
+/* The atom-pair l2 distances themselves, fget_atomic_distance_arad
+ * (fml/kernels/farad_kernels.f90:902-1030): D[i, j] = l2(i, j) as above, D
+ * (na1, na2) row-major; same workspace as fmlb_arad_atomic_kernels. */
+int fmlb_arad_atomic_distances(const double *Q1, const double *Z1, const int *N1, int na1,
+                               const double *Q2, const double *Z2, const int *N2, int na2,
+                               int amax, double width, double cut_distance, double r_width,
+                               double c_width, double *D, void *workspace, size_t ws_bytes,
+                               void *stream);
 int fmlb_arad_atomic_kernels(const double *Q1, const double *Z1, const int *N1, int na1,
                              const double *Q2, const double *Z2, const int *N2, int na2, int amax,
                              const double *sigmas_host, int nsigma, double width,

@@ -186,6 +186,23 @@ def fget_atomic_kernels_arad(q1, q2, z1, z2, n1, n2, sigmas, na1, na2, nsigmas, 
     return K
 
 
+def atomic_distances_arad(q1, q2, z1, z2, n1, n2, width, cut_distance, r_width, c_width):
+    """The l2 distances of fget_atomic_distance_arad (farad_kernels.f90:902-1030),
+    D[i, j] = l2(i, j), shape (na1, na2)."""
+    amax = max(np.shape(q1)[2], np.shape(q2)[2])
+    Q1, Q2 = (np.zeros((q.shape[0], 5, amax)) for q in (np.asarray(q1), np.asarray(q2)))
+    Q1[:, :, :np.shape(q1)[2]] = q1
+    Q2[:, :, :np.shape(q2)[2]] = q2
+    D = np.zeros((len(Q1), len(Q2)))
+    _lib().orc_arad_atomic_distances(
+        _p(Q1), _p(Q2), _p(np.ascontiguousarray(z1, np.float64)),
+        _p(np.ascontiguousarray(z2, np.float64)), _p(np.ascontiguousarray(n1, np.int32), _ip),
+        _p(np.ascontiguousarray(n2, np.int32), _ip), len(Q1), len(Q2), amax,
+        ctypes.c_double(width), ctypes.c_double(cut_distance), ctypes.c_double(r_width),
+        ctypes.c_double(c_width), _p(D))
+    return D
+
+
 # --------------------------------------------------------------------------
 # solve
 # --------------------------------------------------------------------------

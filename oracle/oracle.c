@@ -259,10 +259,11 @@ static double orc_arad_pair(const double *Q1, const double *Z1, const int *N1, c
 
 /* fget_atomic_kernels_arad: farad_kernels.f90:757-899. Q (na, 5, amax) per-atom
  * descriptors, Z (na, 2), N (na,) neighbour counts; K (nsig, na1, na2). */
-void orc_arad_atomic_kernels(const double *Q1, const double *Q2, const double *Z1,
-                             const double *Z2, const int *N1, const int *N2,
-                             const double *sigmas, int na1, int na2, int nsig, int amax,
-                             double width, double cut, double rw, double cw, double *K)
+static void orc_arad_atomic(const double *Q1, const double *Q2, const double *Z1,
+                            const double *Z2, const int *N1, const int *N2,
+                            const double *sigmas, int na1, int na2, int nsig, int amax,
+                            double width, double cut, double rw, double cw, double *K,
+                            int distance)
 {
     const double pi = 4.0 * atan(1.0);
     const double inv_cut = pi / (2.0 * cut); /* :828 */
@@ -296,10 +297,32 @@ void orc_arad_atomic_kernels(const double *Q1, const double *Q2, const double *Z
             l2 = self1[i] + self2[j] -
                  2.0 * l2 * (rw2 / (rw2 + dz1 * dz1) * cw2 / (cw2 + dz2 * dz2));
             if (fabs(l2) < eps) l2 = 0.0;
+            if (distance) { /* fget_atomic_distance_arad stores l2 (:1019) */
+                K[(size_t)i * na2 + j] = l2;
+                continue;
+            }
             for (int k = 0; k < nsig; ++k)
                 K[((size_t)k * na1 + i) * na2 + j] = exp(l2 * (-1.0 / (sigmas[k] * sigmas[k])));
         }
     free(s1); free(s2); free(self1); free(self2);
+}
+
+void orc_arad_atomic_kernels(const double *Q1, const double *Q2, const double *Z1,
+                             const double *Z2, const int *N1, const int *N2,
+                             const double *sigmas, int na1, int na2, int nsig, int amax,
+                             double width, double cut, double rw, double cw, double *K)
+{
+    orc_arad_atomic(Q1, Q2, Z1, Z2, N1, N2, sigmas, na1, na2, nsig, amax, width, cut, rw, cw,
+                    K, 0);
+}
+
+/* fget_atomic_distance_arad: farad_kernels.f90:902-1030; D[i, j] = l2(i, j). */
+void orc_arad_atomic_distances(const double *Q1, const double *Q2, const double *Z1,
+                               const double *Z2, const int *N1, const int *N2, int na1, int na2,
+                               int amax, double width, double cut, double rw, double cw,
+                               double *D)
+{
+    orc_arad_atomic(Q1, Q2, Z1, Z2, N1, N2, NULL, na1, na2, 0, amax, width, cut, rw, cw, D, 1);
 }
 
 /* fget_kernels_arad: farad_kernels.f90:439-616. K (nsig, nm1, nm2). */

@@ -41,3 +41,16 @@ def test_atomic_kernel_sums_to_molecular_symmetric_kernel(oracle_mod):
     # self pairs: l2 = 0 exactly, so the diagonal of every sigma is 1
     for k in range(len(sig)):
         np.testing.assert_array_equal(np.diag(Ka[k]), 1.0)
+
+
+def test_atomic_distances_are_the_kernel_exponents(oracle_mod):
+    """fget_atomic_distance_arad's l2 and fget_atomic_kernels_arad's exp(-l2/s^2)
+    come from the same l2 (farad_kernels.f90:873-891 and :1005-1019)."""
+    b = synthetic.generate(6, nmax=9, seed=5)
+    X = oracle_mod.arad_descriptors(b.charges, b.coords, b.offsets, 9, 1e6)
+    Z = [b.molecule(i)[0] for i in range(b.nmol)]
+    q, z, n, _ = atoms_of(X, Z)
+    D = oracle_mod.atomic_distances_arad(q, q[:20], z, z[:20], n, n[:20], 0.2, 6.0, 1.0, 0.5)
+    K = oracle_mod.fget_atomic_kernels_arad(q, q[:20], z, z[:20], n, n[:20], [1.3], len(q), 20,
+                                            1, 0.2, 6.0, 1.0, 0.5)
+    np.testing.assert_allclose(K[0], np.exp(D * (-1.0 / 1.3 ** 2)), rtol=1e-15, atol=0)

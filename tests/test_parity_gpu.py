@@ -536,3 +536,19 @@ def test_atomic_kernels_arad_vs_oracle(oracle_mod):
                                              1.0, 0.5)
     for k in range(3):
         np.testing.assert_array_equal(np.diag(same[k]), 1.0)
+
+
+def test_atomic_distance_arad_vs_oracle(oracle_mod):
+    from tests.test_arad_atomic_cpu import atoms_of
+    b = synthetic.generate(10, nmax=11, seed=13)
+    X = oracle_mod.arad_descriptors(b.charges, b.coords, b.offsets, 11, 1e6)
+    Z = [b.molecule(i)[0] for i in range(b.nmol)]
+    q, z, n, _ = atoms_of(X, Z)
+    q1, q2 = q[:40], q[-40:]
+    z1, z2, n1, n2 = z[:40], z[-40:], n[:40], n[-40:]
+    got = fml_b200.fget_atomic_distance_arad(q1, q2, z1, z2, n1, n2, 40, 40, 0.2, 6.0, 1.0, 0.5)
+    D = oracle_mod.atomic_distances_arad(q1, q2, z1, z2, n1, n2, 0.2, 6.0, 1.0, 0.5)
+    np.testing.assert_allclose(got, D.T, rtol=1e-12, atol=1e-12 * np.abs(D).max())
+    with pytest.raises(ValueError):
+        fml_b200.fget_atomic_distance_arad(q1, q2[:5], z1, z2[:5], n1, n2[:5], 40, 5, 0.2, 6.0,
+                                           1.0, 0.5)
