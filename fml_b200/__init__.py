@@ -3,32 +3,39 @@
 Drop-in names (same signatures and error behaviour as the reference):
 
 * ``Molecule`` with ``read_xyz``, ``generate_coulomb_matrix``,
+  ``generate_local_coulomb_matrix``, ``generate_atomic_coulomb_matrix``,
   ``generate_arad_descriptor`` (fml/fml.py)
 * ``gaussian_kernel``, ``laplacian_kernel``, ``get_atomic_kernels_arad``,
   ``get_atomic_symmetric_kernels_arad`` (fml/kernels/kernels.py) and the
   atom-level ``fget_atomic_kernels_arad`` / ``fget_atomic_distance_arad``
-  (fml/kernels/farad_kernels.f90)
-* ``cho_solve`` (fml/math/cho_solve.py)
+  and ``fget_alpha_arad`` (fml/kernels/farad_kernels.f90), ``get_atomic_kernels_gaussian``,
+  ``get_atomic_kernels_laplacian`` (fml/kernels/kernels.py)
+* ``cho_solve``, ``cho_invert`` (fml/math/cho_solve.py)
 
-Batched forms: ``generate_coulomb_matrices``, ``generate_arad_descriptors``.
+Batched forms: ``generate_coulomb_matrices``, ``generate_local_coulomb_matrices``,
+``generate_arad_descriptors``.
 
 All compute runs in libfmlb.so (hand-written CUDA for sm_100a) through its C
 ABI; torch is used for device buffers and streams only. There is no CPU
 fallback: without the built library or a CUDA device the calls raise.
 """
 
-from .cho_solve import CholeskyWarning, cho_solve
+from .cho_solve import CholeskyWarning, cho_invert, cho_solve
 from .data import NUCLEAR_CHARGE, PTP
-from .descriptors import generate_arad_descriptors, generate_coulomb_matrices
-from .kernels import (fget_atomic_distance_arad, fget_atomic_kernels_arad, gaussian_kernel,
-                      get_atomic_kernels_arad, get_atomic_symmetric_kernels_arad,
+from .descriptors import (generate_arad_descriptors, generate_coulomb_matrices,
+                          generate_local_coulomb_matrices)
+from .kernels import (fget_alpha_arad, fget_atomic_distance_arad, fget_atomic_kernels_arad,
+                      gaussian_kernel, get_atomic_kernels_arad, get_atomic_kernels_gaussian,
+                      get_atomic_kernels_laplacian, get_atomic_symmetric_kernels_arad,
                       laplacian_kernel)
 from .molecule import Molecule
 
 __all__ = [
     "Molecule", "gaussian_kernel", "laplacian_kernel", "get_atomic_kernels_arad",
-    "get_atomic_symmetric_kernels_arad", "fget_atomic_kernels_arad",
-    "fget_atomic_distance_arad", "cho_solve",
+    "get_atomic_symmetric_kernels_arad", "fget_atomic_kernels_arad", "fget_alpha_arad",
+    "fget_atomic_distance_arad", "get_atomic_kernels_gaussian", "get_atomic_kernels_laplacian",
+    "cho_solve", "cho_invert",
     "CholeskyWarning",
-    "generate_coulomb_matrices", "generate_arad_descriptors", "NUCLEAR_CHARGE", "PTP",
+    "generate_coulomb_matrices", "generate_local_coulomb_matrices", "generate_arad_descriptors",
+    "NUCLEAR_CHARGE", "PTP",
 ]

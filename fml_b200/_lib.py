@@ -24,6 +24,9 @@ SIGNATURES = {
     "fmlb_last_error_string": (ctypes.c_char_p, []),
     "fmlb_version": (_i, []),
     "fmlb_coulomb_matrices": (_i, [_vp, _vp, _vp, _i, _i, _vp, _i, _vp, _i, _vp, _vp, _vp]),
+    "fmlb_local_coulomb_matrices": (_i, [_vp, _vp, _vp, _i, _i, _i, _vp, _i, _vp, _vp]),
+    "fmlb_vector_kernels_f64": (_i, [_i, _vp, _vp, _i, _i, _vp, _vp, _i, _i, _i, _dp, _i, _vp,
+                                     _vp, _vp]),
     "fmlb_arad_descriptors": (_i, [_vp, _vp, _vp, _i, _i, _d, _vp, _vp, _vp]),
     "fmlb_gaussian_kernel_f64": (_i, [_vp, _i, _i, _vp, _i, _i, _i, _dp, _i, _vp, _ll, _ll, _i,
                                       _vp]),
@@ -33,12 +36,14 @@ SIGNATURES = {
     "fmlb_arad_kernels": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp, _i, _i, _dp, _i, _d, _d, _d, _d,
                                _i, _i, _vp, _vp, _sz, _vp]),
     "fmlb_arad_atomic_workspace_bytes": (_sz, [_i, _i, _i]),
+    "fmlb_arad_alpha_kernel_f64": (_i, [_vp, _vp, _vp, _i, _i, _d, _d, _vp, _vp, _sz, _vp]),
     "fmlb_arad_atomic_distances": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp, _i, _i, _d, _d, _d, _d,
                                         _vp, _vp, _sz, _vp]),
     "fmlb_arad_atomic_kernels": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp, _i, _i, _dp, _i, _d, _d,
                                       _d, _d, _vp, _vp, _sz, _vp]),
     "fmlb_potrf_workspace_bytes": (_sz, [_i]),
     "fmlb_potrf_f64": (_i, [_vp, _ll, _i, _vp, _vp, _vp]),
+    "fmlb_potri_f64": (_i, [_vp, _ll, _i, _vp, _vp, _ll, _vp, _vp]),
     "fmlb_potrs_f64": (_i, [_vp, _ll, _i, _vp, _vp, _vp]),
     "fmlb_syrk_lower_f64": (_i, [_vp, _ll, _i, _vp, _ll, _i, _i, _vp, _vp]),
     "fmlb_krr_refine_scratch_doubles": (_sz, [_i]),

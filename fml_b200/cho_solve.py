@@ -1,4 +1,4 @@
-"""``cho_solve``: drop-in for fml/math/cho_solve.py:33-58.
+"""``cho_solve`` / ``cho_invert``: drop-ins for fml/math/cho_solve.py:27-58.
 
 Solves ``A x = y`` by a Cholesky factorisation on the GPU (hand-written
 blocked FP64 factor + triangular solves, the replacement for the LAPACK
@@ -12,6 +12,14 @@ reads it. Difference: ``A`` is never modified (with a Fortran-ordered float64
 ``A`` the reference overwrites its upper triangle with the factor as an f2py
 side effect). ``strict=True`` raises ``numpy.linalg.LinAlgError`` instead of
 warning.
+
+``cho_invert`` (fcho_solve.f90:49-68, dpotrf('U') then dpotri('U')) returns
+what the reference returns: a Fortran-ordered array whose upper triangle
+(i <= j) holds inv(A) and whose strict lower triangle is A's, untouched by
+LAPACK. The inversion runs on the GPU from the same factor (``fmlb_potri_f64``).
+On a non-positive pivot the reference prints its DPOTRF warning and still runs
+dpotri on the partial factor; here the warning is the same and the inverse
+triangle is NaN (``strict=True`` raises).
 """
 
 import warnings
@@ -97,3 +105,31 @@ def cho_solve(A, y, strict=False, refine=0, return_residuals=False):
     if return_residuals:
         return out, resid.cpu().numpy()
     return out
+
+
+def cho_invert(A, strict=False):
+    """inv(A) of a symmetric positive-definite A, in the reference's layout."""
+    if len(A.shape) != 2 or A.shape[0] != A.shape[1]:
+        raise ValueError('expected square matrix')
+    n = A.shape[0]
+    Ad, as_np = _upper_as_rowmajor_lower(A)
+    if n == 0:
+        return to_output(Ad, as_np)
+    work, info = potrf(Ad, n)
+    ldv = n + (n & 1)  # even stride: 16-byte aligned rows for the tensor-core tiles
+    V = torch.empty((n, ldv), dtype=torch.float64, device=Ad.device)
+    _lib.call("fmlb_potri_f64", _lib.ptr(Ad), Ad.stride(0), n, _lib.ptr(work), _lib.ptr(V), ldv,
+              _lib.ptr(info), _lib.stream_handle())
+    del V
+    code = int(info.item())
+    if code > 0:
+        msg = "WARNING: Cholesky decomposition DPOTRF() exited with error code: %d" % code
+        if strict:
+            raise np.linalg.LinAlgError(msg)
+        warnings.warn(msg, CholeskyWarning, stacklevel=2)
+        Ad.masked_fill_(torch.ones_like(Ad, dtype=torch.bool).tril(), float("nan"))
+    # Ad's lower triangle is inv(A), its strict upper triangle A's strict lower
+    # one transposed: Ad is the row-major image of the result's Fortran layout.
+    if as_np:
+        return Ad.cpu().numpy().T
+    return Ad.t()

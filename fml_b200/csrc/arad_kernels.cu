@@ -31,6 +31,7 @@ struct SigmaTable {
 
 struct AradParams {
     double width, cut, rw2, cw2, inv_width, maxg2, inv_cut;
+    double eps;  // |l2| below eps counts as 0
 };
 
 // Per-set workspace views.
@@ -217,7 +218,7 @@ arad_pair_kernel(const double *__restrict__ X1, const double *__restrict__ Z1,
     const long long npairs = symmetric ? (long long)nm1 * (nm1 + 1) / 2 : (long long)nm1 * nm2;
     const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const double eps = (double)5.0e-12f;  // single-precision literal in the source (:505)
+    const double eps = P.eps;
     const float maxg2s = (float)(P.maxg2 * fp32_scale(P) * fp32_scale(P));
     const float rw2f = (float)P.rw2, cw2f = (float)P.cw2;
 
@@ -983,6 +984,7 @@ static int arad_atomic_impl(const double *Q1, const double *Z1, const int *N1, i
     P.inv_width = -1.0 / (4.0 * width * width);      // :58
     P.maxg2 = (8.0 * width) * (8.0 * width);          // :60
     P.inv_cut = (4.0 * atan(1.0)) / (2.0 * cut_distance);  // :828
+    P.eps = (double)5.0e-12f;                                // :823
     SigmaTable sig;
     for (int s = 0; s < (distance ? 0 : nsigma); ++s)
         sig.inv_sigma2[s] = -1.0 / (sigmas_host[s] * sigmas_host[s]);
@@ -1039,12 +1041,12 @@ extern "C" size_t fmlb_arad_workspace_bytes(int nm1, int nm2, int amax, int symm
            fmlb::align256(sizeof(fmlb::ClassInfo));
 }
 
-extern "C" int fmlb_arad_kernels(const double *X1, const double *Z1, const int *N1, int nm1,
-                                 const double *X2, const double *Z2, const int *N2, int nm2,
-                                 int amax, const double *sigmas_host, int nsigma, double width,
-                                 double cut_distance, double r_width, double c_width,
-                                 int symmetric, int precision, double *K, void *workspace,
-                                 size_t ws_bytes, void *stream) {
+static int arad_kernels_impl(const double *X1, const double *Z1, const int *N1, int nm1,
+                             const double *X2, const double *Z2, const int *N2, int nm2,
+                             int amax, const double *sigmas_host, int nsigma, double width,
+                             double cut_distance, double r_width, double c_width, int symmetric,
+                             int precision, double eps, double *K, void *workspace,
+                             size_t ws_bytes, void *stream) {
     using namespace fmlb;
     cudaStream_t st = FMLB_STREAM(stream);
     FMLB_REQUIRE(nm1 >= 0 && amax >= 1, "fmlb_arad_kernels: bad sizes");
@@ -1070,6 +1072,7 @@ extern "C" int fmlb_arad_kernels(const double *X1, const double *Z1, const int *
     P.inv_width = -1.0 / (4.0 * width * width);      // :58
     P.maxg2 = (8.0 * width) * (8.0 * width);          // :60
     P.inv_cut = (4.0 * atan(1.0)) / (2.0 * cut_distance);  // :502, :510
+    P.eps = eps;
 
     char *p = static_cast<char *>(workspace);
     SetWs w1 = carve(p, nm1, amax);
@@ -1141,4 +1144,32 @@ extern "C" int fmlb_arad_kernels(const double *X1, const double *Z1, const int *
         FMLB_TRY(launch_status("arad_pair_kernel"));
     }
     return FMLB_OK;
+}
+
+extern "C" int fmlb_arad_kernels(const double *X1, const double *Z1, const int *N1, int nm1,
+                                 const double *X2, const double *Z2, const int *N2, int nm2,
+                                 int amax, const double *sigmas_host, int nsigma, double width,
+                                 double cut_distance, double r_width, double c_width,
+                                 int symmetric, int precision, double *K, void *workspace,
+                                 size_t ws_bytes, void *stream) {
+    // eps: the single-precision literal 5.0e-12 of farad_kernels.f90:505 / :679
+    return arad_kernels_impl(X1, Z1, N1, nm1, X2, Z2, N2, nm2, amax, sigmas_host, nsigma, width,
+                             cut_distance, r_width, c_width, symmetric, precision,
+                             (double)5.0e-12f, K, workspace, ws_bytes, stream);
+}
+
+// The kernel matrix of fget_alpha_arad (farad_kernels.f90:231-393): the
+// symmetric FP64 ARAD kernel for one sigma with the routine's fixed
+// parameters (width 0.2, cut 6, r_width 1, c_width 0.5, :237-240) and its eps
+// (the single-precision literal 1.0e-11, :309), plus lambda on the diagonal
+// (:385-389).
+extern "C" int fmlb_arad_alpha_kernel_f64(const double *X, const double *Z, const int *N,
+                                          int nm, int amax, double sigma, double lambda,
+                                          double *K, void *workspace, size_t ws_bytes,
+                                          void *stream) {
+    using namespace fmlb;
+    FMLB_REQUIRE(sigma > 0.0, "fmlb_arad_alpha_kernel_f64: sigma must be positive");
+    FMLB_TRY(arad_kernels_impl(X, Z, N, nm, X, Z, N, nm, amax, &sigma, 1, 0.2, 6.0, 1.0, 0.5, 1,
+                               0, (double)1.0e-11f, K, workspace, ws_bytes, stream));
+    return fmlb_add_diagonal_f64(K, nm, nm, lambda, stream);
 }

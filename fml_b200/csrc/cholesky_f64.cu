@@ -176,22 +176,20 @@ potf2_block_kernel(double *__restrict__ A, long long lda, int k0, int kn,
 constexpr int TRSM_ROWS = 64;
 constexpr size_t kTrsmSmem = (size_t)(NB + TRSM_ROWS) * LDL * sizeof(double);
 
-__global__ void __launch_bounds__(TPB)
-panel_trsm_kernel(double *__restrict__ A, long long lda, int n, int k0, int kn,
-                  const double *__restrict__ Linv, const int *__restrict__ info) {
-    extern __shared__ double trsm_smem[];
-    double(*Li)[LDL] = reinterpret_cast<double(*)[LDL]>(trsm_smem);
-    double(*P)[LDL] = reinterpret_cast<double(*)[LDL]>(trsm_smem + NB * LDL);
-    if (failed(info)) return;
-    const int r0 = k0 + kn + blockIdx.x * TRSM_ROWS;
+// Rows [r0, r0 + TRSM_ROWS) (clipped to rend) of columns [k0, k0 + kn):
+// out[r][c] = sum_{k <= c} X[r][k] * Linv[c][k], in place.
+__device__ __forceinline__ void trsm_rows(double *__restrict__ A, long long lda, int r0, int rend,
+                                          int k0, int kn, const double *__restrict__ Linv,
+                                          double *smem) {
+    double(*Li)[LDL] = reinterpret_cast<double(*)[LDL]>(smem);
+    double(*P)[LDL] = reinterpret_cast<double(*)[LDL]>(smem + NB * LDL);
     const int tid = threadIdx.x;
     for (int t = tid; t < NB * NB; t += TPB) Li[t / NB][t % NB] = Linv[t];
     for (int t = tid; t < TRSM_ROWS * NB; t += TPB) {
         const int r = t / NB, c = t % NB;
-        P[r][c] = (r0 + r < n && c < kn) ? A[(size_t)(r0 + r) * lda + k0 + c] : 0.0;
+        P[r][c] = (r0 + r < rend && c < kn) ? A[(size_t)(r0 + r) * lda + k0 + c] : 0.0;
     }
     __syncthreads();
-    // out[r][c] = sum_{k <= c} P[r][k] * Linv[c][k]
     const int c = tid & (NB - 1), rq = tid / NB;  // 2 row groups of 32 rows
     double out[32];
 #pragma unroll
@@ -204,8 +202,26 @@ panel_trsm_kernel(double *__restrict__ A, long long lda, int n, int k0, int kn,
 #pragma unroll
     for (int i = 0; i < 32; ++i) {
         const int r = r0 + rq * 32 + i;
-        if (r < n && c < kn) A[(size_t)r * lda + k0 + c] = out[i];
+        if (r < rend && c < kn) A[(size_t)r * lda + k0 + c] = out[i];
     }
+}
+
+__global__ void __launch_bounds__(TPB)
+panel_trsm_kernel(double *__restrict__ A, long long lda, int n, int k0, int kn,
+                  const double *__restrict__ Linv, const int *__restrict__ info) {
+    extern __shared__ double trsm_smem[];
+    if (failed(info)) return;
+    trsm_rows(A, lda, k0 + kn + blockIdx.x * TRSM_ROWS, n, k0, kn, Linv, trsm_smem);
+}
+
+// Rows [0, rend) of columns [k0, k0 + kn): X <- X Linv^T (the inverse's
+// column-block step, section 5).
+__global__ void __launch_bounds__(TPB)
+rows_trsm_kernel(double *__restrict__ A, long long lda, int rend, int k0, int kn,
+                 const double *__restrict__ Linv, const int *__restrict__ info) {
+    extern __shared__ double trsm_smem[];
+    if (failed(info)) return;
+    trsm_rows(A, lda, blockIdx.x * TRSM_ROWS, rend, k0, kn, Linv, trsm_smem);
 }
 
 // ---- 3. trailing update on the FP64 tensor cores ---------------------------
@@ -600,6 +616,162 @@ backward_step_kernel(const double *__restrict__ L, long long lda, int k0, int kn
     }
 }
 
+// ---- 5. inverse from the factor (potri) ------------------------------------
+// inv(A) = L^-T L^-1 = V V^T with V = L^-T (upper triangular). V solves
+// V L^T = I column block by column block, right-looking:
+//   V[:, i] = U[:, i] Linv_ii^T                      (rows_trsm_kernel)
+//   U[:, j] -= V[:, i] L[j, i]^T for blocks j > i    (gemm_nt_dmma_kernel)
+// with U = I initially (only rows above block i+1 are non-zero). Then the
+// lower triangle of V V^T (gemm_nt_dmma_kernel, triangle mode, k from the
+// tile's first row on since V is upper triangular). 2n^3/3 flops, as LAPACK
+// dpotri; both products on the FP64 tensor cores with the trailing update's
+// tiles (128 x 64, DMMA m8n8k4, 3-stage cp.async).
+//
+// kTri = false: C (M x N) -= A B^T, A (M x K), B (N x K), all row-major.
+// kTri = true:  C (M x M, triangle c <= r) = A A^T with A upper triangular
+//               (B = A, the k-loop of row block r0 starts at r0).
+template <bool kAligned16, bool kTri>
+__global__ void __launch_bounds__(SY_TPB, 2)
+gemm_nt_dmma_kernel(double *__restrict__ C, long long ldc, int M, int N,
+                    const double *__restrict__ A, long long lda, const double *__restrict__ B,
+                    long long ldb, int K, int tiles_n, const int *__restrict__ info) {
+    extern __shared__ __align__(16) double sy_smem[];
+    if (failed(info)) return;
+    const long long t = blockIdx.x;
+    int by, bx;
+    if (kTri) {  // tile t -> (by, bx <= 2 by + 1), as the trailing update
+        by = (int)((sqrt(4.0 * (double)t + 1.0) - 1.0) * 0.5);
+        while ((long long)by * by + by > t) --by;
+        while ((long long)(by + 1) * (by + 1) + (by + 1) <= t) ++by;
+        bx = (int)(t - (long long)by * by - by);
+    } else {
+        by = (int)(t / tiles_n);
+        bx = (int)(t % tiles_n);
+    }
+    const int row0 = by * SY_TM, col0 = bx * SY_TN;
+    if (row0 >= M || col0 >= N) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wr = warp >> 1, wc = warp & 1;
+    const int g = lane >> 2, tq = lane & 3;
+
+    double acc[8][4][2];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+    const int kt0 = kTri ? row0 / SY_TK : 0;  // row0 is a multiple of SY_TK
+    const int nk = (K + SY_TK - 1) / SY_TK;
+#pragma unroll
+    for (int s = 0; s < SY_STAGES - 1; ++s) {
+        if (kt0 + s < nk) {
+            double *st = sy_smem + s * SY_STAGE_DOUBLES;
+            syrk_load_tile<SY_TM, kAligned16>(st, A, lda, M, K, row0, (kt0 + s) * SY_TK);
+            syrk_load_tile<SY_TN, kAligned16>(st + SY_TM * SY_LD, B, ldb, N, K, col0,
+                                              (kt0 + s) * SY_TK);
+        }
+        cp_async_commit();
+    }
+    for (int kt = kt0; kt < nk; ++kt) {
+        cp_async_wait<SY_STAGES - 2>();
+        __syncthreads();
+        const int nxt = kt + SY_STAGES - 1;
+        if (nxt < nk) {
+            double *st = sy_smem + ((nxt - kt0) % SY_STAGES) * SY_STAGE_DOUBLES;
+            syrk_load_tile<SY_TM, kAligned16>(st, A, lda, M, K, row0, nxt * SY_TK);
+            syrk_load_tile<SY_TN, kAligned16>(st + SY_TM * SY_LD, B, ldb, N, K, col0,
+                                              nxt * SY_TK);
+        }
+        cp_async_commit();
+        const double *As = sy_smem + ((kt - kt0) % SY_STAGES) * SY_STAGE_DOUBLES;
+        const double *Bs = As + SY_TM * SY_LD;
+#pragma unroll
+        for (int kk = 0; kk < SY_TK / 4; ++kk) {
+            double a[8], b[4];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) a[i] = As[(wr * 64 + i * 8 + g) * SY_LD + kk * 4 + tq];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[(wc * 32 + j * 8 + g) * SY_LD + kk * 4 + tq];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j], a[i], b[j]);
+        }
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    double *Cs = sy_smem;  // SY_TM x SY_CLD
+    const int tid = threadIdx.x;
+    for (int e = tid; e < SY_TM * (SY_TN / 2); e += SY_TPB) {
+        const int r = e / (SY_TN / 2), c = (e % (SY_TN / 2)) * 2;
+        const int gr = row0 + r, gc = col0 + c;
+        double v0 = 0.0, v1 = 0.0;
+        if (!kTri && gr < M) {
+            const double *src = C + (size_t)gr * ldc + gc;
+            if (gc < N) v0 = src[0];
+            if (gc + 1 < N) v1 = src[1];
+        }
+        Cs[r * SY_CLD + c] = v0;
+        Cs[r * SY_CLD + c + 1] = v1;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int rl = wr * 64 + i * 8 + g;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int cl = wc * 32 + j * 8 + 2 * tq;
+            if (kTri) {
+                Cs[rl * SY_CLD + cl] += acc[i][j][0];
+                Cs[rl * SY_CLD + cl + 1] += acc[i][j][1];
+            } else {
+                Cs[rl * SY_CLD + cl] -= acc[i][j][0];
+                Cs[rl * SY_CLD + cl + 1] -= acc[i][j][1];
+            }
+        }
+    }
+    __syncthreads();
+    for (int e = tid; e < SY_TM * (SY_TN / 2); e += SY_TPB) {
+        const int r = e / (SY_TN / 2), c = (e % (SY_TN / 2)) * 2;
+        const int gr = row0 + r, gc = col0 + c;
+        if (gr >= M) continue;
+        double *dst = C + (size_t)gr * ldc + gc;
+        if (gc < N && (!kTri || gc <= gr)) dst[0] = Cs[r * SY_CLD + c];
+        if (gc + 1 < N && (!kTri || gc + 1 <= gr)) dst[1] = Cs[r * SY_CLD + c + 1];
+    }
+}
+
+template <bool kTri>
+int launch_gemm_nt(double *C, long long ldc, int M, int N, const double *A, long long lda,
+                   const double *B, long long ldb, int K, const int *info, cudaStream_t st) {
+    if (M <= 0 || N <= 0 || K <= 0) return FMLB_OK;
+    const bool al = (uintptr_t)A % 16 == 0 && lda % 2 == 0 && (uintptr_t)B % 16 == 0 &&
+                    ldb % 2 == 0;
+    const long long Tr = ceil_div(M, SY_TM);
+    const int tiles_n = ceil_div(N, SY_TN);
+    const long long ntiles = kTri ? Tr * Tr + Tr : Tr * tiles_n;
+    if (al) {
+        FMLB_TRY(cuda_status(cudaFuncSetAttribute(gemm_nt_dmma_kernel<true, kTri>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)kSyrkSmem), "gemm smem attribute"));
+        gemm_nt_dmma_kernel<true, kTri><<<(unsigned)ntiles, SY_TPB, kSyrkSmem, st>>>(
+            C, ldc, M, N, A, lda, B, ldb, K, tiles_n, info);
+    } else {
+        FMLB_TRY(cuda_status(cudaFuncSetAttribute(gemm_nt_dmma_kernel<false, kTri>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)kSyrkSmem), "gemm smem attribute"));
+        gemm_nt_dmma_kernel<false, kTri><<<(unsigned)ntiles, SY_TPB, kSyrkSmem, st>>>(
+            C, ldc, M, N, A, lda, B, ldb, K, tiles_n, info);
+    }
+    return launch_status("gemm_nt_dmma_kernel");
+}
+
+// V = I on the leading (n, n) block of a row-major buffer with stride ldv
+__global__ void identity_kernel(double *__restrict__ V, long long ldv, int n) {
+    const int r = blockIdx.y, c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n && c < n) V[(size_t)r * ldv + c] = (r == c) ? 1.0 : 0.0;
+}
+
 int set_smem_attrs() {
     static int attr_dev = -1;
     int dev = 0;
@@ -609,6 +781,9 @@ int set_smem_attrs() {
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)kPotf2Smem), "potf2 smem attribute"));
     FMLB_TRY(cuda_status(cudaFuncSetAttribute(panel_trsm_kernel,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)kTrsmSmem), "trsm smem attribute"));
+    FMLB_TRY(cuda_status(cudaFuncSetAttribute(rows_trsm_kernel,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)kTrsmSmem), "trsm smem attribute"));
     attr_dev = dev;
@@ -787,4 +962,28 @@ extern "C" int fmlb_syrk_lower_f64(double *C, long long ldc, int m, const double
     if (m == 0 || k == 0) return FMLB_OK;
     FMLB_REQUIRE(C && P, "fmlb_syrk_lower_f64: null pointer");
     return launch_syrk(C, ldc, m, P, ldp, k, info, FMLB_STREAM(stream), strip_cols);
+}
+
+extern "C" int fmlb_potri_f64(double *A, long long lda, int n, const void *work, double *V,
+                              long long ldv, const int *info, void *stream) {
+    using namespace fmlb;
+    cudaStream_t st = FMLB_STREAM(stream);
+    FMLB_REQUIRE(n >= 0 && lda >= n && ldv >= n, "fmlb_potri_f64: bad n=%d / lda / ldv", n);
+    if (n == 0) return FMLB_OK;
+    FMLB_REQUIRE(A && work && V, "fmlb_potri_f64: null pointer");
+    FMLB_REQUIRE(n <= 65535, "fmlb_potri_f64: n=%d above 65535", n);
+    FMLB_TRY(set_smem_attrs());
+    const double *Linv = static_cast<const double *>(work);
+    identity_kernel<<<dim3(ceil_div(n, 256), n), 256, 0, st>>>(V, ldv, n);
+    FMLB_TRY(launch_status("identity_kernel"));
+    for (int k0 = 0, kb = 0; k0 < n; k0 += NB, ++kb) {
+        const int kn = std::min(NB, n - k0), R = k0 + kn;
+        rows_trsm_kernel<<<ceil_div(R, TRSM_ROWS), TPB, kTrsmSmem, st>>>(
+            V, ldv, R, k0, kn, Linv + (size_t)kb * NB * NB, info);
+        FMLB_TRY(launch_status("rows_trsm_kernel"));
+        if (R < n)
+            FMLB_TRY(launch_gemm_nt<false>(V + R, ldv, R, n - R, V + k0, ldv,
+                                           A + (size_t)R * lda + k0, lda, kn, info, st));
+    }
+    return launch_gemm_nt<true>(A, lda, n, n, V, ldv, V, ldv, n, info, st);
 }

@@ -44,6 +44,17 @@ __device__ __forceinline__ double cm_pair(const double *X, const double *Y, cons
     return __ddiv_rn(__dmul_rn(Q[a], Q[b]), __dsqrt_rn(s));
 }
 
+// |R_b - R_a| for a < b (the distance matrix of frepresentations.f90:336-342)
+__device__ __forceinline__ double cm_dist(const double *X, const double *Y, const double *Zc,
+                                          int a, int b) {
+    if (a > b) { int t = a; a = b; b = t; }
+    double dx = __dsub_rn(X[b], X[a]);
+    double dy = __dsub_rn(Y[b], Y[a]);
+    double dz = __dsub_rn(Zc[b], Zc[a]);
+    return __dsqrt_rn(
+        __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+}
+
 // One warp per molecule.
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 cm_sorted_kernel(const double *__restrict__ charges, const double *__restrict__ coords,
@@ -111,6 +122,101 @@ cm_sorted_kernel(const double *__restrict__ charges, const double *__restrict__ 
         for (int idx = L + lane; idx < ldcm32; idx += 32) frow[idx] = 0.0f;
     if (order)
         for (int p = lane; p < nmax; p += 32) order[(size_t)mol * nmax + p] = p < n ? S[p] : -1;
+}
+
+// ---------------------------------------------------------------------------
+// Local and atomic Coulomb matrices, one row per atom: the packed lower
+// triangle of the molecule's Coulomb matrix with the atoms reordered around
+// the central atom k.
+//   kind 0, fgenerate_local_coulomb_matrix (frepresentations.f90:204-294):
+//     k first, then the others in the row-norm order of the sorted matrix
+//     (descending norm, ties -> higher index first, :262-277);
+//   kind 1, fgenerate_atomic_coulomb_matrix (:297-390): every atom by its
+//     distance to k, ascending, ties -> lower index first (minloc, :366-371).
+// One warp per molecule; FP64 in the reference's operation order.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+cm_local_kernel(const double *__restrict__ charges, const double *__restrict__ coords,
+                const int *__restrict__ offsets, int nmol, int nmax, int kind,
+                double *__restrict__ cm, int ldcm, DiagTable diag, int *__restrict__ status) {
+    extern __shared__ double smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mol = blockIdx.x * kWarpsPerBlock + warp;
+    if (mol >= nmol) return;
+    const int per_warp = 5 * nmax + nmax;  // X Y Z Q N (doubles) + S, O (ints)
+    double *X = smem + warp * per_warp;
+    double *Y = X + nmax, *Zc = Y + nmax, *Q = Zc + nmax, *N = Q + nmax;
+    int *S = reinterpret_cast<int *>(N + nmax), *O = S + nmax;
+    const int a0 = offsets[mol];
+    const int n = offsets[mol + 1] - a0;
+    const int L = nmax * (nmax + 1) / 2;
+    if (n < 0 || n > nmax) {  // rejected on the host; stay in bounds regardless
+        if (lane == 0 && status) atomicCAS(status, 0, 1);
+        return;
+    }
+    for (int t = lane; t < n; t += 32) {
+        X[t] = coords[3 * (size_t)(a0 + t) + 0];
+        Y[t] = coords[3 * (size_t)(a0 + t) + 1];
+        Zc[t] = coords[3 * (size_t)(a0 + t) + 2];
+        Q[t] = charges[a0 + t];
+    }
+    __syncwarp();
+    if (kind == 0) {
+        // row norms (:238-259: diagonal, then every other atom in index order)
+        for (int i = lane; i < n; i += 32) {
+            double s = cm_diag(Q[i], diag);
+            for (int j = 0; j < n; ++j)
+                if (j != i) s = __dadd_rn(s, cm_pair(X, Y, Zc, Q, i, j));
+            N[i] = s;
+        }
+        __syncwarp();
+        for (int i = lane; i < n; i += 32) {
+            const double ni = isnan(N[i]) ? -INFINITY : N[i];
+            int r = 0;
+            for (int j = 0; j < n; ++j) {
+                const double nj = isnan(N[j]) ? -INFINITY : N[j];
+                r += (nj > ni) || (nj == ni && j > i);
+            }
+            S[r] = i;
+        }
+        __syncwarp();
+    }
+    for (int k = 0; k < n; ++k) {
+        if (kind == 0) {  // k, then the sorted atoms without k (:268-277)
+            for (int t = lane; t < n; t += 32) {
+                if (t == 0) {
+                    O[0] = k;
+                } else {
+                    int pos = 0;  // position of k in the sorted order
+                    while (S[pos] != k) ++pos;
+                    O[t] = S[t - 1 + (t - 1 >= pos ? 1 : 0)];
+                }
+            }
+        } else {  // ascending distance to k, ties -> lower index (:366-371)
+            for (int i = lane; i < n; i += 32) {
+                const double di = i == k ? 0.0 : cm_dist(X, Y, Zc, i, k);
+                int r = 0;
+                for (int j = 0; j < n; ++j) {
+                    const double dj = j == k ? 0.0 : cm_dist(X, Y, Zc, j, k);
+                    r += (dj < di) || (dj == di && j < i);
+                }
+                O[r] = i;
+            }
+        }
+        __syncwarp();
+        double *row = cm + (size_t)(a0 + k) * ldcm;
+        for (int idx = lane; idx < L; idx += 32) {
+            int m = (int)((sqrt(8.0 * idx + 1.0) - 1.0) * 0.5);
+            while (m * (m + 1) / 2 > idx) --m;
+            while ((m + 1) * (m + 2) / 2 <= idx) ++m;
+            const int q = idx - m * (m + 1) / 2;
+            double v = 0.0;
+            if (m < n) v = (q == m) ? cm_diag(Q[O[m]], diag) : cm_pair(X, Y, Zc, Q, O[m], O[q]);
+            row[idx] = v;
+        }
+        for (int idx = L + lane; idx < ldcm; idx += 32) row[idx] = 0.0;
+        __syncwarp();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -324,6 +430,27 @@ extern "C" int fmlb_coulomb_matrices(const double *charges, const double *coords
                        FMLB_STREAM(stream)>>>(charges, coords, offsets, nmol, nmax, cm, ldcm,
                                               cm32, ldcm32, order, diag, status);
     return launch_status("cm_sorted_kernel");
+}
+
+extern "C" int fmlb_local_coulomb_matrices(const double *charges, const double *coords,
+                                           const int *offsets, int nmol, int nmax, int kind,
+                                           double *cm, int ldcm, int *status, void *stream) {
+    using namespace fmlb;
+    FMLB_REQUIRE(nmol >= 0, "fmlb_local_coulomb_matrices: nmol < 0");
+    FMLB_REQUIRE(nmax >= 1 && nmax <= 255, "fmlb_local_coulomb_matrices: nmax=%d outside 1..255",
+                 nmax);
+    FMLB_REQUIRE(kind == 0 || kind == 1, "fmlb_local_coulomb_matrices: kind must be 0 or 1");
+    const int L = nmax * (nmax + 1) / 2;
+    FMLB_REQUIRE(ldcm >= L, "fmlb_local_coulomb_matrices: ldcm=%d < %d", ldcm, L);
+    FMLB_REQUIRE(nmol == 0 || (charges && coords && offsets && cm),
+                 "fmlb_local_coulomb_matrices: null pointer");
+    if (nmol == 0) return FMLB_OK;
+    static const DiagTable diag = make_diag_table();
+    const size_t smem = sizeof(double) * (5 * nmax + nmax) * kWarpsPerBlock;
+    cm_local_kernel<<<ceil_div(nmol, kWarpsPerBlock), kWarpsPerBlock * 32, smem,
+                      FMLB_STREAM(stream)>>>(charges, coords, offsets, nmol, nmax, kind, cm, ldcm,
+                                             diag, status);
+    return launch_status("cm_local_kernel");
 }
 
 extern "C" int fmlb_arad_descriptors(const double *charges, const double *coords,

@@ -4,6 +4,11 @@
 * ``laplacian_kernel(A, B, sigma)`` -> flaplacian_kernel (fkernels.f90:351-377)
 * ``get_atomic_kernels_arad`` / ``get_atomic_symmetric_kernels_arad``
   -> fget_kernels_arad / fget_symmetric_kernels_arad (farad_kernels.f90:439-755)
+* ``get_atomic_kernels_gaussian`` / ``get_atomic_kernels_laplacian`` ->
+  fget_vector_kernels_gaussian / fget_vector_kernels_laplacian
+  (fkernels.f90:23-162), sums over atom pairs of per-atom descriptors
+* ``fget_alpha_arad`` -> the routine of that name (farad_kernels.f90:231-436):
+  explicit-inverse ARAD KRR weights
 * ``fget_atomic_kernels_arad`` / ``fget_atomic_distance_arad`` -> the
   atom-level routines of the same names (farad_kernels.f90:757-1030), which
   fml.kernels exports directly
@@ -21,10 +26,13 @@ reference returns Fortran order; values are the same), and
 :348, and raises NameError).
 """
 
+import warnings
+
 import numpy as np
 import torch
 
 from . import _lib
+from .cho_solve import CholeskyWarning, potrf
 from ._tensors import device, is_torch, to_device, to_output, workspace
 from .data import ptp_of
 
@@ -270,6 +278,64 @@ def fget_atomic_distance_arad(q1, q2, z1, z2, n1, n2, na1, na2, width, cut_dista
     return to_output(D.t().contiguous(), not is_torch(q1))
 
 
+def fget_alpha_arad(q, z, n, y, sigma, lambda_, alpha=None):
+    """Explicit-inverse ARAD KRR weights, the routine fml.kernels exports from
+    its Fortran (farad_kernels.f90:231-436; the f2py argument order is kept).
+
+    q (nm, amax, 5, amax) ARAD descriptors, z (nm, amax, 2) PTP rows/columns,
+    n (nm,) atom counts, y (nm,) properties. Builds K + lambda I (the routine's
+    fixed ARAD parameters), inverts it from its Cholesky factor (dpotrf +
+    dpotri) and multiplies by y (dsymv), all on the GPU; every atom of
+    molecule j gets inv(K + lambda I)[j] . y. ``alpha`` (sum(n),) is filled in
+    place as f2py's intent(inout) does; without it a new array is returned.
+    A non-positive pivot prints the reference's DPOTRF warning as a
+    CholeskyWarning, and the weights are NaN.
+    """
+    qa = q if is_torch(q) else np.asarray(q, dtype=np.float64)
+    if qa.ndim != 4 or qa.shape[2] != 5 or qa.shape[3] != qa.shape[1]:
+        raise ValueError("q must be (nm, amax, 5, amax)")
+    nm, amax = qa.shape[0], qa.shape[1]
+    nn = np.asarray(n.cpu() if is_torch(n) else n, dtype=np.int32).reshape(-1)
+    if len(nn) != nm or (nm and (nn.min() < 0 or nn.max() > amax)):
+        raise ValueError("n must hold nm atom counts in 0..amax")
+    if len(y) != nm:
+        raise ValueError("y must hold one value per molecule")
+    x, _ = to_device(qa, torch.float64)
+    zd, _ = to_device(z if is_torch(z) else np.asarray(z, dtype=np.float64), torch.float64)
+    nd, _ = to_device(nn, torch.int32)
+    yd, _ = to_device(y if is_torch(y) else np.asarray(y, dtype=np.float64), torch.float64)
+    dev = device()
+    K = torch.empty((nm, nm), dtype=torch.float64, device=dev)
+    ws = workspace(_lib.load().fmlb_arad_workspace_bytes(nm, nm, amax, 1))
+    _lib.call("fmlb_arad_alpha_kernel_f64", _lib.ptr(x), _lib.ptr(zd), _lib.ptr(nd), nm, amax,
+              float(sigma), float(lambda_), _lib.ptr(K), _lib.ptr(ws), ws.numel(),
+              _lib.stream_handle())
+    del ws
+    work, info = potrf(K, nm)
+    ldv = nm + (nm & 1)
+    V = torch.empty((nm, ldv), dtype=torch.float64, device=dev)
+    _lib.call("fmlb_potri_f64", _lib.ptr(K), nm, nm, _lib.ptr(work), _lib.ptr(V), ldv,
+              _lib.ptr(info), _lib.stream_handle())
+    del V
+    _lib.call("fmlb_symmetrize_lower_f64", _lib.ptr(K), nm, nm, _lib.stream_handle())
+    ltcly = torch.empty(nm, dtype=torch.float64, device=dev)
+    _lib.call("fmlb_gemv_f64", _lib.ptr(K), nm, nm, nm, _lib.ptr(yd), _lib.ptr(ltcly),
+              _lib.stream_handle())
+    code = int(info.item())
+    vals = np.repeat(ltcly.cpu().numpy(), nn)  # :407-432, molecule value per atom
+    if code > 0:
+        warnings.warn("WARNING: Cholesky decomposition DPOTRF() exited with error code: %d"
+                      % code, CholeskyWarning, stacklevel=2)
+        vals[:] = np.nan
+    if alpha is None:
+        return vals
+    if len(alpha) < len(vals):
+        raise ValueError("alpha must hold sum(n) = %d entries" % len(vals))
+    alpha[:] = 0.0
+    alpha[:len(vals)] = vals
+    return None
+
+
 def get_atomic_kernels_arad(X1, X2, Z1, Z2, sigmas, width=0.2, cut_distance=6.0, r_width=1.0,
                             c_width=0.5, precision="fp64"):
     """Kernels (nsigma, nm1, nm2) between two sets of ARAD descriptors."""
@@ -291,3 +357,82 @@ def get_atomic_symmetric_kernels_arad(X1, Z1, sigmas, width=0.2, cut_distance=6.
     assert X1.shape[0] == len(Z1), "ERROR: Check ARAD decriptor sizes! code = 4"
     return _arad(X1, None, Z1, None, sigmas, width, cut_distance, r_width, c_width, True,
                  precision)
+
+
+def _vector_kernels(kind, x1, x2, n1, n2, sigmas):
+    """x1 (nm1, amax1, d), x2 (nm2, amax2, d) float64 rows -> (nsig, nm1, nm2)."""
+    sig, _ = _sigma_list(sigmas)
+    if len(sig) > 32:
+        raise ValueError("at most 32 sigmas per call")
+    if any(v <= 0.0 for v in sig):
+        raise ValueError("sigmas must be positive")
+    nm1, amax1, d = x1.shape
+    nm2, amax2, d2 = x2.shape
+    if d != d2:
+        raise ValueError("descriptor sizes differ: %d vs %d" % (d, d2))
+    n1 = np.asarray(n1, dtype=np.int32).reshape(-1)
+    n2 = np.asarray(n2, dtype=np.int32).reshape(-1)
+    if len(n1) != nm1 or len(n2) != nm2:
+        raise ValueError("atom-count lists do not match the number of molecules")
+    for n, amax in ((n1, amax1), (n2, amax2)):
+        if len(n) and (n.min() < 0 or n.max() > amax):
+            raise ValueError("atom counts must lie in 0..%d" % amax)
+    if max(amax1, amax2) > 128:
+        raise ValueError("at most 128 atoms per molecule")
+    dev = device()
+    K = torch.empty((len(sig), nm1, nm2), dtype=torch.float64, device=dev)
+    if nm1 == 0 or nm2 == 0:
+        return K
+    n1d = torch.from_numpy(n1).to(dev)
+    n2d = torch.from_numpy(n2).to(dev)
+    sig_p, _keep = _lib.host_doubles(sig)
+    _lib.call("fmlb_vector_kernels_f64", kind, _lib.ptr(x1), _lib.ptr(n1d), nm1, max(amax1, 1),
+              _lib.ptr(x2), _lib.ptr(n2d), nm2, max(amax2, 1), d, sig_p, len(sig),
+              _lib.ptr(K), None, _lib.stream_handle())
+    return K
+
+
+def _atom_rows(x):
+    """(d, amax, nm) reference layout, x[f, ia, i] -> (nm, amax, d) on the device."""
+    if is_torch(x):
+        t = x.to(device=device(), dtype=torch.float64)
+        return t.permute(2, 1, 0).contiguous(), False
+    a = np.asarray(x, dtype=np.float64)
+    if a.ndim != 3:
+        raise ValueError("expected a 3-D descriptor array (d, amax, nm)")
+    rows, _ = to_device(np.ascontiguousarray(a.transpose(2, 1, 0)), torch.float64)
+    return rows, True
+
+
+def get_atomic_kernels_laplacian(x1, x2, N1, N2, sigmas):
+    """kernels.py:351-363 -> (nsigmas, nm1, nm2) float64.
+
+    ``x1``/``x2`` are (d, amax, nm) (x[f, ia, i], the reference's Fortran
+    argument layout); ``N1``/``N2`` the atoms per molecule.
+    K[k, i, j] = sum over atom pairs of exp(-|x1_ia - x2_ja|_1 / sigma_k).
+    """
+    a, as_np = _atom_rows(x1)
+    b = a if x2 is x1 else _atom_rows(x2)[0]
+    return to_output(_vector_kernels(1, a, b, N1, N2, sigmas), as_np)
+
+
+def _local_cm_rows(mols):
+    n = np.array([m.natoms for m in mols], dtype=np.int32)
+    amax = int(n.max()) if len(n) else 1
+    size = mols[0].local_coulomb_matrix.shape[1]
+    x = np.zeros((len(mols), amax, size), dtype=np.float64)
+    for i, m in enumerate(mols):
+        x[i, :n[i], :size] = np.asarray(m.local_coulomb_matrix)
+    return to_device(x, torch.float64)[0], n
+
+
+def get_atomic_kernels_gaussian(mols1, mols2, sigmas):
+    """kernels.py:379-411 -> (nsigmas, nm1, nm2) float64 numpy.
+
+    Uses each molecule's ``local_coulomb_matrix`` (``Molecule.
+    generate_local_coulomb_matrix``). K[k, i, j] = sum over atom pairs of
+    exp(-|x1_ia - x2_ja|^2 / (2 sigma_k^2)).
+    """
+    a, n1 = _local_cm_rows(mols1)
+    b, n2 = (a, n1) if mols2 is mols1 else _local_cm_rows(mols2)
+    return to_output(_vector_kernels(0, a, b, n1, n2, sigmas), True)

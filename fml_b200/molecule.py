@@ -9,7 +9,8 @@ molecules use ``fml_b200.generate_coulomb_matrices`` /
 import numpy as np
 
 from .data import NUCLEAR_CHARGE
-from .descriptors import generate_arad_descriptors, generate_coulomb_matrices
+from .descriptors import (generate_arad_descriptors, generate_coulomb_matrices,
+                          generate_local_coulomb_matrices)
 
 
 class Molecule:
@@ -41,6 +42,21 @@ class Molecule:
         """fml/fml.py:64-66 -> sorted CM, packed lower triangle (size*(size+1)/2,)."""
         z, r, off = self._packed()
         self.coulomb_matrix = generate_coulomb_matrices(z, r, off, size=size)[0]
+
+    def generate_local_coulomb_matrix(self, calc="all", size=23):
+        """fml/fml.py:72-74 -> (natoms, size*(size+1)/2), one row per central atom.
+
+        ``calc`` is accepted and ignored, as in the reference.
+        """
+        z, r, off = self._packed()
+        self.local_coulomb_matrix = generate_local_coulomb_matrices(z, r, off, size=size,
+                                                                    kind="local")
+
+    def generate_atomic_coulomb_matrix(self, calc="all", size=23):
+        """fml/fml.py:76-78 -> (natoms, size*(size+1)/2), atoms by distance to the centre."""
+        z, r, off = self._packed()
+        self.atomic_coulomb_matrix = generate_local_coulomb_matrices(z, r, off, size=size,
+                                                                     kind="atomic")
 
     def generate_arad_descriptor(self, size=23):
         """fml/fml.py:80-86 -> ARAD descriptor (size, 5, size), cut 5.0 (fml/arad.py:36)."""

@@ -65,6 +65,42 @@ int fmlb_coulomb_matrices(const double *charges, const double *coords, const int
                           int *order, int *status, void *stream);
 
 /* ------------------------------------------------------------------------
+ * Local / atomic Coulomb matrices: one packed lower-triangle row per atom.
+ * Replaces fgenerate_local_coulomb_matrix (kind 0,
+ * fml/representations/frepresentations.f90:204-294) and
+ * fgenerate_atomic_coulomb_matrix (kind 1, :297-390), as called by
+ * Molecule.generate_local_coulomb_matrix / generate_atomic_coulomb_matrix,
+ * fml/fml.py:72-78.
+ *
+ *   cm   (total_atoms, ldcm) float64, row offsets[m] + k holds the matrix of
+ *        central atom k of molecule m, nmax(nmax+1)/2 entries, zero padded.
+ *        kind 0: k first, then the other atoms by descending row norm;
+ *        kind 1: all atoms by ascending distance to k.
+ *   status device int (may be NULL): 1 if a molecule has more than nmax atoms.
+ * ---------------------------------------------------------------------- */
+int fmlb_local_coulomb_matrices(const double *charges, const double *coords, const int *offsets,
+                                int nmol, int nmax, int kind, double *cm, int ldcm, int *status,
+                                void *stream);
+
+/* ------------------------------------------------------------------------
+ * Atomic vector kernels over per-atom descriptors.
+ * Replaces fget_vector_kernels_gaussian (kind 0, fml/kernels/fkernels.f90:106-162)
+ * and fget_vector_kernels_laplacian (kind 1, :23-104), as called by
+ * get_atomic_kernels_gaussian / get_atomic_kernels_laplacian,
+ * fml/kernels/kernels.py:351-411.
+ *
+ *   X1 (nm1, amax1, d), X2 (nm2, amax2, d) float64 device; N1/N2 atom counts.
+ *   K  (nsig, nm1, nm2): sum over atom pairs of exp(c_k * dist), dist the
+ *      squared L2 (kind 0, c_k = -0.5/sigma_k^2) or the L1 distance (kind 1,
+ *      c_k = -1/sigma_k).
+ *   sigmas_host host array of nsig (1..32) values; amax1, amax2 1..128.
+ * ---------------------------------------------------------------------- */
+int fmlb_vector_kernels_f64(int kind, const double *X1, const int *N1, int nm1, int amax1,
+                            const double *X2, const int *N2, int nm2, int amax2, int d,
+                            const double *sigmas_host, int nsig, double *K, int *status,
+                            void *stream);
+
+/* ------------------------------------------------------------------------
  * ARAD descriptors for a packed ragged batch of molecules.
  * Replaces ARAD.describe, fml/arad.py:70-145 (non-periodic path), as called
  * by Molecule.generate_arad_descriptor, fml/fml.py:80-86.
@@ -148,6 +184,16 @@ int fmlb_arad_kernels(const double *X1, const double *Z1, const int *N1, int nm1
                       double r_width, double c_width, int symmetric, int precision, double *K,
                       void *workspace, size_t ws_bytes, void *stream);
 
+/* The regularised kernel matrix of fget_alpha_arad (fml/kernels/
+ * farad_kernels.f90:231-389): K (nm, nm) = the symmetric FP64 ARAD kernel for
+ * one sigma with that routine's fixed width 0.2, cut 6, r_width 1, c_width 0.5
+ * and eps 1e-11, plus lambda on the diagonal. X, Z, N and the workspace as
+ * for fmlb_arad_kernels (fmlb_arad_workspace_bytes(nm, nm, amax, 1)). The
+ * rest of the routine is fmlb_potrf_f64, fmlb_potri_f64 and fmlb_gemv_f64. */
+int fmlb_arad_alpha_kernel_f64(const double *X, const double *Z, const int *N, int nm, int amax,
+                               double sigma, double lambda, double *K, void *workspace,
+                               size_t ws_bytes, void *stream);
+
 /* ------------------------------------------------------------------------
  * Cholesky factorisation and solve, FP64.
  * Replace LAPACK dpotrf('U') / dpotrs('U') as called by fcho_solve,
@@ -168,6 +214,20 @@ size_t fmlb_potrf_workspace_bytes(int n);
 int fmlb_potrf_f64(double *A, long long lda, int n, void *work, int *info, void *stream);
 int fmlb_potrs_f64(const double *L, long long lda, int n, const void *work, double *x,
                    void *stream);
+
+/* Inverse from the factor, the replacement for LAPACK dpotri('U') after
+ * dpotrf('U') as fcho_invert calls them (fml/math/fcho_solve.f90:49-68,
+ * wrapper cho_invert, fml/math/cho_solve.py:27-30).
+ *
+ *   A     the factor from fmlb_potrf_f64 (triangle i >= j); on return that
+ *         triangle holds inv(A). The other triangle is not touched.
+ *   work  the fmlb_potrf_f64 workspace (inverted diagonal blocks).
+ *   V     device scratch (n, ldv), ldv >= n: receives L^-T.
+ *   info  the fmlb_potrf_f64 info (device, may be NULL): when non-zero the
+ *         inversion is skipped.
+ * n <= 65535. */
+int fmlb_potri_f64(double *A, long long lda, int n, const void *work, double *V, long long ldv,
+                   const int *info, void *stream);
 
 /* Trailing update of the blocked factorisation: C -= P P^T on the triangle
  * i >= j of the row-major (m, m) matrix C, P is (m, k) with stride ldp; the

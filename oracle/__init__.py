@@ -47,6 +47,7 @@ def _lib():
         lib = ctypes.CDLL(path)
         lib.orc_cm_sorted.restype = ctypes.c_int
         lib.orc_cm_sorted_batch.restype = ctypes.c_int
+        lib.orc_cm_local_batch.restype = ctypes.c_int
         lib.orc_potrf_upper.restype = ctypes.c_int
         lib.orc_num_threads.restype = ctypes.c_int
         _LIB = lib
@@ -91,6 +92,36 @@ def coulomb_matrices(charges, coords, offsets, size=23, return_order=False):
     if rc:
         raise ValueError("molecule has more atoms than size")
     return (cm, order) if return_order else cm
+
+
+def local_coulomb_matrices(charges, coords, offsets, size=23, kind="local"):
+    """Per-atom CMs (total_atoms, size*(size+1)/2): frepresentations.f90:204-294
+    (kind "local") and :297-390 (kind "atomic"), restated in oracle.c."""
+    z = np.ascontiguousarray(charges, dtype=np.float64)
+    r = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1, 3)
+    off = np.ascontiguousarray(offsets, dtype=np.int32)
+    nmol = len(off) - 1
+    cm = np.zeros((int(off[-1]) if nmol else 0, size * (size + 1) // 2))
+    rc = _lib().orc_cm_local_batch(nmol, _p(off, _ip), _p(z), _p(r), size,
+                                   {"local": 0, "atomic": 1}[kind], _p(cm))
+    if rc:
+        raise ValueError("molecule has more atoms than size")
+    return cm
+
+
+def vector_kernels(kind, x1, x2, n1, n2, sigmas):
+    """fkernels.f90:23-162 restated in oracle.c; x (nm, amax, d) rows,
+    kind "gaussian" or "laplacian" -> (nsig, nm1, nm2)."""
+    x1 = np.ascontiguousarray(x1, dtype=np.float64)
+    x2 = np.ascontiguousarray(x2, dtype=np.float64)
+    n1 = np.ascontiguousarray(n1, dtype=np.int32)
+    n2 = np.ascontiguousarray(n2, dtype=np.int32)
+    sig = np.ascontiguousarray(np.atleast_1d(sigmas), dtype=np.float64)
+    K = np.zeros((len(sig), x1.shape[0], x2.shape[0]))
+    _lib().orc_vector_kernels({"gaussian": 0, "laplacian": 1}[kind], _p(x1), _p(n1, _ip),
+                              x1.shape[0], x1.shape[1], _p(x2), _p(n2, _ip), x2.shape[0],
+                              x2.shape[1], x1.shape[2], _p(sig), len(sig), _p(K))
+    return K
 
 
 def arad_descriptors(charges, coords, offsets, size=23, cut=5.0):
@@ -168,6 +199,25 @@ def get_atomic_symmetric_kernels_arad(X1, Z1, sigmas, width=0.2, cut_distance=6.
     return K
 
 
+def fget_alpha_arad(q, z, n, y, sigma, lambda_):
+    """farad_kernels.f90:231-436: K + lambda I from oracle.c, then LAPACK
+    dpotrf('U'), dpotri('U') and BLAS dsymv('U') as the routine calls them
+    (:391-403), and the per-molecule value spread over its atoms (:407-432).
+    Returns (alpha (sum(n),), potrf info, potri info)."""
+    from scipy.linalg import blas, lapack
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    z = np.ascontiguousarray(z, dtype=np.float64)
+    n = np.ascontiguousarray(n, dtype=np.int32)
+    nm, amax = q.shape[0], q.shape[1]
+    K = np.zeros((nm, nm))
+    _lib().orc_arad_alpha_kernel(_p(q), _p(z), _p(n, _ip), nm, amax, ctypes.c_double(sigma),
+                                 ctypes.c_double(lambda_), _p(K))
+    c, info = lapack.dpotrf(np.asfortranarray(K), lower=0, clean=0)
+    inv, info2 = lapack.dpotri(c, lower=0)
+    ltcly = blas.dsymv(1.0, inv, np.asarray(y, dtype=np.float64), lower=0)
+    return np.repeat(ltcly, n), int(info), int(info2)
+
+
 def fget_atomic_kernels_arad(q1, q2, z1, z2, n1, n2, sigmas, na1, na2, nsigmas, width,
                              cut_distance, r_width, c_width):
     """farad_kernels.f90:757-899 (the f2py routine fml.kernels exports).
@@ -216,6 +266,20 @@ def cho_solve(A, y):
     c, info = lapack.dpotrf(np.asfortranarray(A), lower=0, clean=0, overwrite_a=0)
     x, info2 = lapack.dpotrs(c, np.asarray(y, dtype=np.float64), lower=0)
     return x, int(info)
+
+
+def cho_invert(A):
+    """fml/math/cho_solve.py:27-30 -> fcho_solve.f90:49-68: LAPACK dpotrf('U')
+    then dpotri('U') on a Fortran copy; the strict lower triangle keeps A's
+    values (LAPACK does not touch it)."""
+    from scipy.linalg import lapack
+    a = np.asfortranarray(np.array(A, dtype=np.float64))
+    c, info = lapack.dpotrf(a, lower=0, clean=0, overwrite_a=0)
+    inv, info2 = lapack.dpotri(c, lower=0, overwrite_c=0)
+    out = np.asfortranarray(inv)
+    il = np.tril_indices(len(a), -1)
+    out[il] = a[il]
+    return out, int(info), int(info2)
 
 
 def cho_solve_restated(A, y):

@@ -111,6 +111,133 @@ int orc_cm_sorted_batch(int nmol, const int *offsets, const double *charges,
 }
 
 /* ------------------------------------------------------------------------ */
+/* Local / atomic Coulomb matrices: frepresentations.f90:204-294 / :297-390   */
+/* ------------------------------------------------------------------------ */
+/* One molecule: cm (n, len) rows, kind 0 local, 1 atomic. Returns -1 if n > nmax. */
+int orc_cm_local(int n, const double *charges, const double *coords, int nmax, int kind,
+                 double *cm)
+{
+    if (n > nmax || n < 0) return -1;
+    const int len = nmax * (nmax + 1) / 2;
+    for (size_t t = 0; t < (size_t)n * len; ++t) cm[t] = 0.0;
+    if (n == 0) return 0;
+    double *pair = (double *)malloc(sizeof(double) * (size_t)n * n);
+    double *dist = (double *)malloc(sizeof(double) * (size_t)n * n);
+    double *row_norms = (double *)malloc(sizeof(double) * n);
+    int *sorted_atoms = (int *)malloc(sizeof(int) * n);
+    int *order = (int *)malloc(sizeof(int) * n);
+    for (int i = 0; i < n; ++i) { /* :238-244, :344-346 */
+        double pn = 0.5 * pow(charges[i], 2.4);
+        row_norms[i] = 0.0 + pn;
+        pair[i * n + i] = pn;
+        dist[i * n + i] = 0.0;
+    }
+    for (int i = 0; i < n; ++i) /* :246-259, :336-354 */
+        for (int j = i + 1; j < n; ++j) {
+            double dx = coords[j * 3 + 0] - coords[i * 3 + 0];
+            double dy = coords[j * 3 + 1] - coords[i * 3 + 1];
+            double dz = coords[j * 3 + 2] - coords[i * 3 + 2];
+            double s = dx * dx;
+            s = s + dy * dy;
+            s = s + dz * dz;
+            double d = sqrt(s);
+            double pn = charges[i] * charges[j] / d;
+            row_norms[j] = row_norms[j] + pn;
+            row_norms[i] = row_norms[i] + pn;
+            pair[i * n + j] = pn;
+            pair[j * n + i] = pn;
+            dist[i * n + j] = d;
+            dist[j * n + i] = d;
+        }
+    for (int it = 0; it < n; ++it) { /* :262-266 */
+        int jmin = 0;
+        for (int j = 1; j < n; ++j)
+            if (row_norms[j] < row_norms[jmin]) jmin = j;
+        sorted_atoms[n - it - 1] = jmin;
+        row_norms[jmin] = DBL_MAX;
+    }
+    for (int k = 0; k < n; ++k) {
+        if (kind == 0) { /* :268-277: k, then the sorted atoms without k */
+            order[0] = k;
+            int m = 0;
+            for (int i = 0; i < n - 1; ++i) {
+                if (sorted_atoms[i] == k) m = 1;
+                order[i + 1] = sorted_atoms[i + m];
+            }
+        } else { /* :366-371: repeated minloc over the distances to k */
+            double *col = (double *)malloc(sizeof(double) * n);
+            for (int i = 0; i < n; ++i) col[i] = dist[i * n + k];
+            for (int it = 0; it < n; ++it) {
+                int jmin = 0;
+                for (int j = 1; j < n; ++j)
+                    if (col[j] < col[jmin]) jmin = j;
+                order[it] = jmin;
+                col[jmin] = DBL_MAX;
+            }
+            free(col);
+        }
+        for (int m = 0; m < n; ++m) { /* :281-291 / :375-386 */
+            int idx = m * (m + 1) / 2;
+            for (int q = 0; q <= m; ++q)
+                cm[(size_t)k * len + idx + q] = pair[order[m] * n + order[q]];
+        }
+    }
+    free(pair); free(dist); free(row_norms); free(sorted_atoms); free(order);
+    return 0;
+}
+
+/* Batch: rows of every atom, cm (total_atoms, len). */
+int orc_cm_local_batch(int nmol, const int *offsets, const double *charges,
+                       const double *coords, int nmax, int kind, double *cm)
+{
+    const int len = nmax * (nmax + 1) / 2;
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(| : bad)
+    for (int m = 0; m < nmol; ++m) {
+        int a0 = offsets[m], n = offsets[m + 1] - offsets[m];
+        if (orc_cm_local(n, charges + a0, coords + 3 * (size_t)a0, nmax, kind,
+                         cm + (size_t)a0 * len))
+            bad |= 1;
+    }
+    return bad ? -1 : 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Atomic vector kernels: fkernels.f90:23-104 (Laplacian, Gaussian)           */
+/* ------------------------------------------------------------------------ */
+/* X (nm, amax, d) row-major; K (nsig, nm1, nm2); kind 0 Gaussian, 1 Laplacian */
+void orc_vector_kernels(int kind, const double *X1, const int *N1, int nm1, int amax1,
+                        const double *X2, const int *N2, int nm2, int amax2, int d,
+                        const double *sigmas, int nsig, double *K)
+{
+#pragma omp parallel for schedule(dynamic)
+    for (int j = 0; j < nm2; ++j) {
+        double *ad = (double *)malloc(sizeof(double) * (size_t)amax1 * amax2);
+        for (int i = 0; i < nm1; ++i) {
+            int ni = N1[i], nj = N2[j];
+            for (int ja = 0; ja < nj; ++ja)
+                for (int ia = 0; ia < ni; ++ia) {
+                    const double *a = X1 + ((size_t)i * amax1 + ia) * d;
+                    const double *b = X2 + ((size_t)j * amax2 + ja) * d;
+                    double s = 0.0;
+                    for (int f = 0; f < d; ++f) {
+                        double t = a[f] - b[f];
+                        s = s + (kind == 0 ? t * t : fabs(t));
+                    }
+                    ad[(size_t)ja * ni + ia] = s; /* column-major (ia fastest) */
+                }
+            for (int k = 0; k < nsig; ++k) {
+                double c = kind == 0 ? -0.5 / (sigmas[k] * sigmas[k]) : -1.0 / sigmas[k];
+                double acc = 0.0;
+                for (int t = 0; t < ni * nj; ++t) acc = acc + exp(ad[t] * c);
+                K[((size_t)k * nm1 + i) * nm2 + j] = acc;
+            }
+        }
+        free(ad);
+    }
+}
+
+/* ------------------------------------------------------------------------ */
 /* Gaussian kernel: fkernels.f90:317-349                                      */
 /* ------------------------------------------------------------------------ */
 void orc_gaussian_kernel(const double *A, int na, const double *B, int nb, int d,
@@ -227,9 +354,11 @@ static double orc_arad_pair(const double *Q1, const double *Z1, const int *N1, c
                             const double *self1, int i, const double *Q2, const double *Z2,
                             const int *N2, const double *S2, const double *self2, int j,
                             int amax, double width, double cut, double rw, double cw,
-                            const double *inv_sigma2, int nsig, double *ad, double *out)
+                            const double *inv_sigma2, int nsig, double eps, double *ad,
+                            double *out)
 {
-    const double eps = 5.0e-12f; /* :505 a single-precision literal in the source */
+    /* eps: the single-precision literal 5.0e-12 of :505 / :679, or 1.0e-11 (:309)
+     * for fget_alpha_arad */
     const double rw2 = rw * rw, cw2 = cw * cw;
     int ni = N1[i], nj = N2[j];
     for (int j1 = 0; j1 < nj; ++j1) {
@@ -345,7 +474,7 @@ void orc_arad_kernels(const double *Q1, const double *Q2, const double *Z1, cons
         for (int j = 0; j < nm2; ++j) { /* :576-577 OMP over molecules of set 2 */
             for (int i = 0; i < nm1; ++i) {
                 orc_arad_pair(Q1, Z1, N1, S1, self1, i, Q2, Z2, N2, S2, self2, j, amax, width,
-                              cut, rw, cw, inv_sigma2, nsig, ad, out);
+                              cut, rw, cw, inv_sigma2, nsig, (double)5.0e-12f, ad, out);
                 for (int k = 0; k < nsig; ++k)
                     K[((size_t)k * nm1 + i) * nm2 + j] = out[k];
             }
@@ -360,10 +489,34 @@ void orc_arad_kernels(const double *Q1, const double *Q2, const double *Z1, cons
     free(self2);
 }
 
+static void orc_arad_symmetric(const double *Q1, const double *Z1, const int *N1,
+                               const double *sigmas, int nm1, int nsig, int amax, double width,
+                               double cut, double rw, double cw, double eps, double *K);
+
 /* fget_symmetric_kernels_arad: farad_kernels.f90:619-755. K (nsig, nm, nm). */
 void orc_arad_symmetric_kernels(const double *Q1, const double *Z1, const int *N1,
                                 const double *sigmas, int nm1, int nsig, int amax, double width,
                                 double cut, double rw, double cw, double *K)
+{
+    orc_arad_symmetric(Q1, Z1, N1, sigmas, nm1, nsig, amax, width, cut, rw, cw,
+                       (double)5.0e-12f, K);
+}
+
+/* The matrix fget_alpha_arad factors (farad_kernels.f90:231-389): the
+ * symmetric kernel for one sigma with width 0.2, cut 6, r_width 1,
+ * c_width 0.5 (:237-240), eps the single-precision literal 1.0e-11 (:309),
+ * then lambda added to the diagonal (:385-389). K (nm, nm). */
+void orc_arad_alpha_kernel(const double *Q1, const double *Z1, const int *N1, int nm1, int amax,
+                           double sigma, double lambda, double *K)
+{
+    orc_arad_symmetric(Q1, Z1, N1, &sigma, nm1, 1, amax, 0.2, 6.0, 1.0, 0.5,
+                       (double)1.0e-11f, K);
+    for (int i = 0; i < nm1; ++i) K[(size_t)i * nm1 + i] = K[(size_t)i * nm1 + i] + lambda;
+}
+
+static void orc_arad_symmetric(const double *Q1, const double *Z1, const int *N1,
+                               const double *sigmas, int nm1, int nsig, int amax, double width,
+                               double cut, double rw, double cw, double eps, double *K)
 {
     double *inv_sigma2 = (double *)malloc(sizeof(double) * (nsig > 0 ? nsig : 1));
     for (int k = 0; k < nsig; ++k) inv_sigma2[k] = -1.0 / (sigmas[k] * sigmas[k]); /* :685 */
@@ -377,7 +530,7 @@ void orc_arad_symmetric_kernels(const double *Q1, const double *Z1, const int *N
         for (int j = 0; j < nm1; ++j) {      /* :717-718 */
             for (int i = 0; i <= j; ++i) {   /* :720 only i <= j */
                 orc_arad_pair(Q1, Z1, N1, S1, self1, i, Q1, Z1, N1, S1, self1, j, amax, width,
-                              cut, rw, cw, inv_sigma2, nsig, ad, out);
+                              cut, rw, cw, inv_sigma2, nsig, eps, ad, out);
                 for (int k = 0; k < nsig; ++k) {
                     K[((size_t)k * nm1 + i) * nm1 + j] = out[k];
                     K[((size_t)k * nm1 + j) * nm1 + i] = out[k]; /* :744 mirror */

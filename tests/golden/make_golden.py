@@ -13,7 +13,10 @@ available, so only its Python-3-runnable parts are executed here:
 * ``fml/representations/representations.py``: the pure-Python sorted Coulomb
   matrix ``generate_coulomb_matrix`` and ``triangular_to_vector`` (their
   module fails to parse under Python 3 only because of a Python-2 ``print``
-  statement, which is rewritten as a call before the two functions are run);
+  statement, which is rewritten as a call before the two functions are run),
+  and the per-atom ``generate_local_coulomb_matrix`` /
+  ``generate_atomic_coulomb_matrix`` (the latter's Python-2 debug line
+  ``print distances`` is dropped: it only prints);
 * ``tests/test_arad.py``: the reference test's own ARAD distance / kernel
   restatement (``calcNorm``, ``calcProd``, ``_MDist``, ``_dist``,
   ``_StochDist``, the ``PTP`` table), evaluated serially the way
@@ -134,6 +137,19 @@ def main():
                                       syn_cm.molecule(i)[1], size=23)
         for i in range(syn_cm.nmol)])
 
+    # ---- per-atom (local / atomic) Coulomb matrices from representations.py
+    src = _extract(rep_path, ["generate_local_coulomb_matrix", "generate_atomic_coulomb_matrix"])
+    assert src.count("print distances") == 1
+    exec(src.replace("print distances", "pass"), ns)
+    lcm = {}
+    for kind in ("local", "atomic"):
+        fn = ns["generate_%s_coulomb_matrix" % kind]
+        lcm[kind + "_xyz_s23"] = np.concatenate(
+            [np.array(fn(m[1], m[2], size=23)) for m in mols])
+        lcm[kind + "_syn_s23"] = np.concatenate([
+            np.array(fn([inv[z] for z in syn_cm.molecule(i)[0]], syn_cm.molecule(i)[1],
+                        size=23)) for i in range(syn_cm.nmol)])
+
     # ---- ARAD kernels from tests/test_arad.py's restatement ----------------
     ta_path = os.path.join(REF, "tests/test_arad.py")
     tns = {"np": np}
@@ -183,6 +199,7 @@ def main():
         **{"xyz_" + k: v for k, v in xyz.items()},
         **{"arad_" + k: v for k, v in arad.items()},
         **{"cm_" + k: v for k, v in cm.items()},
+        **{"lcm_" + k: v for k, v in lcm.items()},
         syn11_charges=syn.charges, syn11_coords=syn.coords, syn11_offsets=syn.offsets,
         syn12_charges=syn_cm.charges, syn12_coords=syn_cm.coords,
         syn12_offsets=syn_cm.offsets,

@@ -54,3 +54,26 @@ def test_atomic_distances_are_the_kernel_exponents(oracle_mod):
     K = oracle_mod.fget_atomic_kernels_arad(q, q[:20], z, z[:20], n, n[:20], [1.3], len(q), 20,
                                             1, 0.2, 6.0, 1.0, 0.5)
     np.testing.assert_allclose(K[0], np.exp(D * (-1.0 / 1.3 ** 2)), rtol=1e-15, atol=0)
+
+
+def test_alpha_kernel_is_symmetric_kernel_plus_lambda(oracle_mod):
+    """fget_alpha_arad's matrix (farad_kernels.f90:231-389) is the symmetric
+    ARAD kernel with the routine's fixed parameters plus lambda I; only its eps
+    differs (1e-11 vs 5e-12), which moves no entry by more than 1e-12
+    relative. The weights are inv(K + lambda I) y, spread over each
+    molecule's atoms."""
+    b = synthetic.generate(12, nmax=9, seed=14)
+    X = oracle_mod.arad_descriptors(b.charges, b.coords, b.offsets, 9, 1e6)
+    Z = [b.molecule(i)[0] for i in range(b.nmol)]
+    n = np.array([len(z) for z in Z], np.int32)
+    zp = np.zeros((b.nmol, 9, 2))
+    for i, z in enumerate(Z):
+        zp[i, :len(z)] = ptp_of(z)
+    y = np.random.default_rng(0).standard_normal(b.nmol)
+    sigma, lam = 2.0, 1e-2
+    alpha, info, info2 = oracle_mod.fget_alpha_arad(X, zp, n, y, sigma, lam)
+    assert info == info2 == 0 and alpha.shape == (n.sum(),)
+    K = oracle_mod.get_atomic_symmetric_kernels_arad(X, Z, [sigma])[0] + lam * np.eye(b.nmol)
+    mol_alpha = np.linalg.solve(K, y)
+    np.testing.assert_allclose(alpha, np.repeat(mol_alpha, n), rtol=1e-9,
+                               atol=1e-12 * np.abs(mol_alpha).max())

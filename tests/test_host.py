@@ -96,3 +96,15 @@ def test_serving_ptp_packing_matches_reference_marshalling():
     np.testing.assert_array_equal(n, nref)
     with pytest.raises(KeyError):
         _ptp_packed(np.array([1.0, 200.0]), np.array([0, 2]), 4)
+
+
+@pytest.mark.parametrize("fn", ["generate_coulomb_matrices", "generate_local_coulomb_matrices",
+                                "generate_arad_descriptors"])
+def test_descriptor_offsets_checked_before_launch(fn):
+    """Offsets past the charge / coordinate buffers are rejected on the host."""
+    import fml_b200
+    z, r = np.ones(4), np.zeros((4, 3))
+    with pytest.raises(ValueError):
+        getattr(fml_b200, fn)(z, r, [0, 2, 6], size=8)
+    with pytest.raises(ValueError):
+        getattr(fml_b200, fn)(z, r, [-1, 2], size=8)

@@ -15,6 +15,7 @@ import torch
 
 import fml_b200
 from fml_b200 import synthetic
+from fml_b200.data import ptp_of
 
 pytestmark = pytest.mark.gpu
 
@@ -233,6 +234,53 @@ def test_cho_solve_not_positive_definite_warns(oracle_mod):
         fml_b200.cho_solve(A, y, strict=True)
 
 
+@pytest.mark.parametrize("n", [1, 2, 5, 127, 128, 129, 300, 1031, 2304, 4099])
+def test_cho_invert_vs_lapack(oracle_mod, n):
+    rng = np.random.default_rng(100 + n)
+    M = rng.standard_normal((n, n))
+    A = M @ M.T / n + np.eye(n)
+    A[np.tril_indices(n, -1)] += 3.0  # not symmetric: only the upper triangle is read
+    out = fml_b200.cho_invert(A)
+    ref, info, info2 = oracle_mod.cho_invert(A)
+    assert info == info2 == 0
+    assert out.flags["F_CONTIGUOUS"] and out.shape == (n, n)
+    iu, il = np.triu_indices(n), np.tril_indices(n, -1)
+    np.testing.assert_allclose(out[iu], ref[iu], rtol=1e-10, atol=1e-12 * np.abs(ref).max())
+    np.testing.assert_array_equal(out[il], A[il])  # untouched, as LAPACK leaves it
+
+
+def test_cho_invert_kernel_matrix_and_torch(oracle_mod):
+    import torch
+    b = synthetic.generate(1500, nmax=23, seed=55)
+    X = oracle_mod.coulomb_matrices(b.charges, b.coords, b.offsets, 23)
+    K = oracle_mod.gaussian_kernel(X.T, X.T, 724.0) + 1e-3 * np.eye(1500)
+    ref, _, _ = oracle_mod.cho_invert(K)
+    Kt = torch.from_numpy(K).cuda()
+    out = fml_b200.cho_invert(Kt)
+    assert out.is_cuda
+    iu = np.triu_indices(1500)
+    o = out.cpu().numpy()
+    np.testing.assert_allclose(o[iu], ref[iu], rtol=1e-8, atol=1e-9 * np.abs(ref).max())
+    # alpha = inv(K) y through the symmetric inverse equals the solve
+    y = np.random.default_rng(3).standard_normal(1500)
+    full = np.triu(o) + np.triu(o, 1).T
+    np.testing.assert_allclose(full @ y, oracle_mod.cho_solve(K, y)[0], rtol=1e-7,
+                               atol=1e-8 * np.abs(full @ y).max())
+
+
+def test_cho_invert_not_positive_definite(oracle_mod):
+    A = np.eye(300) * 2.0
+    A[200, 200] = -1.0
+    with pytest.warns(fml_b200.CholeskyWarning, match="error code: 201"):
+        out = fml_b200.cho_invert(A)
+    assert np.isnan(out[np.triu_indices(300)]).all()
+    assert oracle_mod.cho_invert(A)[1] == 201
+    with pytest.raises(np.linalg.LinAlgError):
+        fml_b200.cho_invert(A, strict=True)
+    with pytest.raises(ValueError):
+        fml_b200.cho_invert(np.ones((3, 4)))
+
+
 # ---------------------------------------------------------------------------
 # end to end: plain FP64 KRR on sorted Coulomb matrices (2000 molecules)
 # ---------------------------------------------------------------------------
@@ -370,7 +418,7 @@ def test_syrk_lower_strip(m, strip):
     np.testing.assert_array_equal(out[~upd], buf[~upd])
 
 
-def test_cho_solve_wide_outer_panels(oracle_mod):
+def test_cho_solve_512_outer_panels(oracle_mod):
     """n >= 8192 takes 512-column outer panels; n = 8300 ends in a partial one."""
     n = 8300
     rng = np.random.default_rng(7)
@@ -396,6 +444,36 @@ def _arad_set(oracle_mod, nmol, nmax, seed, cut, zpool=None):
     X = oracle_mod.arad_descriptors(charges, b.coords, b.offsets, nmax, cut)
     Z = [charges[b.offsets[i]:b.offsets[i + 1]] for i in range(nmol)]
     return X, Z
+
+
+@pytest.mark.parametrize("nmol,nmax,seed", [(40, 23, 61), (301, 12, 62), (1, 5, 63)])
+def test_fget_alpha_arad_vs_oracle(oracle_mod, nmol, nmax, seed):
+    X, Z = _arad_set(oracle_mod, nmol, nmax, seed, 1e6)
+    n = np.array([len(z) for z in Z], np.int32)
+    zp = np.zeros((nmol, nmax, 2))
+    for i, z in enumerate(Z):
+        zp[i, :len(z)] = ptp_of(z)
+    y = np.random.default_rng(seed).standard_normal(nmol)
+    ref, info, info2 = oracle_mod.fget_alpha_arad(X, zp, n, y, 2.0, 1e-2)
+    assert info == info2 == 0
+    alpha = np.zeros(n.sum() + 3)  # f2py intent(inout): filled in place, the rest zeroed
+    alpha[-1] = 7.0
+    assert fml_b200.fget_alpha_arad(X, zp, n, y, 2.0, 1e-2, alpha) is None
+    np.testing.assert_allclose(alpha[:n.sum()], ref, rtol=1e-8, atol=1e-10 * np.abs(ref).max())
+    assert (alpha[n.sum():] == 0).all()
+    np.testing.assert_array_equal(fml_b200.fget_alpha_arad(X, zp, n, y, 2.0, 1e-2),
+                                  alpha[:n.sum()])
+
+
+def test_fget_alpha_arad_not_positive_definite(oracle_mod):
+    X, Z = _arad_set(oracle_mod, 6, 8, 64, 1e6)
+    n = np.array([len(z) for z in Z], np.int32)
+    zp = np.zeros((6, 8, 2))
+    for i, z in enumerate(Z):
+        zp[i, :len(z)] = ptp_of(z)
+    with pytest.warns(fml_b200.CholeskyWarning, match="DPOTRF"):
+        out = fml_b200.fget_alpha_arad(X, zp, n, np.ones(6), 2.0, -1e6)
+    assert np.isnan(out).all()
 
 
 @pytest.mark.parametrize("zpool,nmax", [(None, 23), ([1, 3, 4, 5, 6, 7, 8, 9, 11, 12, 13, 14, 15,
