@@ -24,6 +24,8 @@ SIGNATURES = {
     "fmlb_last_error_string": (ctypes.c_char_p, []),
     "fmlb_version": (_i, []),
     "fmlb_coulomb_matrices": (_i, [_vp, _vp, _vp, _i, _i, _vp, _i, _vp, _i, _vp, _vp, _vp]),
+    "fmlb_xyz_scan": (_i, [_vp, _i, _vp, _vp, _i]),
+    "fmlb_xyz_parse": (_i, [_vp, _i, _vp, _vp, _vp, _i, _vp, _vp, _vp, _i]),
     "fmlb_local_coulomb_matrices": (_i, [_vp, _vp, _vp, _i, _i, _i, _vp, _i, _vp, _vp]),
     "fmlb_vector_kernels_f64": (_i, [_i, _vp, _vp, _i, _i, _vp, _vp, _i, _i, _i, _dp, _i, _vp,
                                      _vp, _vp]),
@@ -37,6 +39,8 @@ SIGNATURES = {
                                _i, _i, _vp, _vp, _sz, _vp]),
     "fmlb_arad_atomic_workspace_bytes": (_sz, [_i, _i, _i]),
     "fmlb_arad_alpha_kernel_f64": (_i, [_vp, _vp, _vp, _i, _i, _d, _d, _vp, _vp, _sz, _vp]),
+    "fmlb_arad_distances": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp, _i, _i, _d, _d, _d, _d, _vp,
+                                 _vp, _sz, _vp]),
     "fmlb_arad_atomic_distances": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp, _i, _i, _d, _d, _d, _d,
                                         _vp, _vp, _sz, _vp]),
     "fmlb_arad_atomic_kernels": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp, _i, _i, _dp, _i, _d, _d,
@@ -100,9 +104,13 @@ def load(require_cuda=True):
     return _LIB
 
 
+# host-only entry points (no device work): callable without a GPU
+HOST_ONLY = frozenset(["fmlb_xyz_scan", "fmlb_xyz_parse"])
+
+
 def call(name, *args):
     """Call an fmlb entry point and raise FmlbError on a negative return."""
-    lib = load()
+    lib = load(require_cuda=name not in HOST_ONLY)
     rc = getattr(lib, name)(*args)
     if isinstance(rc, int) and rc < 0:
         msg = lib.fmlb_last_error_string().decode(errors="replace")

@@ -1,4 +1,4 @@
-"""Build libfmlb.so (all CUDA sources under fml_b200/csrc) for sm_100a, in-tree.
+"""Build libfmlb.so (all CUDA and host C++ sources under fml_b200/csrc) for sm_100a, in-tree.
 
     python -m fml_b200.build            # incremental: rebuild when a source is newer
     python -m fml_b200.build --force
@@ -35,7 +35,8 @@ def nvcc_path():
 
 
 def sources():
-    return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    """CUDA sources and the host-only C++ sources (compiled by nvcc as C++)."""
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
 
 
 def _deps():
@@ -75,7 +76,7 @@ def build(force=False, verbose=False, jobs=None):
     if failed:
         raise RuntimeError("nvcc failed for: " + ", ".join(os.path.basename(f) for f in failed))
     tmp = OUT + ".tmp"
-    cmd = [nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs
+    cmd = [nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs + ["-lpthread"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, OUT)
     return OUT

@@ -205,13 +205,16 @@ __device__ __forceinline__ void pair_index(long long t, int symmetric, int nm2, 
 }
 
 // Stage 2: one warp per molecule pair; lanes stride over atom pairs.
-template <bool kF64>
+// kDist: store every atom pair's l2 in D (nm1, nm2, amax, amax) instead of
+// the kernel sums (atomic_arad_l2_distance_all, farad.f90:452-600).
+template <bool kF64, bool kDist = false>
 __global__ void __launch_bounds__(128)
 arad_pair_kernel(const double *__restrict__ X1, const double *__restrict__ Z1,
                  const int *__restrict__ N1, SetWs w1, int nm1, const double *__restrict__ X2,
                  const double *__restrict__ Z2, const int *__restrict__ N2, SetWs w2, int nm2,
                  int amax, AradParams P, SigmaTable sig, int nsig, int symmetric,
-                 double *__restrict__ K, const ClassInfo *fast_ci) {
+                 double *__restrict__ K, const ClassInfo *fast_ci,
+                 double *__restrict__ D = nullptr) {
     // when the fast FP32 kernel handled this call, the generic one does nothing
     if (fast_ci && fast_ci->flag == 0) return;
     const int lane = threadIdx.x & 31;
@@ -252,10 +255,15 @@ arad_pair_kernel(const double *__restrict__ X1, const double *__restrict__ Z1,
                 l2 = (double)(w1.self32[b1] + w2.self32[b2] - 2.0f * S * (float)stoch);
             }
             if (fabs(l2) < eps) l2 = 0.0;  // :594
+            if (kDist) {  // farad.f90:589
+                D[(((size_t)I * nm2 + J) * amax + i1) * amax + j1] = l2;
+                continue;
+            }
 #pragma unroll
             for (int s = 0; s < MAXSIG; ++s)
                 if (s < nsig) acc[s] += exp(l2 * sig.inv_sigma2[s]);
         }
+        if (kDist) continue;
 #pragma unroll
         for (int s = 0; s < MAXSIG; ++s) {
             if (s < nsig) {
@@ -1172,4 +1180,55 @@ extern "C" int fmlb_arad_alpha_kernel_f64(const double *X, const double *Z, cons
     FMLB_TRY(arad_kernels_impl(X, Z, N, nm, X, Z, N, nm, amax, &sigma, 1, 0.2, 6.0, 1.0, 0.5, 1,
                                0, (double)1.0e-11f, K, workspace, ws_bytes, stream));
     return fmlb_add_diagonal_f64(K, nm, nm, lambda, stream);
+}
+
+// atomic_arad_l2_distance_all (farad.f90:452-600), called by
+// get_l2_distance_arad (fml/math/distance.py:120-189): D (nm1, nm2, amax, amax)
+// with l2 of every atom pair, zero past each molecule's atoms. Sine factors
+// for every listed neighbour in both sets (:519-539), eps the single-precision
+// literal 5.0e-12 (:509).
+extern "C" int fmlb_arad_distances(const double *X1, const double *Z1, const int *N1, int nm1,
+                                   const double *X2, const double *Z2, const int *N2, int nm2,
+                                   int amax, double width, double cut_distance, double r_width,
+                                   double c_width, double *D, void *workspace, size_t ws_bytes,
+                                   void *stream) {
+    using namespace fmlb;
+    cudaStream_t st = FMLB_STREAM(stream);
+    FMLB_REQUIRE(nm1 >= 0 && nm2 >= 0 && amax >= 1, "fmlb_arad_distances: bad sizes");
+    const size_t need = fmlb_arad_workspace_bytes(nm1, nm2, amax, 0);
+    if (ws_bytes < need || (need && !workspace)) {
+        set_error("fmlb_arad_distances: workspace %zu bytes < required %zu", ws_bytes, need);
+        return FMLB_ENOMEM;
+    }
+    if (nm1 == 0 || nm2 == 0) return FMLB_OK;
+    FMLB_REQUIRE(X1 && Z1 && N1 && X2 && Z2 && N2 && D, "fmlb_arad_distances: null pointer");
+    AradParams P;
+    P.width = width;
+    P.cut = cut_distance;
+    P.rw2 = r_width * r_width;
+    P.cw2 = c_width * c_width;
+    P.inv_width = -1.0 / (4.0 * width * width);
+    P.maxg2 = (8.0 * width) * (8.0 * width);
+    P.inv_cut = (4.0 * atan(1.0)) / (2.0 * cut_distance);  // farad.f90:515
+    P.eps = (double)5.0e-12f;
+    char *p = static_cast<char *>(workspace);
+    SetWs w1 = carve(p, nm1, amax);
+    SetWs w2 = carve(p, nm2, amax);
+    const int tpb = 128;
+    arad_prep_kernel<<<ceil_div((long long)nm1 * amax, tpb), tpb, 0, st>>>(X1, N1, nm1, amax, P,
+                                                                           0, w1);
+    FMLB_TRY(launch_status("arad_prep_kernel"));
+    arad_prep_kernel<<<ceil_div((long long)nm2 * amax, tpb), tpb, 0, st>>>(X2, N2, nm2, amax, P,
+                                                                           0, w2);
+    FMLB_TRY(launch_status("arad_prep_kernel"));
+    FMLB_TRY(cuda_status(cudaMemsetAsync(D, 0, sizeof(double) * nm1 * nm2 * amax * amax, st),
+                         "fmlb_arad_distances: clear D"));
+    const long long npairs = (long long)nm1 * nm2;
+    const int blocks =
+        (int)std::min<long long>(ceil_div(npairs, tpb / 32), (long long)sm_count() * 64);
+    SigmaTable sig{};
+    arad_pair_kernel<true, true><<<blocks, tpb, 0, st>>>(X1, Z1, N1, w1, nm1, X2, Z2, N2, w2, nm2,
+                                                         amax, P, sig, 0, 0, nullptr, nullptr,
+                                                         D);
+    return launch_status("arad_pair_kernel<distance>");
 }

@@ -65,6 +65,28 @@ int fmlb_coulomb_matrices(const double *charges, const double *coords, const int
                           int *order, int *status, void *stream);
 
 /* ------------------------------------------------------------------------
+ * Batched XYZ ingestion (host code, no GPU): many .xyz files parsed with the
+ * rules of Molecule.read_xyz (fml/fml.py:109-132) into one packed ragged
+ * buffer, on `nthreads` host threads (<= 0: all cores).
+ *
+ * fmlb_xyz_scan: per file the declared atom count (line 1; may be NULL) and
+ *   the number of atom lines (lines 3.. up to the first with fewer than 4
+ *   tokens), which sizes the molecule as in the reference.
+ * fmlb_xyz_parse: with offsets (nfiles + 1) from the parsed counts, writes
+ *   charges (A,), coords (A, 3) and, when not NULL, symbol_index (A,) (index
+ *   of the element in the caller's table: table_symbols / table_charges,
+ *   the reference's NUCLEAR_CHARGE). Pass page-locked buffers to follow with
+ *   one asynchronous copy per array.
+ * Errors: FMLB_EINVAL with the file and line in the error string (unreadable
+ * file, bad atom count, unknown element, a coordinate that is not a number).
+ * ---------------------------------------------------------------------- */
+int fmlb_xyz_scan(const char *const *paths, int nfiles, int *natoms_declared, int *natoms_parsed,
+                  int nthreads);
+int fmlb_xyz_parse(const char *const *paths, int nfiles, const int *offsets,
+                   const char *const *table_symbols, const double *table_charges, int ntable,
+                   double *charges, double *coords, int *symbol_index, int nthreads);
+
+/* ------------------------------------------------------------------------
  * Local / atomic Coulomb matrices: one packed lower-triangle row per atom.
  * Replaces fgenerate_local_coulomb_matrix (kind 0,
  * fml/representations/frepresentations.f90:204-294) and
@@ -193,6 +215,18 @@ int fmlb_arad_kernels(const double *X1, const double *Z1, const int *N1, int nm1
 int fmlb_arad_alpha_kernel_f64(const double *X, const double *Z, const int *N, int nm, int amax,
                                double sigma, double lambda, double *K, void *workspace,
                                size_t ws_bytes, void *stream);
+
+/* Atom-pair ARAD distances of two molecule sets, the replacement for
+ * atomic_arad_l2_distance_all (fml/math/farad.f90:452-600) as called by
+ * get_l2_distance_arad (fml/math/distance.py:120-189).
+ *   D (nm1, nm2, amax, amax) float64: l2 of atom i1 of molecule i and atom j1
+ *     of molecule j, zero past each molecule's atoms.
+ * X, Z, N as for fmlb_arad_kernels; workspace of
+ * fmlb_arad_workspace_bytes(nm1, nm2, amax, 0) bytes. */
+int fmlb_arad_distances(const double *X1, const double *Z1, const int *N1, int nm1,
+                        const double *X2, const double *Z2, const int *N2, int nm2, int amax,
+                        double width, double cut_distance, double r_width, double c_width,
+                        double *D, void *workspace, size_t ws_bytes, void *stream);
 
 /* ------------------------------------------------------------------------
  * Cholesky factorisation and solve, FP64.

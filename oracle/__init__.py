@@ -199,6 +199,24 @@ def get_atomic_symmetric_kernels_arad(X1, Z1, sigmas, width=0.2, cut_distance=6.
     return K
 
 
+def get_l2_distance_arad(X1, X2, Z1, Z2, width=0.2, cut_distance=6.0, r_width=1.0,
+                         c_width=0.5):
+    """fml/math/distance.py:120-189 -> atomic_arad_l2_distance_all (farad.f90:452-600),
+    restated in oracle.c: D (nm1, nm2, amax, amax)."""
+    X1 = np.ascontiguousarray(X1, dtype=np.float64)
+    X2 = np.ascontiguousarray(X2, dtype=np.float64)
+    amax = X1.shape[1]
+    n1 = np.array([len(z) for z in Z1], dtype=np.int32)
+    n2 = np.array([len(z) for z in Z2], dtype=np.int32)
+    z1, z2 = _ptp_pad(Z1, amax), _ptp_pad(Z2, amax)
+    D = np.zeros((len(Z1), len(Z2), amax, amax))
+    _lib().orc_arad_l2_distance_all(_p(X1), _p(X2), _p(z1), _p(z2), _p(n1, _ip), _p(n2, _ip),
+                                    len(Z1), len(Z2), amax, ctypes.c_double(width),
+                                    ctypes.c_double(cut_distance), ctypes.c_double(r_width),
+                                    ctypes.c_double(c_width), _p(D))
+    return D
+
+
 def fget_alpha_arad(q, z, n, y, sigma, lambda_):
     """farad_kernels.f90:231-436: K + lambda I from oracle.c, then LAPACK
     dpotrf('U'), dpotri('U') and BLAS dsymv('U') as the routine calls them

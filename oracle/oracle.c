@@ -493,6 +493,46 @@ static void orc_arad_symmetric(const double *Q1, const double *Z1, const int *N1
                                const double *sigmas, int nm1, int nsig, int amax, double width,
                                double cut, double rw, double cw, double eps, double *K);
 
+/* atomic_arad_l2_distance_all: farad.f90:452-600 (its atomic_distl2,
+ * :62-123, is the same function as farad_kernels.f90:29-90). Sines for every
+ * listed neighbour of both sets (:519-539), eps 5.0e-12 single-precision
+ * (:509). D (nm1, nm2, amax, amax), zero past each molecule's atoms. */
+void orc_arad_l2_distance_all(const double *Q1, const double *Q2, const double *Z1,
+                              const double *Z2, const int *N1, const int *N2, int nm1, int nm2,
+                              int amax, double width, double cut, double rw, double cw, double *D)
+{
+    const double eps = 5.0e-12f;
+    const double rw2 = rw * rw, cw2 = cw * cw;
+    double *S1 = orc_arad_sines(Q1, N1, nm1, amax, cut, 0);
+    double *S2 = orc_arad_sines(Q2, N2, nm2, amax, cut, 0);
+    double *self1 = orc_arad_self(Q1, N1, S1, nm1, amax, width, cut, rw, cw);
+    double *self2 = orc_arad_self(Q2, N2, S2, nm2, amax, width, cut, rw, cw);
+    for (size_t t = 0; t < (size_t)nm1 * nm2 * amax * amax; ++t) D[t] = 0.0;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int j = 0; j < nm2; ++j) {
+        for (int i = 0; i < nm1; ++i) {
+            for (int i1 = 0; i1 < N1[i]; ++i1) {
+                for (int j1 = 0; j1 < N2[j]; ++j1) {
+                    const size_t a = (size_t)i * amax + i1, b = (size_t)j * amax + j1;
+                    double l2 = orc_atomic_distl2(Q1 + a * 5 * amax, Q2 + b * 5 * amax, N1[i],
+                                                  N2[j], S1 + a * amax, S2 + b * amax, amax,
+                                                  width, cut, rw, cw);
+                    double dz1 = Z1[a * 2 + 0] - Z2[b * 2 + 0];
+                    double dz2 = Z1[a * 2 + 1] - Z2[b * 2 + 1];
+                    l2 = self1[a] + self2[b] -
+                         2.0 * l2 * (rw2 / (rw2 + dz1 * dz1) * cw2 / (cw2 + dz2 * dz2));
+                    if (fabs(l2) < eps) l2 = 0.0;
+                    D[(((size_t)i * nm2 + j) * amax + i1) * amax + j1] = l2; /* :587 */
+                }
+            }
+        }
+    }
+    free(S1);
+    free(S2);
+    free(self1);
+    free(self2);
+}
+
 /* fget_symmetric_kernels_arad: farad_kernels.f90:619-755. K (nsig, nm, nm). */
 void orc_arad_symmetric_kernels(const double *Q1, const double *Z1, const int *N1,
                                 const double *sigmas, int nm1, int nsig, int amax, double width,

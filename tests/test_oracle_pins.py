@@ -69,6 +69,22 @@ def test_arad_kernel_oracle_matches_reference_test_restatement(golden, oracle_mo
     np.testing.assert_allclose(K, g["testarad_K_5v5"], rtol=1e-11)
 
 
+def test_arad_l2_distance_oracle_matches_reference_test_restatement(golden, oracle_mod):
+    """get_l2_distance_arad (atomic_arad_l2_distance_all, farad.f90:452-600)
+    against the distance matrix Da of tests/test_arad.py:358 (condense with
+    molecular=False), which is what the reference test compares it with. Da
+    holds NaN past each molecule's atoms; the Fortran routine holds 0."""
+    g = golden
+    x = g["arad_xyz_s30_c5"]
+    Z = [z for z, _ in _mols(g, "xyz_")]
+    D = oracle_mod.get_l2_distance_arad(x[:5], x[5:], Z[:5], Z[5:])
+    Da = g["testarad_D_5v5"]
+    assert D.shape == Da.shape
+    ok = ~np.isnan(Da)
+    np.testing.assert_allclose(D[ok], Da[ok], rtol=1e-12, atol=1e-13)
+    assert (D[~ok] == 0).all()
+
+
 def test_arad_symmetric_kernel_oracle_matches_reference_test_restatement(golden, oracle_mod):
     # the test restatement has no |l2| < 5e-12 clamp (farad_kernels.f90:735); on the
     # diagonal (identical atoms, l2 ~ 1e-15) that changes exp(-l2/0.1**2) by ~1e-10

@@ -465,6 +465,35 @@ def test_fget_alpha_arad_vs_oracle(oracle_mod, nmol, nmax, seed):
                                   alpha[:n.sum()])
 
 
+def test_l2_distance_arad_vs_reference_test_and_oracle(golden, oracle_mod):
+    """get_l2_distance_arad against the reference test's own distance matrix
+    (tests/test_arad.py:358-363 compares the two) and the oracle; exp-sums of
+    it reproduce the molecular kernel (tests/test_arad.py:379-387)."""
+    g = golden
+    x = g["arad_xyz_s30_c5"]
+    off = g["xyz_offsets"]
+    Z = [g["xyz_charges"][off[i]:off[i + 1]] for i in range(len(off) - 1)]
+    D = fml_b200.get_l2_distance_arad(x[:5], x[5:], Z[:5], Z[5:])
+    Da = g["testarad_D_5v5"]
+    ok = ~np.isnan(Da)
+    np.testing.assert_allclose(D[ok], Da[ok], rtol=1e-12, atol=1e-13)
+    assert (D[~ok] == 0).all()
+    np.testing.assert_allclose(D, oracle_mod.get_l2_distance_arad(x[:5], x[5:], Z[:5], Z[5:]),
+                               rtol=1e-12, atol=1e-13)
+    Ka = np.zeros((4, 5, 5))
+    for s, sigma in enumerate(g["testarad_sigmas"]):
+        Ka[s] = np.nansum(np.exp(np.where(ok, D, np.nan) * (-1.0 / sigma ** 2)), axis=(-2, -1))
+    np.testing.assert_allclose(Ka, g["testarad_K_5v5"], rtol=1e-11)
+
+
+@pytest.mark.parametrize("nm1,nm2,nmax,seed", [(37, 21, 23, 71), (3, 50, 9, 72)])
+def test_l2_distance_arad_synthetic(oracle_mod, nm1, nm2, nmax, seed):
+    X, Z = _arad_set(oracle_mod, nm1 + nm2, nmax, seed, 1e6)
+    D = fml_b200.get_l2_distance_arad(X[:nm1], X[nm1:], Z[:nm1], Z[nm1:])
+    ref = oracle_mod.get_l2_distance_arad(X[:nm1], X[nm1:], Z[:nm1], Z[nm1:])
+    np.testing.assert_allclose(D, ref, rtol=1e-12, atol=1e-12)
+
+
 def test_fget_alpha_arad_not_positive_definite(oracle_mod):
     X, Z = _arad_set(oracle_mod, 6, 8, 64, 1e6)
     n = np.array([len(z) for z in Z], np.int32)
