@@ -10,8 +10,8 @@ Drop-in names (same signatures and error behaviour as the reference):
   atom-level ``fget_atomic_kernels_arad`` / ``fget_atomic_distance_arad``
   and ``fget_alpha_arad`` (fml/kernels/farad_kernels.f90), ``get_atomic_kernels_gaussian``,
   ``get_atomic_kernels_laplacian`` (fml/kernels/kernels.py)
-* ``cho_solve``, ``cho_invert`` (fml/math/cho_solve.py), ``get_l2_distance_arad``
-  (fml/math/distance.py)
+* ``cho_solve``, ``cho_invert`` (fml/math/cho_solve.py), ``get_l2_distance_arad``,
+  ``manhattan_distance``, ``l2_distance``, ``p_distance`` (fml/math/distance.py)
 
 Batched forms: ``read_xyz_batch`` (many .xyz files into one packed buffer),
 ``generate_coulomb_matrices``, ``generate_local_coulomb_matrices``,
@@ -26,7 +26,7 @@ from .cho_solve import CholeskyWarning, cho_invert, cho_solve
 from .data import NUCLEAR_CHARGE, PTP
 from .descriptors import (generate_arad_descriptors, generate_coulomb_matrices,
                           generate_local_coulomb_matrices)
-from .distance import get_l2_distance_arad
+from .distance import get_l2_distance_arad, l2_distance, manhattan_distance, p_distance
 from .kernels import (fget_alpha_arad, fget_atomic_distance_arad, fget_atomic_kernels_arad,
                       gaussian_kernel, get_atomic_kernels_arad, get_atomic_kernels_gaussian,
                       get_atomic_kernels_laplacian, get_atomic_symmetric_kernels_arad,
@@ -38,7 +38,8 @@ __all__ = [
     "Molecule", "gaussian_kernel", "laplacian_kernel", "get_atomic_kernels_arad",
     "get_atomic_symmetric_kernels_arad", "fget_atomic_kernels_arad", "fget_alpha_arad",
     "fget_atomic_distance_arad", "get_atomic_kernels_gaussian", "get_atomic_kernels_laplacian",
-    "get_l2_distance_arad", "cho_solve", "cho_invert",
+    "get_l2_distance_arad", "manhattan_distance", "l2_distance", "p_distance", "cho_solve",
+    "cho_invert",
     "CholeskyWarning",
     "generate_coulomb_matrices", "generate_local_coulomb_matrices", "generate_arad_descriptors",
     "read_xyz_batch", "NUCLEAR_CHARGE", "PTP",

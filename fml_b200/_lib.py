@@ -45,6 +45,7 @@ SIGNATURES = {
                                         _vp, _vp, _sz, _vp]),
     "fmlb_arad_atomic_kernels": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp, _i, _i, _dp, _i, _d, _d,
                                       _d, _d, _vp, _vp, _sz, _vp]),
+    "fmlb_distance_matrix_f64": (_i, [_i, _vp, _i, _i, _vp, _i, _i, _i, _i, _d, _vp, _ll, _vp]),
     "fmlb_potrf_workspace_bytes": (_sz, [_i]),
     "fmlb_potrf_f64": (_i, [_vp, _ll, _i, _vp, _vp, _vp]),
     "fmlb_potri_f64": (_i, [_vp, _ll, _i, _vp, _vp, _ll, _vp, _vp]),

@@ -1,16 +1,67 @@
-"""ARAD distance matrices: drop-in for ``get_l2_distance_arad``
-(fml/math/distance.py:120-189 -> atomic_arad_l2_distance_all,
-fml/math/farad.f90:452-600).
+"""Distance matrices: drop-ins for fml/math/distance.py.
 
-The l2 distance of every atom pair of two molecule sets, computed by the
-same FP64 atom-pair core as the ARAD kernels (``fmlb_arad_distances``).
+* ``manhattan_distance``, ``l2_distance``, ``p_distance`` (distance.py:58-117
+  -> fdistance.f90): ``A`` (d, na), ``B`` (d, nb) with descriptors as
+  columns; D (na, nb), Fortran-ordered like the reference's ``empty(...,
+  order='F')`` (``fmlb_distance_matrix_f64``).
+* ``get_l2_distance_arad`` (distance.py:120-189 -> atomic_arad_l2_distance_all,
+  farad.f90:452-600): the l2 distance of every atom pair of two molecule
+  sets, computed by the same FP64 atom-pair core as the ARAD kernels
+  (``fmlb_arad_distances``).
 """
 
+import numpy as np
 import torch
 
 from . import _lib
-from ._tensors import device, to_device, to_output, workspace
-from .kernels import _ptp_arrays
+from ._tensors import device, is_torch, to_device, to_output, workspace
+from .kernels import _descriptor_rows, _ptp_arrays
+
+
+def _check_pair(A, B):
+    if len(A.shape) != 2 or len(B.shape) != 2:
+        raise ValueError('expected matrices of dimension=2')
+    if B.shape[0] != A.shape[0]:
+        raise ValueError('expected matrices containing vectors of same size')
+
+
+def _distance(kind, A, B, p_int=0, p_real=0.0):
+    a, as_np = _descriptor_rows(A)
+    b = a if B is A else _descriptor_rows(B)[0]
+    na, d = a.shape
+    nb = b.shape[0]
+    D = torch.empty((na, nb), dtype=torch.float64, device=a.device)
+    _lib.call("fmlb_distance_matrix_f64", kind, _lib.ptr(a), na, d, _lib.ptr(b), nb, d, d,
+              int(p_int), float(p_real), _lib.ptr(D), nb, _lib.stream_handle())
+    if as_np and not is_torch(B):
+        return np.asfortranarray(D.cpu().numpy())
+    return D
+
+
+def manhattan_distance(A, B):
+    """fmanhattan_distance, fdistance.f90:23-46: D[j, i] = sum |A[:, j] - B[:, i]|."""
+    _check_pair(A, B)
+    return _distance(0, A, B)
+
+
+def l2_distance(A, B):
+    """fl2_distance, fdistance.f90:49-80: D[j, i] = ||A[:, j] - B[:, i]||_2."""
+    _check_pair(A, B)
+    return _distance(1, A, B)
+
+
+def p_distance(A, B, p=2):
+    """fdistance.f90:83-155: (sum (A[:, j] - B[:, i])**p)**(1/p); an int p of 2
+    is l2_distance, another int p the integer form, a float p the real form,
+    anything else ValueError (distance.py:92-117)."""
+    _check_pair(A, B)
+    if type(p) == type(1):
+        if p == 2:
+            return _distance(1, A, B)
+        return _distance(2, A, B, p_int=p)
+    elif type(p) == type(1.0):
+        return _distance(3, A, B, p_real=p)
+    raise ValueError('expected exponent of integer or float type')
 
 
 def get_l2_distance_arad(X1, X2, Z1, Z2, width=0.2, cut_distance=6.0, r_width=1.0,

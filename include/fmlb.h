@@ -228,6 +228,18 @@ int fmlb_arad_distances(const double *X1, const double *Z1, const int *N1, int n
                         double width, double cut_distance, double r_width, double c_width,
                         double *D, void *workspace, size_t ws_bytes, void *stream);
 
+/* Generic distance matrices, the replacement for fml/math/fdistance.f90 as
+ * called by manhattan_distance / l2_distance / p_distance
+ * (fml/math/distance.py:58-117):
+ *   kind 0 fmanhattan_distance, 1 fl2_distance, 2 fp_distance_integer
+ *   (p_int), 3 fp_distance_double (p_real).
+ * A (na, d), B (nb, d) row-major device rows; D (na, nb) with row stride ldd,
+ * D[j, i] = dist(A_j, B_i). The p forms raise the signed difference as the
+ * reference does. */
+int fmlb_distance_matrix_f64(int kind, const double *A, int na, int lda, const double *B, int nb,
+                             int ldb, int d, int p_int, double p_real, double *D, long long ldd,
+                             void *stream);
+
 /* ------------------------------------------------------------------------
  * Cholesky factorisation and solve, FP64.
  * Replace LAPACK dpotrf('U') / dpotrs('U') as called by fcho_solve,

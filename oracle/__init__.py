@@ -199,6 +199,19 @@ def get_atomic_symmetric_kernels_arad(X1, Z1, sigmas, width=0.2, cut_distance=6.
     return K
 
 
+def distance_matrix(kind, A, B, p=None):
+    """fdistance.f90:23-155 restated in oracle.c; A (d, na), B (d, nb) in the
+    reference layout, kind "manhattan" | "l2" | "p_int" | "p_real"."""
+    a = np.ascontiguousarray(np.asarray(A, dtype=np.float64).T)
+    b = np.ascontiguousarray(np.asarray(B, dtype=np.float64).T)
+    D = np.zeros((a.shape[0], b.shape[0]))
+    k = {"manhattan": 0, "l2": 1, "p_int": 2, "p_real": 3}[kind]
+    _lib().orc_distance_matrix(k, _p(a), a.shape[0], _p(b), b.shape[0], a.shape[1],
+                               int(p) if k == 2 else 0,
+                               ctypes.c_double(float(p) if k == 3 else 0.0), _p(D))
+    return D
+
+
 def get_l2_distance_arad(X1, X2, Z1, Z2, width=0.2, cut_distance=6.0, r_width=1.0,
                          c_width=0.5):
     """fml/math/distance.py:120-189 -> atomic_arad_l2_distance_all (farad.f90:452-600),

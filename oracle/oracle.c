@@ -238,6 +238,33 @@ void orc_vector_kernels(int kind, const double *X1, const int *N1, int nm1, int 
 }
 
 /* ------------------------------------------------------------------------ */
+/* Distance matrices: fdistance.f90:23-155. A (na, nv), B (nb, nv) rows;      */
+/* D (na, nb). kind 0 manhattan, 1 l2, 2 integer p, 3 real p.                 */
+/* ------------------------------------------------------------------------ */
+void orc_distance_matrix(int kind, const double *A, int na, const double *B, int nb, int nv,
+                         int p_int, double p_real, double *D)
+{
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < nb; ++i)
+        for (int j = 0; j < na; ++j) {
+            double s = 0.0;
+            for (int k = 0; k < nv; ++k) {
+                double t = A[(size_t)j * nv + k] - B[(size_t)i * nv + k];
+                double term;
+                if (kind == 0) term = fabs(t);
+                else if (kind == 1) term = t * t;
+                else if (kind == 2) term = pow(t, (double)p_int);
+                else term = pow(t, p_real);
+                s = s + term;
+            }
+            if (kind == 1) s = sqrt(s);
+            else if (kind == 2) s = pow(s, 1.0 / (double)p_int);
+            else if (kind == 3) s = pow(s, 1.0 / p_real);
+            D[(size_t)j * nb + i] = s;
+        }
+}
+
+/* ------------------------------------------------------------------------ */
 /* Gaussian kernel: fkernels.f90:317-349                                      */
 /* ------------------------------------------------------------------------ */
 void orc_gaussian_kernel(const double *A, int na, const double *B, int nb, int d,
