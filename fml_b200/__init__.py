@@ -9,7 +9,9 @@ Drop-in names (same signatures and error behaviour as the reference):
   ``get_atomic_symmetric_kernels_arad`` (fml/kernels/kernels.py) and the
   atom-level ``fget_atomic_kernels_arad`` / ``fget_atomic_distance_arad``
   and ``fget_alpha_arad`` (fml/kernels/farad_kernels.f90), ``get_atomic_kernels_gaussian``,
-  ``get_atomic_kernels_laplacian`` (fml/kernels/kernels.py)
+  ``get_atomic_kernels_laplacian``, ``get_alpha``, ``get_prediction``,
+  ``get_alpha_from_distance``, ``get_prediction_from_distance``
+  (fml/kernels/kernels.py)
 * ``cho_solve``, ``cho_invert`` (fml/math/cho_solve.py), ``get_l2_distance_arad``,
   ``manhattan_distance``, ``l2_distance``, ``p_distance`` (fml/math/distance.py)
 
@@ -28,9 +30,10 @@ from .descriptors import (generate_arad_descriptors, generate_coulomb_matrices,
                           generate_local_coulomb_matrices)
 from .distance import get_l2_distance_arad, l2_distance, manhattan_distance, p_distance
 from .kernels import (fget_alpha_arad, fget_atomic_distance_arad, fget_atomic_kernels_arad,
-                      gaussian_kernel, get_atomic_kernels_arad, get_atomic_kernels_gaussian,
+                      gaussian_kernel, get_alpha, get_alpha_from_distance,
+                      get_atomic_kernels_arad, get_atomic_kernels_gaussian,
                       get_atomic_kernels_laplacian, get_atomic_symmetric_kernels_arad,
-                      laplacian_kernel)
+                      get_prediction, get_prediction_from_distance, laplacian_kernel)
 from .molecule import Molecule
 from .xyz import read_xyz_batch
 
@@ -38,6 +41,7 @@ __all__ = [
     "Molecule", "gaussian_kernel", "laplacian_kernel", "get_atomic_kernels_arad",
     "get_atomic_symmetric_kernels_arad", "fget_atomic_kernels_arad", "fget_alpha_arad",
     "fget_atomic_distance_arad", "get_atomic_kernels_gaussian", "get_atomic_kernels_laplacian",
+    "get_alpha", "get_prediction", "get_alpha_from_distance", "get_prediction_from_distance",
     "get_l2_distance_arad", "manhattan_distance", "l2_distance", "p_distance", "cho_solve",
     "cho_invert",
     "CholeskyWarning",

@@ -24,6 +24,11 @@ SIGNATURES = {
     "fmlb_last_error_string": (ctypes.c_char_p, []),
     "fmlb_version": (_i, []),
     "fmlb_coulomb_matrices": (_i, [_vp, _vp, _vp, _i, _i, _vp, _i, _vp, _i, _vp, _vp, _vp]),
+    "fmlb_vector_kernels_packed_f64": (_i, [_i, _vp, _vp, _i, _i, _vp, _vp, _i, _i, _i, _dp,
+                                            _i, _vp, _vp, _vp]),
+    "fmlb_segment_exp_sum_f64": (_i, [_vp, _ll, _i, _i, _vp, _i, _vp, _i, _d, _vp, _ll, _vp]),
+    "fmlb_exp_colsum_scratch_doubles": (_sz, [_i]),
+    "fmlb_exp_weighted_colsum_f64": (_i, [_vp, _ll, _i, _i, _d, _vp, _vp, _vp, _vp]),
     "fmlb_xyz_scan": (_i, [_vp, _i, _vp, _vp, _i]),
     "fmlb_xyz_parse": (_i, [_vp, _i, _vp, _vp, _vp, _i, _vp, _vp, _vp, _i]),
     "fmlb_local_coulomb_matrices": (_i, [_vp, _vp, _vp, _i, _i, _i, _vp, _i, _vp, _vp]),

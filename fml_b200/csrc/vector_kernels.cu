@@ -41,12 +41,15 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 
 // PP atom pairs per thread per pass: the distance sums of the PP pairs are
 // independent chains, interleaved feature by feature.
+// Packed mode (O1 / O2 not null): molecule m's atoms are rows O[m] .. O[m+1]
+// of a (total_atoms, d) matrix; N and amax then bound the counts only.
 template <int KIND, int PP>
 __global__ void __launch_bounds__(VK_TPB)
 vector_kernels_kernel(const double *__restrict__ X1, const int *__restrict__ N1, int nm1,
                       int amax1, const double *__restrict__ X2, const int *__restrict__ N2,
                       int nm2, int amax2, int d, const Coefs coef, int nsig,
-                      double *__restrict__ K, int *__restrict__ status) {
+                      double *__restrict__ K, int *__restrict__ status,
+                      const int *__restrict__ O1, const int *__restrict__ O2) {
     extern __shared__ double sm[];
     double *A = sm;                                   // [amax1][VK_FS]
     double *B = A + (size_t)amax1 * VK_FS;            // [amax2][VK_FS]
@@ -55,15 +58,15 @@ vector_kernels_kernel(const double *__restrict__ X1, const int *__restrict__ N1,
     const long long pair = blockIdx.x;
     const int i = (int)(pair / nm2), j = (int)(pair % nm2);
     const int t = threadIdx.x;
-    int ni = N1[i], nj = N2[j];
+    int ni = O1 ? O1[i + 1] - O1[i] : N1[i], nj = O2 ? O2[j + 1] - O2[j] : N2[j];
     if (ni < 0 || ni > amax1 || nj < 0 || nj > amax2) {  // rejected on the host as well
         if (t == 0 && status) atomicCAS(status, 0, 1);
         ni = min(max(ni, 0), amax1);
         nj = min(max(nj, 0), amax2);
     }
     for (int k = 0; k < nsig; ++k) acc[k * VK_TPB + t] = 0.0;
-    const double *x1 = X1 + (size_t)i * amax1 * d;
-    const double *x2 = X2 + (size_t)j * amax2 * d;
+    const double *x1 = X1 + (O1 ? (size_t)O1[i] : (size_t)i * amax1) * d;
+    const double *x2 = X2 + (O2 ? (size_t)O2[j] : (size_t)j * amax2) * d;
     const int np = ni * nj;
     for (int p0 = 0; p0 < np; p0 += VK_TPB * PP) {
         double dist[PP];
@@ -126,14 +129,14 @@ size_t vk_smem_bytes(int amax1, int amax2, int nsig) {
 template <int KIND, int PP>
 int launch_vk(const double *X1, const int *N1, int nm1, int amax1, const double *X2,
               const int *N2, int nm2, int amax2, int d, const Coefs &coef, int nsig, double *K,
-              int *status, cudaStream_t st) {
+              int *status, const int *O1, const int *O2, cudaStream_t st) {
     const size_t smem = vk_smem_bytes(amax1, amax2, nsig);
     FMLB_TRY(cuda_status(cudaFuncSetAttribute(vector_kernels_kernel<KIND, PP>,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)smem),
                          "cudaFuncSetAttribute"));
     vector_kernels_kernel<KIND, PP><<<(unsigned)((long long)nm1 * nm2), VK_TPB, smem, st>>>(
-        X1, N1, nm1, amax1, X2, N2, nm2, amax2, d, coef, nsig, K, status);
+        X1, N1, nm1, amax1, X2, N2, nm2, amax2, d, coef, nsig, K, status, O1, O2);
     return launch_status(KIND == 0 ? "vector_kernels_kernel<gaussian>"
                                    : "vector_kernels_kernel<laplacian>");
 }
@@ -143,11 +146,12 @@ int launch_vk(const double *X1, const int *N1, int nm1, int amax1, const double 
 template <int KIND>
 int launch_vk_pp(int pairs, const double *X1, const int *N1, int nm1, int amax1,
                  const double *X2, const int *N2, int nm2, int amax2, int d, const Coefs &coef,
-                 int nsig, double *K, int *status, cudaStream_t st) {
+                 int nsig, double *K, int *status, const int *O1, const int *O2,
+                 cudaStream_t st) {
 #define FMLB_VK(PP)                                                                            \
     if (pairs <= PP * VK_TPB || PP == 16)                                                     \
         return launch_vk<KIND, PP>(X1, N1, nm1, amax1, X2, N2, nm2, amax2, d, coef, nsig, K,  \
-                                   status, st);
+                                   status, O1, O2, st);
     FMLB_VK(2) FMLB_VK(4) FMLB_VK(6) FMLB_VK(9) FMLB_VK(12) FMLB_VK(16)
 #undef FMLB_VK
     return FMLB_OK;
@@ -156,10 +160,10 @@ int launch_vk_pp(int pairs, const double *X1, const int *N1, int nm1, int amax1,
 }  // namespace
 }  // namespace fmlb
 
-extern "C" int fmlb_vector_kernels_f64(int kind, const double *X1, const int *N1, int nm1,
-                                       int amax1, const double *X2, const int *N2, int nm2,
-                                       int amax2, int d, const double *sigmas_host, int nsig,
-                                       double *K, int *status, void *stream) {
+static int vector_kernels_impl(int kind, const double *X1, const int *N1, int nm1, int amax1,
+                               const double *X2, const int *N2, int nm2, int amax2, int d,
+                               const double *sigmas_host, int nsig, double *K, int *status,
+                               const int *O1, const int *O2, void *stream) {
     using namespace fmlb;
     FMLB_REQUIRE(kind == 0 || kind == 1, "fmlb_vector_kernels_f64: kind must be 0 or 1");
     FMLB_REQUIRE(nm1 >= 0 && nm2 >= 0 && d >= 0, "fmlb_vector_kernels_f64: bad sizes");
@@ -169,7 +173,8 @@ extern "C" int fmlb_vector_kernels_f64(int kind, const double *X1, const int *N1
                  "fmlb_vector_kernels_f64: nsig=%d outside 1..%d", nsig, VK_MAX_SIGMAS);
     FMLB_REQUIRE(sigmas_host, "fmlb_vector_kernels_f64: null sigmas");
     if ((long long)nm1 * nm2 == 0) return FMLB_OK;
-    FMLB_REQUIRE(X1 && N1 && X2 && N2 && K, "fmlb_vector_kernels_f64: null pointer");
+    FMLB_REQUIRE(X1 && (N1 || O1) && X2 && (N2 || O2) && K,
+                 "fmlb_vector_kernels_f64: null pointer");
     Coefs coef;
     for (int k = 0; k < nsig; ++k) {
         FMLB_REQUIRE(sigmas_host[k] > 0.0, "fmlb_vector_kernels_f64: sigma %d not positive", k);
@@ -181,7 +186,30 @@ extern "C" int fmlb_vector_kernels_f64(int kind, const double *X1, const int *N1
     const int pairs = amax1 * amax2;
     if (kind == 0)
         return launch_vk_pp<0>(pairs, X1, N1, nm1, amax1, X2, N2, nm2, amax2, d, coef, nsig, K,
-                               status, st);
+                               status, O1, O2, st);
     return launch_vk_pp<1>(pairs, X1, N1, nm1, amax1, X2, N2, nm2, amax2, d, coef, nsig, K,
-                           status, st);
+                           status, O1, O2, st);
+}
+
+extern "C" int fmlb_vector_kernels_f64(int kind, const double *X1, const int *N1, int nm1,
+                                       int amax1, const double *X2, const int *N2, int nm2,
+                                       int amax2, int d, const double *sigmas_host, int nsig,
+                                       double *K, int *status, void *stream) {
+    return vector_kernels_impl(kind, X1, N1, nm1, amax1, X2, N2, nm2, amax2, d, sigmas_host,
+                               nsig, K, status, nullptr, nullptr, stream);
+}
+
+// Packed form: X (total_atoms, d) rows with molecule offsets O (nm + 1);
+// amax bounds the atoms of one molecule (checked on the device through
+// status). The molecule kernel of fget_alpha (fkernels.f90:380-440) is the
+// Laplacian form with X1 = X2.
+extern "C" int fmlb_vector_kernels_packed_f64(int kind, const double *X1, const int *O1, int nm1,
+                                              int amax1, const double *X2, const int *O2, int nm2,
+                                              int amax2, int d, const double *sigmas_host,
+                                              int nsig, double *K, int *status, void *stream) {
+    using namespace fmlb;
+    FMLB_REQUIRE(nm1 == 0 || O1, "fmlb_vector_kernels_packed_f64: null offsets");
+    FMLB_REQUIRE(nm2 == 0 || O2, "fmlb_vector_kernels_packed_f64: null offsets");
+    return vector_kernels_impl(kind, X1, nullptr, nm1, amax1, X2, nullptr, nm2, amax2, d,
+                               sigmas_host, nsig, K, status, O1, O2, stream);
 }

@@ -9,6 +9,9 @@
   (fkernels.f90:23-162), sums over atom pairs of per-atom descriptors
 * ``fget_alpha_arad`` -> the routine of that name (farad_kernels.f90:231-436):
   explicit-inverse ARAD KRR weights
+* ``get_alpha`` / ``get_prediction`` / ``get_alpha_from_distance`` /
+  ``get_prediction_from_distance`` -> fget_alpha, fget_prediction and their
+  from-distance forms (fkernels.f90:380-702): atomic Laplacian KRR
 * ``fget_atomic_kernels_arad`` / ``fget_atomic_distance_arad`` -> the
   atom-level routines of the same names (farad_kernels.f90:757-1030), which
   fml.kernels exports directly
@@ -278,6 +281,169 @@ def fget_atomic_distance_arad(q1, q2, z1, z2, n1, n2, na1, na2, width, cut_dista
     return to_output(D.t().contiguous(), not is_torch(q1))
 
 
+def _explicit_inverse_weights(Kt, yd, counts):
+    """The common tail of the reference's explicit-inverse KRR routines
+    (fget_alpha, fget_alpha_from_distance, fget_alpha_arad): dpotrf('U'),
+    dpotri('U'), dsymv('U') with y, and each molecule's value spread over its
+    atoms. ``Kt`` (nm, nm) device holds K + lambda I with K's upper triangle
+    in its row-major lower triangle (it is overwritten). Returns numpy
+    (sum(counts),); NaN after a non-positive pivot, with the reference's
+    DPOTRF warning."""
+    nm = Kt.shape[0]
+    dev = Kt.device
+    work, info = potrf(Kt, nm)
+    ldv = nm + (nm & 1)
+    V = torch.empty((nm, ldv), dtype=torch.float64, device=dev)
+    _lib.call("fmlb_potri_f64", _lib.ptr(Kt), nm, nm, _lib.ptr(work), _lib.ptr(V), ldv,
+              _lib.ptr(info), _lib.stream_handle())
+    del V
+    _lib.call("fmlb_symmetrize_lower_f64", _lib.ptr(Kt), nm, nm, _lib.stream_handle())
+    ltcly = torch.empty(nm, dtype=torch.float64, device=dev)
+    _lib.call("fmlb_gemv_f64", _lib.ptr(Kt), nm, nm, nm, _lib.ptr(yd), _lib.ptr(ltcly),
+              _lib.stream_handle())
+    code = int(info.item())
+    vals = np.repeat(ltcly.cpu().numpy(), counts)
+    if code > 0:
+        warnings.warn("WARNING: Cholesky decomposition DPOTRF() exited with error code: %d"
+                      % code, CholeskyWarning, stacklevel=3)
+        vals[:] = np.nan
+    return vals
+
+
+def _counts(N, what):
+    n = np.asarray(N.cpu() if is_torch(N) else N, dtype=np.int64).reshape(-1)
+    if len(n) and n.min() < 0:
+        raise ValueError("%s: atom counts must be >= 0" % what)
+    off = np.zeros(len(n) + 1, dtype=np.int64)
+    np.cumsum(n, out=off[1:])
+    return n.astype(np.int32), off
+
+
+def _segment_sums(v, off):
+    """Y[j] = sum(v[off[j]:off[j+1]]) (the reference's per-molecule sums)."""
+    counts = np.diff(off)
+    out = np.zeros(len(counts))
+    nz = counts > 0
+    if nz.any():
+        out[nz] = np.add.reduceat(v[:off[-1]], off[:-1][nz])
+    return out
+
+
+def get_alpha(Q, N, Y, sigma, llambda):
+    """kernels.py:119-126 -> fget_alpha (fkernels.f90:380-478): atomic
+    Laplacian KRR weights. Q (d, na) per-atom descriptors as columns, N atoms
+    per molecule, Y (nm,). K[i, j] = sum over atom pairs of molecules i, j of
+    exp(-|q_a - q_b|_1 / sigma), plus llambda on the diagonal, inverted from
+    its Cholesky factor on the GPU; returns alpha (sum(N),), each atom holding
+    its molecule's weight."""
+    n, off = _counts(N, "get_alpha")
+    nm = len(n)
+    q, _ = _descriptor_rows(Q)  # (na, d)
+    if off[-1] > q.shape[0]:
+        raise ValueError("get_alpha: sum(N) = %d exceeds the %d atoms of Q"
+                         % (off[-1], q.shape[0]))
+    if len(Y) != nm:
+        raise ValueError("get_alpha: Y must hold one value per molecule")
+    if nm == 0:
+        return np.zeros(0)
+    dev = q.device
+    amax = max(int(n.max()), 1)
+    if amax > 128:
+        raise ValueError("get_alpha: at most 128 atoms per molecule")
+    od = torch.from_numpy(off.astype(np.int32)).to(dev)
+    K = torch.empty((nm, nm), dtype=torch.float64, device=dev)
+    sp, keep = _lib.host_doubles([float(sigma)])
+    _lib.call("fmlb_vector_kernels_packed_f64", 1, _lib.ptr(q), _lib.ptr(od), nm, amax,
+              _lib.ptr(q), _lib.ptr(od), nm, amax, q.shape[1], sp, 1, _lib.ptr(K), None,
+              _lib.stream_handle())
+    del keep
+    _lib.call("fmlb_add_diagonal_f64", _lib.ptr(K), nm, nm, float(llambda), _lib.stream_handle())
+    yd, _ = to_device(Y if is_torch(Y) else np.asarray(Y, dtype=np.float64), torch.float64)
+    return _explicit_inverse_weights(K, yd, n)
+
+
+def get_prediction(Q, Q2, N2, alpha, sigma):
+    """kernels.py:101-108 -> fget_prediction (fkernels.f90:480-539):
+    Y[j] = sum over the atoms a2 of test molecule j of sum over all training
+    atoms a of exp(-|q_a - q2_a2|_1 / sigma) alpha[a]. The atom sums run in
+    the fused kernel-times-weights launch (the kernel matrix is not stored)."""
+    n2, off2 = _counts(N2, "get_prediction")
+    q, _ = _descriptor_rows(Q)
+    q2, _ = _descriptor_rows(Q2)
+    if q.shape[1] != q2.shape[1]:
+        raise ValueError("get_prediction: descriptor sizes differ")
+    if off2[-1] > q2.shape[0]:
+        raise ValueError("get_prediction: sum(N2) exceeds the atoms of Q2")
+    na, na2 = q.shape[0], q2.shape[0]
+    if len(alpha) < na:
+        raise ValueError("get_prediction: alpha must hold one weight per atom of Q")
+    if na2 == 0 or na == 0:
+        return np.zeros(len(n2))
+    ad, _ = to_device(alpha if is_torch(alpha) else np.asarray(alpha, dtype=np.float64),
+                      torch.float64)
+    csa = torch.empty(na2, dtype=torch.float64, device=q.device)
+    lib = _lib.load()
+    ws = workspace(lib.fmlb_kernel_predict_workspace_bytes(na2, na, 1))
+    sp, keep = _lib.host_doubles([float(sigma)])
+    _lib.call("fmlb_kernel_predict_f64", 1, _lib.ptr(q2), na2, q2.shape[1], _lib.ptr(q), na,
+              q.shape[1], q.shape[1], sp, 1, _lib.ptr(ad), na, _lib.ptr(csa), na2,
+              _lib.ptr(ws), ws.numel(), _lib.stream_handle())
+    del keep
+    return _segment_sums(csa.cpu().numpy(), off2)
+
+
+def get_alpha_from_distance(D, N, Y, sigma, llambda):
+    """kernels.py:127-134 -> fget_alpha_from_distance (fkernels.f90:541-641):
+    the molecule kernel sum over atom pairs of exp(-D[b, a] / sigma) from a
+    precomputed (na, na) atom distance matrix, plus llambda, inverted from its
+    Cholesky factor; returns alpha (sum(N),)."""
+    n, off = _counts(N, "get_alpha_from_distance")
+    nm = len(n)
+    d, _ = to_device(D if is_torch(D) else np.asarray(D, dtype=np.float64), torch.float64)
+    if d.dim() != 2 or off[-1] > min(d.shape):
+        raise ValueError("get_alpha_from_distance: D must be (na, na) with na >= sum(N)")
+    if len(Y) != nm:
+        raise ValueError("get_alpha_from_distance: Y must hold one value per molecule")
+    if nm == 0:
+        return np.zeros(0)
+    od = torch.from_numpy(off.astype(np.int32)).to(d.device)
+    S = torch.empty((nm, nm), dtype=torch.float64, device=d.device)
+    _lib.call("fmlb_segment_exp_sum_f64", _lib.ptr(d), d.stride(0), d.shape[0], d.shape[1],
+              _lib.ptr(od), nm, _lib.ptr(od), nm, -1.0 / float(sigma), _lib.ptr(S), nm,
+              _lib.stream_handle())
+    # S[j, i] = K(i, j): its row-major lower triangle is K's upper one
+    _lib.call("fmlb_add_diagonal_f64", _lib.ptr(S), nm, nm, float(llambda), _lib.stream_handle())
+    yd, _ = to_device(Y if is_torch(Y) else np.asarray(Y, dtype=np.float64), torch.float64)
+    return _explicit_inverse_weights(S, yd, n)
+
+
+def get_prediction_from_distance(D2, N2, alpha, sigma):
+    """kernels.py:110-117 -> fget_prediction_from_distance (fkernels.f90:645-702):
+    D2 (na, na2) distances between training and test atoms; Y[j] = sum over
+    the atoms i of test molecule j of sum_a exp(-D2[a, i] / sigma) alpha[a].
+    Difference: the reference leaves its per-atom accumulator uninitialised
+    (no csa = 0 before :688); here it starts at zero."""
+    n2, off2 = _counts(N2, "get_prediction_from_distance")
+    d2, _ = to_device(D2 if is_torch(D2) else np.asarray(D2, dtype=np.float64), torch.float64)
+    if d2.dim() != 2 or off2[-1] > d2.shape[1]:
+        raise ValueError("get_prediction_from_distance: D2 must be (na, na2), na2 >= sum(N2)")
+    na, na2 = d2.shape
+    if len(alpha) < na:
+        raise ValueError("get_prediction_from_distance: alpha must hold na weights")
+    if na2 == 0:
+        return np.zeros(len(n2))
+    ad, _ = to_device(alpha if is_torch(alpha) else np.asarray(alpha, dtype=np.float64),
+                      torch.float64)
+    csa = torch.empty(na2, dtype=torch.float64, device=d2.device)
+    lib = _lib.load()
+    scratch = torch.empty(lib.fmlb_exp_colsum_scratch_doubles(na2), dtype=torch.float64,
+                          device=d2.device)
+    _lib.call("fmlb_exp_weighted_colsum_f64", _lib.ptr(d2), d2.stride(0), na, na2,
+              -1.0 / float(sigma), _lib.ptr(ad), _lib.ptr(csa), _lib.ptr(scratch),
+              _lib.stream_handle())
+    return _segment_sums(csa.cpu().numpy(), off2)
+
+
 def fget_alpha_arad(q, z, n, y, sigma, lambda_, alpha=None):
     """Explicit-inverse ARAD KRR weights, the routine fml.kernels exports from
     its Fortran (farad_kernels.f90:231-436; the f2py argument order is kept).
@@ -311,22 +477,7 @@ def fget_alpha_arad(q, z, n, y, sigma, lambda_, alpha=None):
               float(sigma), float(lambda_), _lib.ptr(K), _lib.ptr(ws), ws.numel(),
               _lib.stream_handle())
     del ws
-    work, info = potrf(K, nm)
-    ldv = nm + (nm & 1)
-    V = torch.empty((nm, ldv), dtype=torch.float64, device=dev)
-    _lib.call("fmlb_potri_f64", _lib.ptr(K), nm, nm, _lib.ptr(work), _lib.ptr(V), ldv,
-              _lib.ptr(info), _lib.stream_handle())
-    del V
-    _lib.call("fmlb_symmetrize_lower_f64", _lib.ptr(K), nm, nm, _lib.stream_handle())
-    ltcly = torch.empty(nm, dtype=torch.float64, device=dev)
-    _lib.call("fmlb_gemv_f64", _lib.ptr(K), nm, nm, nm, _lib.ptr(yd), _lib.ptr(ltcly),
-              _lib.stream_handle())
-    code = int(info.item())
-    vals = np.repeat(ltcly.cpu().numpy(), nn)  # :407-432, molecule value per atom
-    if code > 0:
-        warnings.warn("WARNING: Cholesky decomposition DPOTRF() exited with error code: %d"
-                      % code, CholeskyWarning, stacklevel=2)
-        vals[:] = np.nan
+    vals = _explicit_inverse_weights(K, yd, nn)  # :391-432
     if alpha is None:
         return vals
     if len(alpha) < len(vals):

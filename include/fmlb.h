@@ -64,6 +64,33 @@ int fmlb_coulomb_matrices(const double *charges, const double *coords, const int
                           int nmol, int nmax, double *cm, int ldcm, float *cm32, int ldcm32,
                           int *order, int *status, void *stream);
 
+/* Packed form of fmlb_vector_kernels_f64: X1 (total_atoms1, d) rows with
+ * molecule offsets O1 (nm1 + 1), likewise X2 / O2; amax1 / amax2 bound the
+ * atoms of one molecule. With kind 1 and X1 = X2 this is the molecule kernel
+ * of fget_alpha (fml/kernels/fkernels.f90:380-440, wrapper get_alpha,
+ * kernels.py:119-126). */
+int fmlb_vector_kernels_packed_f64(int kind, const double *X1, const int *O1, int nm1, int amax1,
+                                   const double *X2, const int *O2, int nm2, int amax2, int d,
+                                   const double *sigmas_host, int nsig, double *K, int *status,
+                                   void *stream);
+
+/* Atomic KRR from precomputed atom-pair distances (fml/kernels/fkernels.f90:541-702,
+ * wrappers get_alpha_from_distance / get_prediction_from_distance,
+ * kernels.py:110-134):
+ * fmlb_segment_exp_sum_f64: S[p, q] = sum over rows R[p]..R[p+1] and columns
+ *   C[q]..C[q+1] of exp(c M[r, s]) (M row-major, rows x cols); with M the
+ *   atom distance matrix and R = C the molecule offsets, S is the transposed
+ *   molecule kernel of fget_alpha_from_distance (:586-597).
+ * fmlb_exp_weighted_colsum_f64: v[s] = sum_r exp(c M[r, s]) w[r], the per-atom
+ *   sums of fget_prediction_from_distance (:688-693); scratch of
+ *   fmlb_exp_colsum_scratch_doubles(cols) device doubles. Deterministic. */
+int fmlb_segment_exp_sum_f64(const double *M, long long ldm, int rows, int cols, const int *R,
+                             int np, const int *C, int nq, double c, double *S, long long lds,
+                             void *stream);
+size_t fmlb_exp_colsum_scratch_doubles(int cols);
+int fmlb_exp_weighted_colsum_f64(const double *M, long long ldm, int rows, int cols, double c,
+                                 const double *w, double *v, double *scratch, void *stream);
+
 /* ------------------------------------------------------------------------
  * Batched XYZ ingestion (host code, no GPU): many .xyz files parsed with the
  * rules of Molecule.read_xyz (fml/fml.py:109-132) into one packed ragged

@@ -230,12 +230,75 @@ def get_l2_distance_arad(X1, X2, Z1, Z2, width=0.2, cut_distance=6.0, r_width=1.
     return D
 
 
+def _explicit_inverse(K, y, n):
+    """dpotrf('U'), dpotri('U'), dsymv('U') on K (numpy, upper triangle read),
+    then each molecule's value spread over its atoms: the common tail of the
+    reference's explicit-inverse routines. Returns (alpha, info, info2)."""
+    from scipy.linalg import blas, lapack
+    c, info = lapack.dpotrf(np.asfortranarray(K), lower=0, clean=0)
+    inv, info2 = lapack.dpotri(c, lower=0)
+    ltcly = blas.dsymv(1.0, inv, np.asarray(y, dtype=np.float64), lower=0)
+    return np.repeat(ltcly, n), int(info), int(info2)
+
+
+def _offsets(N):
+    n = np.asarray(N, dtype=np.int32)
+    off = np.zeros(len(n) + 1, dtype=np.int32)
+    np.cumsum(n, out=off[1:])
+    return n, off
+
+
+def get_alpha(Q, N, Y, sigma, llambda):
+    """kernels.py:119-126 -> fget_alpha (fkernels.f90:380-478); Q (d, na)."""
+    q = np.ascontiguousarray(np.asarray(Q, dtype=np.float64).T)
+    n, off = _offsets(N)
+    K = np.zeros((len(n), len(n)))
+    _lib().orc_atomic_laplacian_kernel(_p(q), q.shape[0], q.shape[1], _p(off, _ip), len(n),
+                                       ctypes.c_double(sigma), _p(K))
+    K[np.diag_indices(len(n))] += llambda
+    return _explicit_inverse(K, Y, n)
+
+
+def get_prediction(Q, Q2, N2, alpha, sigma):
+    """kernels.py:101-108 -> fget_prediction (fkernels.f90:480-539)."""
+    q = np.ascontiguousarray(np.asarray(Q, dtype=np.float64).T)
+    q2 = np.ascontiguousarray(np.asarray(Q2, dtype=np.float64).T)
+    n2, off2 = _offsets(N2)
+    a = np.ascontiguousarray(alpha, dtype=np.float64)
+    Y = np.zeros(len(n2))
+    _lib().orc_atomic_laplacian_predict(_p(q), q.shape[0], _p(q2), q2.shape[0], q.shape[1],
+                                        _p(off2, _ip), len(n2), _p(a), ctypes.c_double(sigma),
+                                        _p(Y))
+    return Y
+
+
+def get_alpha_from_distance(D, N, Y, sigma, llambda):
+    """kernels.py:127-134 -> fget_alpha_from_distance (fkernels.f90:541-641)."""
+    d = np.ascontiguousarray(D, dtype=np.float64)
+    n, off = _offsets(N)
+    K = np.zeros((len(n), len(n)))
+    _lib().orc_distance_mol_kernel(_p(d), d.shape[0], _p(off, _ip), len(n),
+                                   ctypes.c_double(sigma), _p(K))
+    K[np.diag_indices(len(n))] += llambda
+    return _explicit_inverse(K, Y, n)
+
+
+def get_prediction_from_distance(D2, N2, alpha, sigma):
+    """kernels.py:110-117 -> fget_prediction_from_distance (fkernels.f90:645-702)."""
+    d2 = np.ascontiguousarray(D2, dtype=np.float64)
+    n2, off2 = _offsets(N2)
+    a = np.ascontiguousarray(alpha, dtype=np.float64)
+    Y = np.zeros(len(n2))
+    _lib().orc_distance_predict(_p(d2), d2.shape[0], d2.shape[1], _p(off2, _ip), len(n2), _p(a),
+                                ctypes.c_double(sigma), _p(Y))
+    return Y
+
+
 def fget_alpha_arad(q, z, n, y, sigma, lambda_):
     """farad_kernels.f90:231-436: K + lambda I from oracle.c, then LAPACK
     dpotrf('U'), dpotri('U') and BLAS dsymv('U') as the routine calls them
     (:391-403), and the per-molecule value spread over its atoms (:407-432).
     Returns (alpha (sum(n),), potrf info, potri info)."""
-    from scipy.linalg import blas, lapack
     q = np.ascontiguousarray(q, dtype=np.float64)
     z = np.ascontiguousarray(z, dtype=np.float64)
     n = np.ascontiguousarray(n, dtype=np.int32)
@@ -243,10 +306,7 @@ def fget_alpha_arad(q, z, n, y, sigma, lambda_):
     K = np.zeros((nm, nm))
     _lib().orc_arad_alpha_kernel(_p(q), _p(z), _p(n, _ip), nm, amax, ctypes.c_double(sigma),
                                  ctypes.c_double(lambda_), _p(K))
-    c, info = lapack.dpotrf(np.asfortranarray(K), lower=0, clean=0)
-    inv, info2 = lapack.dpotri(c, lower=0)
-    ltcly = blas.dsymv(1.0, inv, np.asarray(y, dtype=np.float64), lower=0)
-    return np.repeat(ltcly, n), int(info), int(info2)
+    return _explicit_inverse(K, y, n)
 
 
 def fget_atomic_kernels_arad(q1, q2, z1, z2, n1, n2, sigmas, na1, na2, nsigmas, width,

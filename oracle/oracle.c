@@ -238,6 +238,108 @@ void orc_vector_kernels(int kind, const double *X1, const int *N1, int nm1, int 
 }
 
 /* ------------------------------------------------------------------------ */
+/* Atomic Laplacian KRR: fkernels.f90:380-702. Atom descriptors are rows      */
+/* Q (na, nv); molecule m owns atoms off[m] .. off[m+1].                      */
+/* ------------------------------------------------------------------------ */
+/* fget_alpha's matrix before lambda, :409-432: ltcl(i, j) for i <= j as the
+ * reference builds it (ltc over all na atoms, then summed per molecule).
+ * K (nm, nm) receives both triangles (the lower mirrored). */
+void orc_atomic_laplacian_kernel(const double *Q, int na, int nv, const int *off, int nm,
+                                 double sigma, double *K)
+{
+    const double inv_sigma = -1.0 / sigma;
+#pragma omp parallel
+    {
+        double *ltc = (double *)malloc(sizeof(double) * (na > 0 ? na : 1));
+#pragma omp for schedule(dynamic, 1)
+        for (int j = 0; j < nm; ++j) {
+            for (int i = 0; i < na; ++i) {
+                double acc = 0.0;
+                for (int k = off[j]; k < off[j + 1]; ++k) {
+                    double s = 0.0;
+                    for (int f = 0; f < nv; ++f)
+                        s = s + fabs(Q[(size_t)k * nv + f] - Q[(size_t)i * nv + f]);
+                    acc = acc + exp(inv_sigma * s);
+                }
+                ltc[i] = acc;
+            }
+            for (int i = 0; i <= j; ++i) {
+                double t = 0.0;
+                for (int a = off[i]; a < off[i + 1]; ++a) t = t + ltc[a];
+                K[(size_t)i * nm + j] = t;
+                K[(size_t)j * nm + i] = t;
+            }
+        }
+        free(ltc);
+    }
+}
+
+/* fget_prediction, :508-535: csa over all test atoms, then per-molecule sums. */
+void orc_atomic_laplacian_predict(const double *Q, int na, const double *Q2, int na2, int nv,
+                                  const int *off2, int nm2, const double *alpha, double sigma,
+                                  double *Y)
+{
+    const double inv_sigma = -1.0 / sigma;
+    double *csa = (double *)calloc(na2 > 0 ? na2 : 1, sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < na2; ++i) {
+        double acc = 0.0;
+        for (int j = 0; j < na; ++j) {
+            double s = 0.0;
+            for (int f = 0; f < nv; ++f) s = s + fabs(Q[(size_t)j * nv + f] - Q2[(size_t)i * nv + f]);
+            acc = acc + exp(inv_sigma * s) * alpha[j];
+        }
+        csa[i] = acc;
+    }
+    for (int j = 0; j < nm2; ++j) {
+        double t = 0.0;
+        for (int a = off2[j]; a < off2[j + 1]; ++a) t = t + csa[a];
+        Y[j] = t;
+    }
+    free(csa);
+}
+
+/* fget_alpha_from_distance's matrix before lambda, :577-597; D (na, na)
+ * row-major is the numpy array, d(k, i) = D[k][i]. */
+void orc_distance_mol_kernel(const double *D, int na, const int *off, int nm, double dgamma,
+                             double *K)
+{
+    const double inv_gamma = -1.0 / dgamma;
+    double *ltc = (double *)malloc(sizeof(double) * (size_t)(nm > 0 ? nm : 1) * (na > 0 ? na : 1));
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < na; ++i)
+        for (int j = 0; j < nm; ++j) {
+            double acc = 0.0;
+            for (int k = off[j]; k < off[j + 1]; ++k) acc = acc + exp(inv_gamma * D[(size_t)k * na + i]);
+            ltc[(size_t)j * na + i] = acc;
+        }
+    for (int j = 0; j < nm; ++j)
+        for (int i = 0; i < nm; ++i) {
+            double t = 0.0;
+            for (int a = off[i]; a < off[i + 1]; ++a) t = t + ltc[(size_t)j * na + a];
+            K[(size_t)i * nm + j] = t;
+        }
+    free(ltc);
+}
+
+/* fget_prediction_from_distance, :681-698 (csa starts at zero here). */
+void orc_distance_predict(const double *D2, int na, int na2, const int *off2, int nm2,
+                          const double *alpha, double dgamma, double *Y)
+{
+    const double inv_gamma = -1.0 / dgamma;
+    double *csa = (double *)calloc(na2 > 0 ? na2 : 1, sizeof(double));
+    for (int i = 0; i < na2; ++i)
+        for (int j = 0; j < na; ++j)
+            csa[i] = csa[i] + exp(inv_gamma * D2[(size_t)j * na2 + i]) * alpha[j];
+    for (int j = 0; j < nm2; ++j) {
+        double t = 0.0;
+        for (int a = off2[j]; a < off2[j + 1]; ++a) t = t + csa[a];
+        Y[j] = t;
+    }
+    free(csa);
+}
+
+/* ------------------------------------------------------------------------ */
 /* Distance matrices: fdistance.f90:23-155. A (na, nv), B (nb, nv) rows;      */
 /* D (na, nb). kind 0 manhattan, 1 l2, 2 integer p, 3 real p.                 */
 /* ------------------------------------------------------------------------ */
