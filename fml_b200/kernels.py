@@ -7,8 +7,9 @@
 * ``get_atomic_kernels_gaussian`` / ``get_atomic_kernels_laplacian`` ->
   fget_vector_kernels_gaussian / fget_vector_kernels_laplacian
   (fkernels.f90:23-162), sums over atom pairs of per-atom descriptors
-* ``fget_alpha_arad`` -> the routine of that name (farad_kernels.f90:231-436):
-  explicit-inverse ARAD KRR weights
+* ``fget_alpha_arad`` / ``fget_kernel_arad`` -> the routines of those names
+  (farad_kernels.f90:95-436): explicit-inverse ARAD KRR weights and the
+  fixed-parameter symmetric ARAD kernel
 * ``get_alpha`` / ``get_prediction`` / ``get_alpha_from_distance`` /
   ``get_prediction_from_distance`` -> fget_alpha, fget_prediction and their
   from-distance forms (fkernels.f90:380-702): atomic Laplacian KRR
@@ -444,6 +445,47 @@ def get_prediction_from_distance(D2, N2, alpha, sigma):
     return _segment_sums(csa.cpu().numpy(), off2)
 
 
+def _alpha_inputs(q, z, n, nm=None):
+    qa = q if is_torch(q) else np.asarray(q, dtype=np.float64)
+    if qa.ndim != 4 or qa.shape[2] != 5 or qa.shape[3] != qa.shape[1]:
+        raise ValueError("q must be (nm, amax, 5, amax)")
+    nm = qa.shape[0] if nm is None else int(nm)
+    amax = qa.shape[1]
+    if nm < 0 or nm > qa.shape[0]:
+        raise ValueError("nm must lie in 0..%d" % qa.shape[0])
+    nn = np.asarray(n.cpu() if is_torch(n) else n, dtype=np.int32).reshape(-1)[:nm]
+    if len(nn) != nm or (nm and (nn.min() < 0 or nn.max() > amax)):
+        raise ValueError("n must hold nm atom counts in 0..amax")
+    x, _ = to_device(qa[:nm], torch.float64)
+    zd, _ = to_device(z[:nm] if is_torch(z) else np.asarray(z, dtype=np.float64)[:nm],
+                      torch.float64)
+    nd, _ = to_device(nn, torch.int32)
+    return x, zd, nd, nn, nm, amax
+
+
+def _arad_fixed_kernel(x, zd, nd, nm, amax, sigma, lam):
+    K = torch.empty((nm, nm), dtype=torch.float64, device=device())
+    ws = workspace(_lib.load().fmlb_arad_workspace_bytes(nm, nm, amax, 1))
+    _lib.call("fmlb_arad_alpha_kernel_f64", _lib.ptr(x), _lib.ptr(zd), _lib.ptr(nd), nm, amax,
+              float(sigma), float(lam), _lib.ptr(K), _lib.ptr(ws), ws.numel(),
+              _lib.stream_handle())
+    return K
+
+
+def fget_kernel_arad(q, z, n, sigma, nm):
+    """The routine fml.kernels exports from its Fortran (farad_kernels.f90:95-227;
+    f2py argument order): the symmetric ARAD kernel (nm, nm) of the first nm
+    molecules for one sigma, with the routine's fixed width 0.2, cut 6,
+    r_width 1, c_width 0.5 and eps 1e-11 (the matrix fget_alpha_arad factors,
+    without lambda)."""
+    x, zd, nd, nn, nm, amax = _alpha_inputs(q, z, n, nm)
+    if nm == 0:
+        return np.zeros((0, 0))
+    if sigma <= 0:
+        raise ValueError("sigma must be positive")
+    return to_output(_arad_fixed_kernel(x, zd, nd, nm, amax, sigma, 0.0), not is_torch(q))
+
+
 def fget_alpha_arad(q, z, n, y, sigma, lambda_, alpha=None):
     """Explicit-inverse ARAD KRR weights, the routine fml.kernels exports from
     its Fortran (farad_kernels.f90:231-436; the f2py argument order is kept).
@@ -457,26 +499,11 @@ def fget_alpha_arad(q, z, n, y, sigma, lambda_, alpha=None):
     A non-positive pivot prints the reference's DPOTRF warning as a
     CholeskyWarning, and the weights are NaN.
     """
-    qa = q if is_torch(q) else np.asarray(q, dtype=np.float64)
-    if qa.ndim != 4 or qa.shape[2] != 5 or qa.shape[3] != qa.shape[1]:
-        raise ValueError("q must be (nm, amax, 5, amax)")
-    nm, amax = qa.shape[0], qa.shape[1]
-    nn = np.asarray(n.cpu() if is_torch(n) else n, dtype=np.int32).reshape(-1)
-    if len(nn) != nm or (nm and (nn.min() < 0 or nn.max() > amax)):
-        raise ValueError("n must hold nm atom counts in 0..amax")
+    x, zd, nd, nn, nm, amax = _alpha_inputs(q, z, n)
     if len(y) != nm:
         raise ValueError("y must hold one value per molecule")
-    x, _ = to_device(qa, torch.float64)
-    zd, _ = to_device(z if is_torch(z) else np.asarray(z, dtype=np.float64), torch.float64)
-    nd, _ = to_device(nn, torch.int32)
     yd, _ = to_device(y if is_torch(y) else np.asarray(y, dtype=np.float64), torch.float64)
-    dev = device()
-    K = torch.empty((nm, nm), dtype=torch.float64, device=dev)
-    ws = workspace(_lib.load().fmlb_arad_workspace_bytes(nm, nm, amax, 1))
-    _lib.call("fmlb_arad_alpha_kernel_f64", _lib.ptr(x), _lib.ptr(zd), _lib.ptr(nd), nm, amax,
-              float(sigma), float(lambda_), _lib.ptr(K), _lib.ptr(ws), ws.numel(),
-              _lib.stream_handle())
-    del ws
+    K = _arad_fixed_kernel(x, zd, nd, nm, amax, sigma, lambda_)
     vals = _explicit_inverse_weights(K, yd, nn)  # :391-432
     if alpha is None:
         return vals

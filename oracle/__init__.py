@@ -294,6 +294,18 @@ def get_prediction_from_distance(D2, N2, alpha, sigma):
     return Y
 
 
+def fget_kernel_arad(q, z, n, sigma, nm):
+    """farad_kernels.f90:95-227: the fixed-parameter symmetric ARAD kernel of
+    the first nm molecules (eps 1e-11), from oracle.c."""
+    q = np.ascontiguousarray(np.asarray(q, dtype=np.float64)[:nm])
+    z = np.ascontiguousarray(np.asarray(z, dtype=np.float64)[:nm])
+    n = np.ascontiguousarray(np.asarray(n)[:nm], dtype=np.int32)
+    K = np.zeros((nm, nm))
+    _lib().orc_arad_alpha_kernel(_p(q), _p(z), _p(n, _ip), nm, q.shape[1],
+                                 ctypes.c_double(sigma), ctypes.c_double(0.0), _p(K))
+    return K
+
+
 def fget_alpha_arad(q, z, n, y, sigma, lambda_):
     """farad_kernels.f90:231-436: K + lambda I from oracle.c, then LAPACK
     dpotrf('U'), dpotri('U') and BLAS dsymv('U') as the routine calls them

@@ -494,6 +494,17 @@ def test_l2_distance_arad_synthetic(oracle_mod, nm1, nm2, nmax, seed):
     np.testing.assert_allclose(D, ref, rtol=1e-12, atol=1e-12)
 
 
+def test_fget_kernel_arad_vs_oracle(oracle_mod):
+    X, Z = _arad_set(oracle_mod, 30, 12, 65, 1e6)
+    n = np.array([len(z) for z in Z], np.int32)
+    zp = np.zeros((30, 12, 2))
+    for i, z in enumerate(Z):
+        zp[i, :len(z)] = ptp_of(z)
+    K = fml_b200.fget_kernel_arad(X, zp, n, 1.5, 25)  # the first 25 molecules
+    assert K.shape == (25, 25)
+    np.testing.assert_allclose(K, oracle_mod.fget_kernel_arad(X, zp, n, 1.5, 25), rtol=1e-12)
+
+
 def test_fget_alpha_arad_not_positive_definite(oracle_mod):
     X, Z = _arad_set(oracle_mod, 6, 8, 64, 1e6)
     n = np.array([len(z) for z in Z], np.int32)
