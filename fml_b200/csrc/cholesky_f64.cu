@@ -800,21 +800,44 @@ extern "C" size_t fmlb_potrf_workspace_bytes(int n) {
            ((size_t)n * sizeof(double) + 255) / 256 * 256;
 }
 
-// Per host thread and device: the high-priority stream that runs the panel
-// chain (strip update, diagonal block, panel solve) of the lookahead, and two
-// events to order it against the caller's stream.
+// Per host thread, device and caller stream: the high-priority stream that
+// runs the panel chain (strip update, diagonal block, panel solve) of the
+// lookahead, and two events to order it against the caller's stream.
+// Factorisations issued on different caller streams get different panel
+// streams, so they can overlap: one's narrow final steps run under another's
+// bulk updates. Past kPerCaller caller streams a thread shares one entry per
+// device; its panel stream then serialises those callers' panel chains, which
+// is slower but still ordered correctly, since every wait names the event
+// recorded by the same call.
 struct Lookahead {
     cudaStream_t panel = nullptr;
     cudaEvent_t main_done = nullptr, panel_done = nullptr;
 };
 
-static int lookahead_for_device(Lookahead **out) {
+static int lookahead_for(cudaStream_t caller, Lookahead **out) {
     using namespace fmlb;
-    static thread_local Lookahead per_dev[64];
+    constexpr int kPerCaller = 16;
+    struct Entry {
+        int dev = -1;
+        cudaStream_t caller = nullptr;
+        Lookahead la;
+    };
+    static thread_local Entry by_caller[kPerCaller];
+    static thread_local Lookahead shared_per_dev[64];
     int dev = 0;
     FMLB_TRY(cuda_status(cudaGetDevice(&dev), "fmlb_potrf_f64: cudaGetDevice"));
     FMLB_REQUIRE(dev >= 0 && dev < 64, "fmlb_potrf_f64: device %d out of range", dev);
-    Lookahead &L = per_dev[dev];
+    Lookahead *lp = nullptr;
+    for (int i = 0; i < kPerCaller && !lp; ++i)
+        if (by_caller[i].dev == dev && by_caller[i].caller == caller) lp = &by_caller[i].la;
+    for (int i = 0; i < kPerCaller && !lp; ++i)
+        if (by_caller[i].dev < 0) {
+            by_caller[i].dev = dev;
+            by_caller[i].caller = caller;
+            lp = &by_caller[i].la;
+        }
+    if (!lp) lp = &shared_per_dev[dev];
+    Lookahead &L = *lp;
     if (!L.panel) {
         int lo = 0, hi = 0;
         FMLB_TRY(cuda_status(cudaDeviceGetStreamPriorityRange(&lo, &hi), "stream priorities"));
@@ -886,7 +909,7 @@ extern "C" int fmlb_potrf_f64(double *A, long long lda, int n, void *work, int *
     FMLB_REQUIRE(A && work, "fmlb_potrf_f64: null pointer");
     FMLB_TRY(set_smem_attrs());
     Lookahead *la = nullptr;
-    FMLB_TRY(lookahead_for_device(&la));
+    FMLB_TRY(lookahead_for(st, &la));
     double *Linv = static_cast<double *>(work);
     const int W = outer_width(n);
     const int nob = ceil_div(n, W);

@@ -78,6 +78,11 @@ class KRRPipeline:
         self.pwork = torch.empty(pb, dtype=torch.uint8, device=self.dev)
         self._sig_arr = (ctypes.c_double * self.nsig)(*self.sigmas)
         self._sig_ptr = ctypes.cast(self._sig_arr, ctypes.POINTER(ctypes.c_double))
+        # one stream per sigma: the factorisations overlap, so one's narrow
+        # final outer steps run under another's bulk updates
+        self._sig_streams = [torch.cuda.Stream(device=self.dev) for _ in range(self.nsig)]
+        self._fork = torch.cuda.Event()
+        self._joins = [torch.cuda.Event() for _ in range(self.nsig)]
 
     def launches_per_run(self):
         """Kernel launches of one ``run`` (mirrors the loops in the C library)."""
@@ -106,14 +111,23 @@ class KRRPipeline:
         fn = "fmlb_gaussian_kernel_f64" if self.kind == 0 else "fmlb_laplacian_kernel_f64"
         _lib.call(fn, _lib.ptr(self.X), n, d, _lib.ptr(self.X), n, d, d, self._sig_ptr, self.nsig,
                   _lib.ptr(self.K), n, n * n, 1, s)
+        main = stream if stream is not None else torch.cuda.current_stream(self.dev)
+        self._fork.record(main)
         for k in range(self.nsig):
             Kk = self.K[k]
-            _lib.call("fmlb_add_diagonal_f64", _lib.ptr(Kk), n, n, self.lam, s)
+            sk = self._sig_streams[k]
+            sk.wait_event(self._fork)
+            h = _lib.stream_handle(sk)
+            _lib.call("fmlb_add_diagonal_f64", _lib.ptr(Kk), n, n, self.lam, h)
             _lib.call("fmlb_potrf_f64", _lib.ptr(Kk), n, n, _lib.ptr(self.work[k]),
-                      _lib.ptr(self.info[k:k + 1]), s)
-            self.alpha[k].copy_(y_train)
+                      _lib.ptr(self.info[k:k + 1]), h)
+            with torch.cuda.stream(sk):
+                self.alpha[k].copy_(y_train)
             _lib.call("fmlb_potrs_f64", _lib.ptr(Kk), n, n, _lib.ptr(self.work[k]),
-                      _lib.ptr(self.alpha[k]), s)
+                      _lib.ptr(self.alpha[k]), h)
+            self._joins[k].record(sk)
+        for ev in self._joins:
+            main.wait_event(ev)
         if self.n_test:
             Xq = self.X[n:]
             _lib.call("fmlb_kernel_predict_f64", self.kind, _lib.ptr(Xq), self.n_test, d,
