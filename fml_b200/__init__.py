@@ -30,7 +30,7 @@ from .descriptors import (generate_arad_descriptors, generate_coulomb_matrices,
                           generate_local_coulomb_matrices)
 from .distance import get_l2_distance_arad, l2_distance, manhattan_distance, p_distance
 from .kernels import (fget_alpha_arad, fget_atomic_distance_arad, fget_atomic_kernels_arad,
-                      fget_kernel_arad,
+                      fget_kernel_arad, fget_vector_kernels_gaussian,
                       gaussian_kernel, get_alpha, get_alpha_from_distance,
                       get_atomic_kernels_arad, get_atomic_kernels_gaussian,
                       get_atomic_kernels_laplacian, get_atomic_symmetric_kernels_arad,
@@ -41,7 +41,7 @@ from .xyz import read_xyz_batch
 __all__ = [
     "Molecule", "gaussian_kernel", "laplacian_kernel", "get_atomic_kernels_arad",
     "get_atomic_symmetric_kernels_arad", "fget_atomic_kernels_arad", "fget_alpha_arad",
-    "fget_kernel_arad",
+    "fget_kernel_arad", "fget_vector_kernels_gaussian",
     "fget_atomic_distance_arad", "get_atomic_kernels_gaussian", "get_atomic_kernels_laplacian",
     "get_alpha", "get_prediction", "get_alpha_from_distance", "get_prediction_from_distance",
     "get_l2_distance_arad", "manhattan_distance", "l2_distance", "p_distance", "cho_solve",

@@ -4,7 +4,8 @@
 * ``laplacian_kernel(A, B, sigma)`` -> flaplacian_kernel (fkernels.f90:351-377)
 * ``get_atomic_kernels_arad`` / ``get_atomic_symmetric_kernels_arad``
   -> fget_kernels_arad / fget_symmetric_kernels_arad (farad_kernels.f90:439-755)
-* ``get_atomic_kernels_gaussian`` / ``get_atomic_kernels_laplacian`` ->
+* ``get_atomic_kernels_gaussian`` / ``get_atomic_kernels_laplacian`` and
+  the directly exported ``fget_vector_kernels_gaussian`` ->
   fget_vector_kernels_gaussian / fget_vector_kernels_laplacian
   (fkernels.f90:23-162), sums over atom pairs of per-atom descriptors
 * ``fget_alpha_arad`` / ``fget_kernel_arad`` -> the routines of those names
@@ -592,6 +593,18 @@ def get_atomic_kernels_laplacian(x1, x2, N1, N2, sigmas):
     a, as_np = _atom_rows(x1)
     b = a if x2 is x1 else _atom_rows(x2)[0]
     return to_output(_vector_kernels(1, a, b, N1, N2, sigmas), as_np)
+
+
+def fget_vector_kernels_gaussian(q1, q2, n1, n2, sigmas, nm1, nm2, nsigmas):
+    """The routine fml.kernels exports from its Fortran (fkernels.f90:93-162;
+    f2py argument order): q1 / q2 (d, amax, nm) per-atom descriptors, n1 / n2
+    atoms per molecule -> (nsigmas, nm1, nm2), K[k, i, j] = sum over atom pairs
+    of exp(-|q1_ia - q2_ja|^2 / (2 sigma_k^2))."""
+    if len(n1) != nm1 or len(n2) != nm2 or len(np.atleast_1d(sigmas)) != nsigmas:
+        raise ValueError("nm1 / nm2 / nsigmas do not match n1 / n2 / sigmas")
+    a, as_np = _atom_rows(q1)
+    b = a if q2 is q1 else _atom_rows(q2)[0]
+    return to_output(_vector_kernels(0, a, b, n1, n2, sigmas), as_np)
 
 
 def _local_cm_rows(mols):

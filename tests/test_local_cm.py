@@ -189,3 +189,7 @@ def test_atomic_kernels_dropins(oracle_mod, golden):
     np.testing.assert_allclose(Kl, refl, rtol=1e-13)
     with pytest.raises(ValueError):
         fml_b200.get_atomic_kernels_laplacian(xf, xf, n, n, [-1.0])
+    # the f2py routine exported as is: same arrays, explicit sizes
+    Kf = fml_b200.fget_vector_kernels_gaussian(xf[:, :, :4], xf[:, :, 4:], n[:4], n[4:], sig, 4,
+                                               len(n) - 4, 2)
+    np.testing.assert_allclose(Kf, ref, rtol=1e-13)
