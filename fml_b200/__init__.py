@@ -3,6 +3,7 @@
 Drop-in names (same signatures and error behaviour as the reference):
 
 * ``Molecule`` with ``read_xyz``, ``generate_coulomb_matrix``,
+  ``generate_unsorted_coulomb_matrix``,
   ``generate_local_coulomb_matrix``, ``generate_atomic_coulomb_matrix``,
   ``generate_arad_descriptor`` (fml/fml.py)
 * ``gaussian_kernel``, ``laplacian_kernel``, ``get_atomic_kernels_arad``,
@@ -27,7 +28,7 @@ fallback: without the built library or a CUDA device the calls raise.
 from .cho_solve import CholeskyWarning, cho_invert, cho_solve
 from .data import NUCLEAR_CHARGE, PTP
 from .descriptors import (generate_arad_descriptors, generate_coulomb_matrices,
-                          generate_local_coulomb_matrices)
+                          generate_local_coulomb_matrices, generate_unsorted_coulomb_matrices)
 from .distance import get_l2_distance_arad, l2_distance, manhattan_distance, p_distance
 from .kernels import (fget_alpha_arad, fget_atomic_distance_arad, fget_atomic_kernels_arad,
                       fget_kernel_arad, fget_vector_kernels_gaussian,
@@ -47,6 +48,7 @@ __all__ = [
     "get_l2_distance_arad", "manhattan_distance", "l2_distance", "p_distance", "cho_solve",
     "cho_invert",
     "CholeskyWarning",
-    "generate_coulomb_matrices", "generate_local_coulomb_matrices", "generate_arad_descriptors",
+    "generate_coulomb_matrices", "generate_unsorted_coulomb_matrices",
+    "generate_local_coulomb_matrices", "generate_arad_descriptors",
     "read_xyz_batch", "NUCLEAR_CHARGE", "PTP",
 ]

@@ -31,6 +31,7 @@ SIGNATURES = {
     "fmlb_exp_weighted_colsum_f64": (_i, [_vp, _ll, _i, _i, _d, _vp, _vp, _vp, _vp]),
     "fmlb_xyz_scan": (_i, [_vp, _i, _vp, _vp, _i]),
     "fmlb_xyz_parse": (_i, [_vp, _i, _vp, _vp, _vp, _i, _vp, _vp, _vp, _i]),
+    "fmlb_unsorted_coulomb_matrices": (_i, [_vp, _vp, _vp, _i, _i, _vp, _i, _vp, _vp]),
     "fmlb_local_coulomb_matrices": (_i, [_vp, _vp, _vp, _i, _i, _i, _vp, _i, _vp, _vp]),
     "fmlb_vector_kernels_f64": (_i, [_i, _vp, _vp, _i, _i, _vp, _vp, _i, _i, _i, _dp, _i, _vp,
                                      _vp, _vp]),

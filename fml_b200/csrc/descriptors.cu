@@ -125,6 +125,48 @@ cm_sorted_kernel(const double *__restrict__ charges, const double *__restrict__ 
 }
 
 // ---------------------------------------------------------------------------
+// Unsorted Coulomb matrix, fgenerate_unsorted_coulomb_matrix
+// (frepresentations.f90:112-202): the packed lower triangle in the input atom
+// order. One warp per molecule.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+cm_unsorted_kernel(const double *__restrict__ charges, const double *__restrict__ coords,
+                   const int *__restrict__ offsets, int nmol, int nmax, double *__restrict__ cm,
+                   int ldcm, DiagTable diag, int *__restrict__ status) {
+    extern __shared__ double smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mol = blockIdx.x * kWarpsPerBlock + warp;
+    if (mol >= nmol) return;
+    double *X = smem + (size_t)warp * 4 * nmax;
+    double *Y = X + nmax, *Zc = Y + nmax, *Q = Zc + nmax;
+    const int a0 = offsets[mol];
+    int n = offsets[mol + 1] - a0;
+    const int L = nmax * (nmax + 1) / 2;
+    if (n < 0 || n > nmax) {  // rejected on the host; emit a zero row, stay in bounds
+        if (lane == 0 && status) atomicCAS(status, 0, 1);
+        n = 0;
+    }
+    for (int t = lane; t < n; t += 32) {
+        X[t] = coords[3 * (size_t)(a0 + t) + 0];
+        Y[t] = coords[3 * (size_t)(a0 + t) + 1];
+        Zc[t] = coords[3 * (size_t)(a0 + t) + 2];
+        Q[t] = charges[a0 + t];
+    }
+    __syncwarp();
+    double *row = cm + (size_t)mol * ldcm;
+    for (int idx = lane; idx < L; idx += 32) {  // :184-192
+        int m = (int)((sqrt(8.0 * idx + 1.0) - 1.0) * 0.5);
+        while (m * (m + 1) / 2 > idx) --m;
+        while ((m + 1) * (m + 2) / 2 <= idx) ++m;
+        const int q = idx - m * (m + 1) / 2;
+        double v = 0.0;
+        if (m < n) v = (q == m) ? cm_diag(Q[m], diag) : cm_pair(X, Y, Zc, Q, m, q);
+        row[idx] = v;
+    }
+    for (int idx = L + lane; idx < ldcm; idx += 32) row[idx] = 0.0;
+}
+
+// ---------------------------------------------------------------------------
 // Local and atomic Coulomb matrices, one row per atom: the packed lower
 // triangle of the molecule's Coulomb matrix with the atoms reordered around
 // the central atom k.
@@ -430,6 +472,26 @@ extern "C" int fmlb_coulomb_matrices(const double *charges, const double *coords
                        FMLB_STREAM(stream)>>>(charges, coords, offsets, nmol, nmax, cm, ldcm,
                                               cm32, ldcm32, order, diag, status);
     return launch_status("cm_sorted_kernel");
+}
+
+extern "C" int fmlb_unsorted_coulomb_matrices(const double *charges, const double *coords,
+                                              const int *offsets, int nmol, int nmax, double *cm,
+                                              int ldcm, int *status, void *stream) {
+    using namespace fmlb;
+    FMLB_REQUIRE(nmol >= 0, "fmlb_unsorted_coulomb_matrices: nmol < 0");
+    FMLB_REQUIRE(nmax >= 1 && nmax <= 255,
+                 "fmlb_unsorted_coulomb_matrices: nmax=%d outside 1..255", nmax);
+    const int L = nmax * (nmax + 1) / 2;
+    FMLB_REQUIRE(ldcm >= L, "fmlb_unsorted_coulomb_matrices: ldcm=%d < %d", ldcm, L);
+    FMLB_REQUIRE(nmol == 0 || (charges && coords && offsets && cm),
+                 "fmlb_unsorted_coulomb_matrices: null pointer");
+    if (nmol == 0) return FMLB_OK;
+    static const DiagTable diag = make_diag_table();
+    const size_t smem = sizeof(double) * 4 * nmax * kWarpsPerBlock;
+    cm_unsorted_kernel<<<ceil_div(nmol, kWarpsPerBlock), kWarpsPerBlock * 32, smem,
+                         FMLB_STREAM(stream)>>>(charges, coords, offsets, nmol, nmax, cm, ldcm,
+                                                diag, status);
+    return launch_status("cm_unsorted_kernel");
 }
 
 extern "C" int fmlb_local_coulomb_matrices(const double *charges, const double *coords,

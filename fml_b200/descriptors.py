@@ -2,6 +2,8 @@
 
 * ``generate_coulomb_matrices`` — sorted Coulomb matrices, the batched form
   of ``fgenerate_coulomb_matrix`` (fml/representations/frepresentations.f90:23-110).
+* ``generate_unsorted_coulomb_matrices`` — the same matrix in the input atom
+  order (``fgenerate_unsorted_coulomb_matrix``, frepresentations.f90:112-202).
 * ``generate_local_coulomb_matrices`` — one Coulomb matrix per atom, the
   batched form of ``fgenerate_local_coulomb_matrix`` (kind "local",
   frepresentations.f90:204-294) and ``fgenerate_atomic_coulomb_matrix``
@@ -75,6 +77,23 @@ def generate_coulomb_matrices(charges, coords, offsets, size=23, return_order=Fa
     if cm32 is not None:
         out.append(cm32)
     return out[0] if len(out) == 1 else tuple(out)
+
+
+def generate_unsorted_coulomb_matrices(charges, coords, offsets, size=23):
+    """Unsorted Coulomb matrices, (nmol, size*(size+1)/2) float64: the packed
+    lower triangle in the input atom order (fgenerate_unsorted_coulomb_matrix,
+    frepresentations.f90:112-202)."""
+    nmol = _check_offsets(offsets, size, "generate_unsorted_coulomb_matrices", charges, coords)
+    if size > 255:
+        raise ValueError("generate_unsorted_coulomb_matrices: size > 255 is not supported")
+    L = size * (size + 1) // 2
+    z, as_np = to_device(charges, torch.float64)
+    r, _ = to_device(coords, torch.float64)
+    off, _ = to_device(offsets, torch.int32)
+    cm = torch.empty((nmol, L), dtype=torch.float64, device=device())
+    _lib.call("fmlb_unsorted_coulomb_matrices", _lib.ptr(z), _lib.ptr(r), _lib.ptr(off), nmol,
+              size, _lib.ptr(cm), L, None, _lib.stream_handle())
+    return to_output(cm, as_np)
 
 
 LOCAL_CM_KINDS = {"local": 0, "atomic": 1}

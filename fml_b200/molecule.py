@@ -10,7 +10,7 @@ import numpy as np
 
 from .data import NUCLEAR_CHARGE
 from .descriptors import (generate_arad_descriptors, generate_coulomb_matrices,
-                          generate_local_coulomb_matrices)
+                          generate_local_coulomb_matrices, generate_unsorted_coulomb_matrices)
 
 
 class Molecule:
@@ -42,6 +42,11 @@ class Molecule:
         """fml/fml.py:64-66 -> sorted CM, packed lower triangle (size*(size+1)/2,)."""
         z, r, off = self._packed()
         self.coulomb_matrix = generate_coulomb_matrices(z, r, off, size=size)[0]
+
+    def generate_unsorted_coulomb_matrix(self, size=23):
+        """fml/fml.py:68-70 -> CM in the input atom order, packed lower triangle."""
+        z, r, off = self._packed()
+        self.unsorted_coulomb_matrix = generate_unsorted_coulomb_matrices(z, r, off, size=size)[0]
 
     def generate_local_coulomb_matrix(self, calc="all", size=23):
         """fml/fml.py:72-74 -> (natoms, size*(size+1)/2), one row per central atom.

@@ -113,6 +113,15 @@ int fmlb_xyz_parse(const char *const *paths, int nfiles, const int *offsets,
                    const char *const *table_symbols, const double *table_charges, int ntable,
                    double *charges, double *coords, int *symbol_index, int nthreads);
 
+/* Unsorted Coulomb matrices: one packed lower triangle per molecule in the
+ * input atom order, the replacement for fgenerate_unsorted_coulomb_matrix
+ * (fml/representations/frepresentations.f90:112-202) as called by
+ * Molecule.generate_unsorted_coulomb_matrix (fml/fml.py:68-70). cm (nmol, ldcm),
+ * zero padded; status as for fmlb_coulomb_matrices. */
+int fmlb_unsorted_coulomb_matrices(const double *charges, const double *coords, const int *offsets,
+                                   int nmol, int nmax, double *cm, int ldcm, int *status,
+                                   void *stream);
+
 /* ------------------------------------------------------------------------
  * Local / atomic Coulomb matrices: one packed lower-triangle row per atom.
  * Replaces fgenerate_local_coulomb_matrix (kind 0,

@@ -48,6 +48,7 @@ def _lib():
         lib.orc_cm_sorted.restype = ctypes.c_int
         lib.orc_cm_sorted_batch.restype = ctypes.c_int
         lib.orc_cm_local_batch.restype = ctypes.c_int
+        lib.orc_cm_unsorted_batch.restype = ctypes.c_int
         lib.orc_potrf_upper.restype = ctypes.c_int
         lib.orc_num_threads.restype = ctypes.c_int
         _LIB = lib
@@ -92,6 +93,17 @@ def coulomb_matrices(charges, coords, offsets, size=23, return_order=False):
     if rc:
         raise ValueError("molecule has more atoms than size")
     return (cm, order) if return_order else cm
+
+
+def unsorted_coulomb_matrices(charges, coords, offsets, size=23):
+    """frepresentations.f90:112-202 restated in oracle.c: (nmol, size*(size+1)/2)."""
+    z = np.ascontiguousarray(charges, dtype=np.float64)
+    r = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1, 3)
+    off = np.ascontiguousarray(offsets, dtype=np.int32)
+    cm = np.zeros((len(off) - 1, size * (size + 1) // 2))
+    if _lib().orc_cm_unsorted_batch(len(off) - 1, _p(off, _ip), _p(z), _p(r), size, _p(cm)):
+        raise ValueError("molecule has more atoms than size")
+    return cm
 
 
 def local_coulomb_matrices(charges, coords, offsets, size=23, kind="local"):

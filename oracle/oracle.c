@@ -111,6 +111,42 @@ int orc_cm_sorted_batch(int nmol, const int *offsets, const double *charges,
 }
 
 /* ------------------------------------------------------------------------ */
+/* Unsorted Coulomb matrix: frepresentations.f90:112-202 (identity order)     */
+/* ------------------------------------------------------------------------ */
+int orc_cm_unsorted_batch(int nmol, const int *offsets, const double *charges,
+                          const double *coords, int nmax, double *cm)
+{
+    const int len = nmax * (nmax + 1) / 2;
+    int bad = 0;
+    for (int mol = 0; mol < nmol; ++mol) {
+        const int a0 = offsets[mol], n = offsets[mol + 1] - offsets[mol];
+        double *row = cm + (size_t)mol * len;
+        for (int t = 0; t < len; ++t) row[t] = 0.0;
+        if (n < 0 || n > nmax) { bad = 1; continue; }
+        const double *z = charges + a0, *r = coords + 3 * (size_t)a0;
+        for (int m = 0; m < n; ++m) {           /* :184-192 */
+            const int idx = m * (m + 1) / 2;
+            for (int q = 0; q <= m; ++q) {
+                double v;
+                if (q == m) {
+                    v = 0.5 * pow(z[m], 2.4);    /* :161-165 */
+                } else {                          /* :167-178, i = q < j = m */
+                    double dx = r[3 * m + 0] - r[3 * q + 0];
+                    double dy = r[3 * m + 1] - r[3 * q + 1];
+                    double dz = r[3 * m + 2] - r[3 * q + 2];
+                    double s2 = dx * dx;
+                    s2 = s2 + dy * dy;
+                    s2 = s2 + dz * dz;
+                    v = z[q] * z[m] / sqrt(s2);
+                }
+                row[idx + q] = v;
+            }
+        }
+    }
+    return bad ? -1 : 0;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Local / atomic Coulomb matrices: frepresentations.f90:204-294 / :297-390   */
 /* ------------------------------------------------------------------------ */
 /* One molecule: cm (n, len) rows, kind 0 local, 1 atomic. Returns -1 if n > nmax. */

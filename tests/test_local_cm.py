@@ -193,3 +193,45 @@ def test_atomic_kernels_dropins(oracle_mod, golden):
     Kf = fml_b200.fget_vector_kernels_gaussian(xf[:, :, :4], xf[:, :, 4:], n[:4], n[4:], sig, 4,
                                                len(n) - 4, 2)
     np.testing.assert_allclose(Kf, ref, rtol=1e-13)
+
+
+# ------------------------------------------------------- unsorted Coulomb matrix
+def _sorted_order_batch(oracle_mod, z, r, off, size):
+    """Atoms of every molecule permuted into the sorted-CM order (the oracle's
+    order, bit-exact against the reference's row-norm sort)."""
+    _, order = oracle_mod.coulomb_matrices(z, r, off, size, return_order=True)
+    idx = np.concatenate([off[m] + order[m][:off[m + 1] - off[m]] for m in range(len(off) - 1)])
+    return z[idx], r[idx]
+
+
+def test_unsorted_cm_oracle_pinned_by_permutation(golden, oracle_mod):
+    """The unsorted CM of atoms already in sorted order is the sorted CM: the
+    oracle against the reference's sorted matrices (representations.py:63-113),
+    which pins it (the reference has no Python unsorted version)."""
+    g = golden
+    for pre, key in (("xyz_", "cm_xyz_s23"), ("syn12_", "cm_syn_s23")):
+        z, r, off = g[pre + "charges"], g[pre + "coords"], g[pre + "offsets"]
+        zs, rs = _sorted_order_batch(oracle_mod, z, r, off, 23)
+        np.testing.assert_allclose(oracle_mod.unsorted_coulomb_matrices(zs, rs, off, 23), g[key],
+                                   rtol=1e-14, atol=1e-13)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nmax,seed,nmol", [(23, 13, 300), (40, 14, 50), (1, 15, 9)])
+def test_unsorted_cm_vs_oracle(oracle_mod, golden, nmax, seed, nmol):
+    import fml_b200
+    b = synthetic.generate(nmol, nmax=nmax, seed=seed, nmin=1)
+    cm = fml_b200.generate_unsorted_coulomb_matrices(b.charges, b.coords, b.offsets, size=nmax)
+    np.testing.assert_allclose(cm, oracle_mod.unsorted_coulomb_matrices(b.charges, b.coords,
+                                                                        b.offsets, nmax),
+                               rtol=1e-14, atol=0)
+    g = golden
+    z, r, off = g["xyz_charges"], g["xyz_coords"], g["xyz_offsets"]
+    zs, rs = _sorted_order_batch(oracle_mod, z, r, off, 23)
+    m = fml_b200.Molecule()
+    m.nuclear_charges = list(zs[off[2]:off[3]])
+    m.coordinates = rs[off[2]:off[3]]
+    m.natoms = len(m.nuclear_charges)
+    m.generate_unsorted_coulomb_matrix(size=23)
+    np.testing.assert_allclose(m.unsorted_coulomb_matrix, g["cm_xyz_s23"][2], rtol=1e-14,
+                               atol=1e-13)
