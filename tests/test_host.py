@@ -108,3 +108,22 @@ def test_descriptor_offsets_checked_before_launch(fn):
         getattr(fml_b200, fn)(z, r, [0, 2, 6], size=8)
     with pytest.raises(ValueError):
         getattr(fml_b200, fn)(z, r, [-1, 2], size=8)
+
+
+def test_segment_sums_and_counts():
+    """Per-molecule sums of per-atom values (fkernels.f90:532-535, :696-698),
+    including empty molecules, and the atom-count checks."""
+    from fml_b200.kernels import _counts, _segment_sums
+    n, off = _counts([2, 0, 3, 0], "t")
+    assert n.tolist() == [2, 0, 3, 0] and off.tolist() == [0, 2, 2, 5, 5]
+    v = np.arange(1.0, 7.0)  # one extra value past the last molecule is ignored
+    np.testing.assert_array_equal(_segment_sums(v, off), [3.0, 0.0, 12.0, 0.0])
+    np.testing.assert_array_equal(_segment_sums(v, _counts([0, 0], "t")[1]), [0.0, 0.0])
+    with pytest.raises(ValueError):
+        _counts([1, -1], "t")
+
+
+def test_vector_kernel_dropin_checks_sizes():
+    with pytest.raises(ValueError):
+        fml_b200.fget_vector_kernels_gaussian(np.zeros((3, 2, 4)), np.zeros((3, 2, 5)),
+                                              [1] * 4, [1] * 5, [1.0], 4, 4, 1)
