@@ -37,7 +37,7 @@ from .kernels import (fget_alpha_arad, fget_atomic_distance_arad, fget_atomic_ke
                       get_atomic_kernels_laplacian, get_atomic_symmetric_kernels_arad,
                       get_prediction, get_prediction_from_distance, laplacian_kernel)
 from .molecule import Molecule
-from .xyz import read_xyz_batch
+from .xyz import read_xyz_batch, read_xyz_molecules
 
 __all__ = [
     "Molecule", "gaussian_kernel", "laplacian_kernel", "get_atomic_kernels_arad",
@@ -50,5 +50,5 @@ __all__ = [
     "CholeskyWarning",
     "generate_coulomb_matrices", "generate_unsorted_coulomb_matrices",
     "generate_local_coulomb_matrices", "generate_arad_descriptors",
-    "read_xyz_batch", "NUCLEAR_CHARGE", "PTP",
+    "read_xyz_batch", "read_xyz_molecules", "NUCLEAR_CHARGE", "PTP",
 ]

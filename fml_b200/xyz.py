@@ -95,3 +95,22 @@ def _call(name, *args):
         if "unknown element " in msg:  # the reference's NUCLEAR_CHARGE[...] KeyError
             raise KeyError(msg.rsplit("unknown element ", 1)[1]) from None
         raise
+
+
+def read_xyz_molecules(paths, nthreads=0):
+    """``Molecule`` objects for many files in one native pass, each as
+    ``Molecule.read_xyz`` (fml/fml.py:109-132) would fill it: ``natoms`` (the
+    declared count), ``atomtypes``, ``nuclear_charges`` and ``coordinates``."""
+    from .molecule import Molecule
+    batch = read_xyz_batch(paths, nthreads=nthreads)
+    coords = batch.coords.numpy()
+    mols = []
+    for m in range(len(batch.offsets) - 1):
+        a, b = int(batch.offsets[m]), int(batch.offsets[m + 1])
+        mol = Molecule()
+        mol.natoms = int(batch.natoms_declared[m])
+        mol.atomtypes = batch.atomtypes(m)
+        mol.nuclear_charges = [NUCLEAR_CHARGE[t] for t in mol.atomtypes]  # the table's values
+        mol.coordinates = coords[a:b].copy()
+        mols.append(mol)
+    return mols

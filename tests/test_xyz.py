@@ -80,6 +80,20 @@ def test_edge_cases_match_python_reader(tmp_path, newline):
     np.testing.assert_array_equal(batch.coords.numpy(), m.coordinates)
 
 
+def test_molecules_match_python_reader(golden, tmp_path):
+    g = golden
+    off, sym = g["xyz_offsets"], g["xyz_symbols"]
+    paths = [_write(tmp_path / ("m%d.xyz" % i),
+                    _xyz_text(sym[off[i]:off[i + 1]], g["xyz_coords"][off[i]:off[i + 1]],
+                              declared=off[i + 1] - off[i] + (i % 2)))
+             for i in range(len(off) - 1)]
+    for p, m in zip(paths, fml_b200.read_xyz_molecules(paths)):
+        r = _python_read(p)
+        assert m.natoms == r.natoms and m.atomtypes == r.atomtypes
+        assert m.nuclear_charges == r.nuclear_charges
+        np.testing.assert_array_equal(m.coordinates, r.coordinates)
+
+
 def test_blank_line_ends_atoms_and_empty_molecule(tmp_path):
     p1 = _write(tmp_path / "a.xyz", "2\n\nH 0 0 0\n\nH 0 0 1\n")
     p2 = _write(tmp_path / "b.xyz", "0\ncomment\n")
