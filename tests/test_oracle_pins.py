@@ -125,3 +125,21 @@ def test_oracle_symmetric_equals_general(golden, oracle_mod):
     s = [0.5, 2.0]
     np.testing.assert_allclose(oracle_mod.get_atomic_symmetric_kernels_arad(x, Z, s),
                                oracle_mod.get_atomic_kernels_arad(x, x, Z, Z, s), rtol=1e-13)
+
+
+def test_gaussian_laplacian_oracle_cross_checked_by_scipy(golden, oracle_mod):
+    """fgaussian_kernel / flaplacian_kernel (fkernels.f90:317-377) have no test
+    or golden vector in the reference; the oracle's restatement is checked
+    against an independent distance code (scipy cdist) on the reference's own
+    sorted CMs."""
+    from scipy.spatial.distance import cdist
+    g = golden
+    X = g["cm_syn_s23"]
+    A, B = X[:40].T, X[40:].T  # reference layout (d, n)
+    for sigma in (50.0, 724.0):
+        np.testing.assert_allclose(oracle_mod.gaussian_kernel(A, B, sigma),
+                                   np.exp(-cdist(A.T, B.T, "sqeuclidean") / (2 * sigma ** 2)),
+                                   rtol=1e-12, atol=1e-300)
+        np.testing.assert_allclose(oracle_mod.laplacian_kernel(A, B, sigma),
+                                   np.exp(-cdist(A.T, B.T, "cityblock") / sigma),
+                                   rtol=1e-12, atol=1e-300)
