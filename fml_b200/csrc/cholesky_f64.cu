@@ -808,7 +808,9 @@ extern "C" size_t fmlb_potrf_workspace_bytes(int n) {
 // bulk updates. Past kPerCaller caller streams a thread shares one entry per
 // device; its panel stream then serialises those callers' panel chains, which
 // is slower but still ordered correctly, since every wait names the event
-// recorded by the same call.
+// recorded by the same call. The streams and events live for the life of the
+// host thread and do not survive cudaDeviceReset: a process that resets a
+// device must not factor on it again from the same thread.
 struct Lookahead {
     cudaStream_t panel = nullptr;
     cudaEvent_t main_done = nullptr, panel_done = nullptr;

@@ -493,6 +493,10 @@ extern "C" int fmlb_gaussian_kernel_tc(const double *A, int na, int lda, const d
     FMLB_REQUIRE(nsigma >= 1 && nsigma <= TC_MAXSIG && sigmas_host,
                  "fmlb_gaussian_kernel_tc: nsigma must be 1..%d", TC_MAXSIG);
     FMLB_REQUIRE(ldk >= nb, "fmlb_gaussian_kernel_tc: ldk < nb");
+    FMLB_REQUIRE(nsigma == 1 || sigma_stride >= (long long)(na - 1) * ldk + nb,
+                 "fmlb_gaussian_kernel_tc: sigma_stride %lld overlaps the previous sigma's "
+                 "(na - 1) * ldk + nb = %lld elements", sigma_stride,
+                 (long long)(na - 1) * ldk + nb);
     FMLB_REQUIRE(mu && status && K, "fmlb_gaussian_kernel_tc: null pointer");
     if (symmetric)
         FMLB_REQUIRE(A == B && na == nb && lda == ldb, "fmlb_gaussian_kernel_tc: symmetric needs A == B");

@@ -12,6 +12,8 @@
 
 #include <algorithm>
 
+#include <limits.h>
+
 #include "common.cuh"
 
 namespace fmlb {
@@ -184,6 +186,9 @@ extern "C" int fmlb_kernel_predict_f64(int kind, const double *Xq, int nq, int l
     FMLB_REQUIRE(nsigma >= 1 && nsigma <= MAXSIG && sigmas_host,
                  "fmlb_kernel_predict_f64: nsigma must be 1..%d", MAXSIG);
     FMLB_REQUIRE(lda_alpha >= nt && ldy >= nq, "fmlb_kernel_predict_f64: bad alpha / y stride");
+    FMLB_REQUIRE((long long)nsigma * nq < INT_MAX,
+                 "fmlb_kernel_predict_f64: nsigma * nq = %lld must stay below 2^31",
+                 (long long)nsigma * nq);
     if (nq == 0) return FMLB_OK;
     if (nt == 0) {
         for (int s = 0; s < nsigma; ++s)
@@ -235,7 +240,10 @@ extern "C" int fmlb_kernel_predict_f64(int kind, const double *Xq, int nq, int l
 // before any stream capture. All calls share the array; a call fully
 // overwrites the part it reads, so nothing needs clearing between calls, but
 // calls that overlap on the GPU (different streams, or host threads) race on
-// it and must be serialised by the caller.
+// it and must be serialised by the caller. The looked-up address is cached per
+// device for the life of the process: it does not survive cudaDeviceReset
+// (after which the module may load at another address), so a process that
+// resets a device must not call this entry point on it again.
 // ---------------------------------------------------------------------------
 #include <mutex>
 

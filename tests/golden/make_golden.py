@@ -1,9 +1,9 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a container where the reference tree is mounted (default
-``/root/reference``, override with ``FML_REFERENCE``)::
+Run where the reference tree is available, naming its root in
+``FML_REFERENCE``::
 
-    python tests/golden/make_golden.py
+    FML_REFERENCE=<path to the andersx/fml checkout> python tests/golden/make_golden.py
 
 The reference is Python 2 + f2py Fortran, and no Fortran compiler is
 available, so only its Python-3-runnable parts are executed here:
@@ -41,7 +41,9 @@ sys.path.insert(0, ROOT)
 
 from fml_b200.synthetic import generate  # noqa: E402
 
-REF = os.environ.get("FML_REFERENCE", "/root/reference")
+REF = os.environ.get("FML_REFERENCE")
+if not REF:
+    sys.exit("make_golden.py: set FML_REFERENCE to the root of the andersx/fml checkout")
 
 
 def _load_module(name, path):
