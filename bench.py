@@ -60,7 +60,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--stages", nargs="?", const="all", default=None,
                    help="time each hot-path kernel on its own (one JSON line per stage); "
-                        "'arad' times only the ARAD kernels")
+                        "'arad' times only the ARAD kernels, 'build' only the descriptors "
+                        "and kernel-matrix builds")
     p.add_argument("--workload", default="krr",
                    choices=["krr", "batched", "serving", "small", "arad"],
                    help="krr: the large-N KRR step (default, the headline line); batched: "
@@ -563,6 +564,9 @@ def run_stages(a):
           "max_abs_err_vs_fp64": _max_abs_diff(torch, Kl32[:, :nl, :nl], Kl),
           "error_sample": "leading %d x %d block" % (nl, nl)})
     del Kl32, Kl
+    if a.stages == "build":  # descriptors and kernel builds only (small ncu captures)
+        del keep
+        return out
 
     # --- Cholesky, solve, prediction ------------------------------------------
     K1 = torch.empty((n, n), dtype=torch.float64, device=dev)

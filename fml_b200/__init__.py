@@ -18,7 +18,9 @@ Drop-in names (same signatures and error behaviour as the reference):
 
 Batched forms: ``read_xyz_batch`` (many .xyz files into one packed buffer),
 ``generate_coulomb_matrices``, ``generate_local_coulomb_matrices``,
-``generate_arad_descriptors``.
+``generate_arad_descriptors``; the fused KRR pipeline ``krr_fit_predict`` /
+``KRRPipeline`` (descriptors, kernels for every sigma, factorisations, solves
+and prediction on the device).
 
 All compute runs in libfmlb.so (hand-written CUDA for sm_100a) through its C
 ABI; torch is used for device buffers and streams only. There is no CPU
@@ -36,6 +38,7 @@ from .kernels import (fget_alpha_arad, fget_atomic_distance_arad, fget_atomic_ke
                       get_atomic_kernels_arad, get_atomic_kernels_gaussian,
                       get_atomic_kernels_laplacian, get_atomic_symmetric_kernels_arad,
                       get_prediction, get_prediction_from_distance, laplacian_kernel)
+from .krr import KRRPipeline, krr_fit_predict
 from .molecule import Molecule
 from .xyz import read_xyz_batch, read_xyz_molecules
 
@@ -50,5 +53,6 @@ __all__ = [
     "CholeskyWarning",
     "generate_coulomb_matrices", "generate_unsorted_coulomb_matrices",
     "generate_local_coulomb_matrices", "generate_arad_descriptors",
-    "read_xyz_batch", "read_xyz_molecules", "NUCLEAR_CHARGE", "PTP",
+    "read_xyz_batch", "read_xyz_molecules", "KRRPipeline", "krr_fit_predict", "NUCLEAR_CHARGE",
+    "PTP",
 ]

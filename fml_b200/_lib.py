@@ -57,6 +57,14 @@ SIGNATURES = {
     "fmlb_potri_f64": (_i, [_vp, _ll, _i, _vp, _vp, _ll, _vp, _vp]),
     "fmlb_potrs_f64": (_i, [_vp, _ll, _i, _vp, _vp, _vp]),
     "fmlb_syrk_lower_f64": (_i, [_vp, _ll, _i, _vp, _ll, _i, _i, _vp, _vp]),
+    "fmlb_potrf_ozaki_workspace_bytes": (_sz, [_i, _i]),
+    "fmlb_potrf_ozaki_f64": (_i, [_vp, _ll, _i, _i, _vp, _sz, _vp, _vp]),
+    "fmlb_syrk_ozaki_workspace_bytes": (_sz, [_i, _i, _i]),
+    "fmlb_syrk_lower_ozaki": (_i, [_vp, _ll, _i, _vp, _ll, _i, _i, _i, _vp, _sz, _vp, _vp]),
+    "fmlb_tc_test_hooks": (_i, [_ll, _i]),
+    "fmlb_get_diagonal_f64": (_i, [_vp, _ll, _i, _vp, _vp]),
+    "fmlb_krr_refine_dd_scratch_doubles": (_sz, [_i]),
+    "fmlb_krr_refine_dd": (_i, [_vp, _ll, _i, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp]),
     "fmlb_krr_refine_scratch_doubles": (_sz, [_i]),
     "fmlb_symmetrize_lower_f64": (_i, [_vp, _ll, _i, _vp]),
     "fmlb_krr_refine_f64": (_i, [_vp, _ll, _i, _d, _vp, _ll, _vp, _vp, _vp, _i, _vp, _vp, _vp]),
@@ -112,7 +120,7 @@ def load(require_cuda=True):
 
 
 # host-only entry points (no device work): callable without a GPU
-HOST_ONLY = frozenset(["fmlb_xyz_scan", "fmlb_xyz_parse"])
+HOST_ONLY = frozenset(["fmlb_xyz_scan", "fmlb_xyz_parse", "fmlb_tc_test_hooks"])
 
 
 def call(name, *args):

@@ -45,12 +45,26 @@ def _upper_as_rowmajor_lower(A):
     return t, True
 
 
-def potrf(Ad, n):
-    """In-place FP64 factorisation of a device (n, n) tensor; returns (work, info)."""
-    work = workspace(_lib.load().fmlb_potrf_workspace_bytes(n))
+def potrf(Ad, n, factor="fp64", slices=7):
+    """In-place factorisation of a device (n, n) tensor; returns (work, info).
+
+    factor="fp64": FP64 tensor-core trailing updates (DMMA);
+    factor="ozaki": trailing updates on the int8 tensor cores with ``slices``
+    7-bit digit planes per entry (the Ozaki scheme), to be followed by
+    iterative refinement.
+    """
+    lib = _lib.load()
     info = torch.zeros(1, dtype=torch.int32, device=Ad.device)
-    _lib.call("fmlb_potrf_f64", _lib.ptr(Ad), Ad.stride(0), n, _lib.ptr(work), _lib.ptr(info),
-              _lib.stream_handle())
+    if factor == "fp64":
+        work = workspace(lib.fmlb_potrf_workspace_bytes(n))
+        _lib.call("fmlb_potrf_f64", _lib.ptr(Ad), Ad.stride(0), n, _lib.ptr(work),
+                  _lib.ptr(info), _lib.stream_handle())
+    elif factor == "ozaki":
+        work = workspace(lib.fmlb_potrf_ozaki_workspace_bytes(n, slices))
+        _lib.call("fmlb_potrf_ozaki_f64", _lib.ptr(Ad), Ad.stride(0), n, int(slices),
+                  _lib.ptr(work), work.numel(), _lib.ptr(info), _lib.stream_handle())
+    else:
+        raise ValueError("factor must be 'fp64' or 'ozaki'")
     return work, info
 
 
@@ -59,49 +73,87 @@ def potrs(Ad, n, work, x):
               _lib.stream_handle())
 
 
-def cho_solve(A, y, strict=False, refine=0, return_residuals=False):
+def _check_info(info, strict):
+    code = int(info.item())
+    if code == _lib.FMLB_ETIMEDOUT:
+        raise _lib.FmlbError(code, "cho_solve: a device-side wait of the factorisation gave up")
+    if code > 0:
+        msg = "WARNING: Cholesky decomposition DPOTRF() exited with error code: %d" % code
+        if strict:
+            raise np.linalg.LinAlgError(msg)
+        warnings.warn(msg, CholeskyWarning, stacklevel=3)
+
+
+def cho_solve(A, y, strict=False, refine=None, return_residuals=False, factor="fp64",
+              slices=7, residual=None):
     """Solve A x = y for symmetric positive-definite A.
 
-    ``refine`` > 0 adds that many FP64 iterative-refinement steps on the
-    device (r = y - A x with A kept unfactored, x += solve(r));
-    ``return_residuals`` also returns ||y - A x||_2 before each step and
-    after the last (``refine`` + 1 values; the plain solve's residual for
-    ``refine=0``). Both are extensions: the reference solves once.
+    Extensions (the reference solves once with LAPACK):
+
+    * ``factor="ozaki"`` factors on the int8 tensor cores (``slices`` digit
+      planes, 1..8) and refines; ``refine`` then defaults to 3 steps and the
+      residual to double-double.
+    * ``refine`` > 0 adds that many iterative-refinement steps on the device
+      (r = y - A x, x += solve(r)); ``residual="fp64"`` (the default for the
+      FP64 factor) forms r in FP64, ``residual="dd"`` in double-double with x
+      kept as a double-double pair (past the FP64 residual floor).
+    * ``return_residuals`` also returns ||y - A x||_2 before each step and
+      after the last (``refine`` + 1 values).
     """
     if len(A.shape) != 2 or A.shape[0] != A.shape[1]:
         raise ValueError('expected square matrix')
     if len(y.shape) != 1 or y.shape[0] != A.shape[1]:
         raise ValueError('expected matrix and vector of same stride size')
     n = A.shape[0]
+    if factor not in ("fp64", "ozaki"):
+        raise ValueError("factor must be 'fp64' or 'ozaki'")
+    if refine is None:
+        refine = 3 if factor == "ozaki" else 0
+    if residual is None:
+        residual = "dd" if factor == "ozaki" else "fp64"
     if refine < 0:
         raise ValueError("refine must be >= 0")
+    if residual not in ("fp64", "dd"):
+        raise ValueError("residual must be 'fp64' or 'dd'")
     Ad, as_np = _upper_as_rowmajor_lower(A)
     x, _ = to_device(y, torch.float64)
     x = x.clone()
     keep = refine > 0 or return_residuals
-    if keep:  # the unfactored matrix, both triangles, for the FP64 residual
+    out_np = as_np or not is_torch(y)
+    if n == 0:
+        return (to_output(x, out_np), np.zeros(refine + 1)) if return_residuals else \
+            to_output(x, out_np)
+    lib = _lib.load()
+    st = _lib.stream_handle()
+    if keep and residual == "fp64":  # the unfactored matrix, both triangles
         yd = x.clone()
         Kf = Ad.clone()
-        _lib.call("fmlb_symmetrize_lower_f64", _lib.ptr(Kf), Kf.stride(0), n,
-                  _lib.stream_handle())
-    work, info = potrf(Ad, n)
-    code = int(info.item())
-    if code > 0:
-        msg = "WARNING: Cholesky decomposition DPOTRF() exited with error code: %d" % code
-        if strict:
-            raise np.linalg.LinAlgError(msg)
-        warnings.warn(msg, CholeskyWarning, stacklevel=2)
+        _lib.call("fmlb_symmetrize_lower_f64", _lib.ptr(Kf), Kf.stride(0), n, st)
+    elif keep:  # K stays in the strict upper triangle the factorisation leaves alone
+        yd = x.clone()
+        _lib.call("fmlb_symmetrize_lower_f64", _lib.ptr(Ad), Ad.stride(0), n, st)
+        diag = torch.empty(n, dtype=torch.float64, device=Ad.device)
+        _lib.call("fmlb_get_diagonal_f64", _lib.ptr(Ad), Ad.stride(0), n, _lib.ptr(diag), st)
+    work, info = potrf(Ad, n, factor, slices)
+    _check_info(info, strict)
     potrs(Ad, n, work, x)
     if not keep:
-        return to_output(x, as_np or not is_torch(y))
-    lib = _lib.load()
-    scratch = torch.empty(lib.fmlb_krr_refine_scratch_doubles(n), dtype=torch.float64,
-                          device=Ad.device)
+        return to_output(x, out_np)
     resid = torch.empty(refine + 1, dtype=torch.float64, device=Ad.device)
-    _lib.call("fmlb_krr_refine_f64", _lib.ptr(Kf), Kf.stride(0), n, 0.0, _lib.ptr(Ad),
-              Ad.stride(0), _lib.ptr(work), _lib.ptr(yd), _lib.ptr(x), int(refine),
-              _lib.ptr(resid), _lib.ptr(scratch), _lib.stream_handle())
-    out = to_output(x, as_np or not is_torch(y))
+    if residual == "fp64":
+        scratch = torch.empty(lib.fmlb_krr_refine_scratch_doubles(n), dtype=torch.float64,
+                              device=Ad.device)
+        _lib.call("fmlb_krr_refine_f64", _lib.ptr(Kf), Kf.stride(0), n, 0.0, _lib.ptr(Ad),
+                  Ad.stride(0), _lib.ptr(work), _lib.ptr(yd), _lib.ptr(x), int(refine),
+                  _lib.ptr(resid), _lib.ptr(scratch), st)
+    else:
+        scratch = torch.empty(lib.fmlb_krr_refine_dd_scratch_doubles(n), dtype=torch.float64,
+                              device=Ad.device)
+        x_lo = torch.zeros_like(x)
+        _lib.call("fmlb_krr_refine_dd", _lib.ptr(Ad), Ad.stride(0), n, _lib.ptr(diag),
+                  _lib.ptr(work), _lib.ptr(yd), _lib.ptr(x), _lib.ptr(x_lo), int(refine),
+                  _lib.ptr(resid), _lib.ptr(scratch), st)
+    out = to_output(x, out_np)
     if return_residuals:
         return out, resid.cpu().numpy()
     return out

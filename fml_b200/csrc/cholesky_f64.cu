@@ -23,6 +23,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "ozaki.cuh"
 
 namespace fmlb {
 namespace {
@@ -900,15 +901,13 @@ static int outer_width(int n) {
 //                  then the factorisation of outer panel K+1;
 //   caller stream: update of the trailing matrix past block K+1 by panel K.
 // The two regions are disjoint, so the panel chain runs under the bulk update.
-extern "C" int fmlb_potrf_f64(double *A, long long lda, int n, void *work, int *info,
-                              void *stream) {
+// With `oz` set, the strip and bulk updates run on the int8 tensor cores
+// (ozaki_f64.cu): panel K's rows below it are split into digit planes once,
+// on the caller stream, before either update reads them; the next split waits
+// for the panel stream, so the planes are never overwritten while read.
+static int potrf_blocked(double *A, long long lda, int n, void *work, int *info,
+                         cudaStream_t st, const fmlb::OzakiSlices *oz) {
     using namespace fmlb;
-    cudaStream_t st = FMLB_STREAM(stream);
-    FMLB_REQUIRE(n >= 0 && lda >= n, "fmlb_potrf_f64: bad n=%d / lda=%lld", n, lda);
-    FMLB_REQUIRE(info, "fmlb_potrf_f64: info pointer is null");
-    FMLB_TRY(cuda_status(cudaMemsetAsync(info, 0, sizeof(int), st), "fmlb_potrf_f64: clear info"));
-    if (n == 0) return FMLB_OK;
-    FMLB_REQUIRE(A && work, "fmlb_potrf_f64: null pointer");
     FMLB_TRY(set_smem_attrs());
     Lookahead *la = nullptr;
     FMLB_TRY(lookahead_for(st, &la));
@@ -923,23 +922,73 @@ extern "C" int fmlb_potrf_f64(double *A, long long lda, int n, void *work, int *
         const int rest = n - (int)base;
         if (panel_used)  // outer panel K was factored on the panel stream
             FMLB_TRY(cuda_status(cudaStreamWaitEvent(st, la->panel_done, 0), "wait panel"));
+        if (oz)  // digit planes of panel K, rows [base, n)
+            FMLB_TRY(ozaki_split(A + base * lda + K0, lda, rest, W, *oz, info, st));
         FMLB_TRY(cuda_status(cudaEventRecord(la->main_done, st), "record main"));
         FMLB_TRY(cuda_status(cudaStreamWaitEvent(la->panel, la->main_done, 0), "wait main"));
-        FMLB_TRY(launch_syrk(A + base * lda + base, lda, rest, A + base * lda + K0, lda, W, info,
-                             la->panel, W));
+        if (oz)
+            FMLB_TRY(ozaki_syrk(A + base * lda + base, lda, rest, *oz, 0, W, info, la->panel));
+        else
+            FMLB_TRY(launch_syrk(A + base * lda + base, lda, rest, A + base * lda + K0, lda, W,
+                                 info, la->panel, W));
         FMLB_TRY(factor_outer_panel(A, lda, n, (int)base, W, Linv, info, la->panel));
         FMLB_TRY(cuda_status(cudaEventRecord(la->panel_done, la->panel), "record panel"));
         panel_used = true;
         const int rest2 = rest - W;
         if (rest2 > 0) {
             const size_t b2 = base + W;
-            FMLB_TRY(launch_syrk(A + b2 * lda + b2, lda, rest2, A + b2 * lda + K0, lda, W, info,
-                                 st));
+            if (oz)
+                FMLB_TRY(ozaki_syrk(A + b2 * lda + b2, lda, rest2, *oz, W, 0, info, st));
+            else
+                FMLB_TRY(launch_syrk(A + b2 * lda + b2, lda, rest2, A + b2 * lda + K0, lda, W,
+                                     info, st));
         }
     }
     if (panel_used)
         FMLB_TRY(cuda_status(cudaStreamWaitEvent(st, la->panel_done, 0), "join panel stream"));
     return FMLB_OK;
+}
+
+extern "C" int fmlb_potrf_f64(double *A, long long lda, int n, void *work, int *info,
+                              void *stream) {
+    using namespace fmlb;
+    cudaStream_t st = FMLB_STREAM(stream);
+    FMLB_REQUIRE(n >= 0 && lda >= n, "fmlb_potrf_f64: bad n=%d / lda=%lld", n, lda);
+    FMLB_REQUIRE(info, "fmlb_potrf_f64: info pointer is null");
+    FMLB_TRY(cuda_status(cudaMemsetAsync(info, 0, sizeof(int), st), "fmlb_potrf_f64: clear info"));
+    if (n == 0) return FMLB_OK;
+    FMLB_REQUIRE(A && work, "fmlb_potrf_f64: null pointer");
+    return potrf_blocked(A, lda, n, work, info, st, nullptr);
+}
+
+extern "C" size_t fmlb_potrf_ozaki_workspace_bytes(int n, int nslices) {
+    if (n <= 0 || nslices <= 0) return 256;
+    const int W = outer_width(n);
+    return (fmlb_potrf_workspace_bytes(n) + 255) / 256 * 256 +
+           fmlb::ozaki_slice_bytes(n, W, nslices);
+}
+
+extern "C" int fmlb_potrf_ozaki_f64(double *A, long long lda, int n, int nslices, void *work,
+                                    size_t ws_bytes, int *info, void *stream) {
+    using namespace fmlb;
+    cudaStream_t st = FMLB_STREAM(stream);
+    FMLB_REQUIRE(n >= 0 && lda >= n, "fmlb_potrf_ozaki_f64: bad n=%d / lda=%lld", n, lda);
+    FMLB_REQUIRE(nslices >= 1 && nslices <= OZAKI_MAX_SLICES,
+                 "fmlb_potrf_ozaki_f64: nslices must be 1..%d", OZAKI_MAX_SLICES);
+    FMLB_REQUIRE(info, "fmlb_potrf_ozaki_f64: info pointer is null");
+    FMLB_TRY(cuda_status(cudaMemsetAsync(info, 0, sizeof(int), st),
+                         "fmlb_potrf_ozaki_f64: clear info"));
+    if (n == 0) return FMLB_OK;
+    FMLB_REQUIRE(A && work, "fmlb_potrf_ozaki_f64: null pointer");
+    const size_t need = fmlb_potrf_ozaki_workspace_bytes(n, nslices);
+    if (ws_bytes < need) {
+        set_error("fmlb_potrf_ozaki_f64: workspace %zu < %zu bytes", ws_bytes, need);
+        return FMLB_ENOMEM;
+    }
+    OzakiSlices oz;
+    const size_t off = (fmlb_potrf_workspace_bytes(n) + 255) / 256 * 256;
+    FMLB_TRY(ozaki_bind(static_cast<char *>(work) + off, n, outer_width(n), nslices, oz));
+    return potrf_blocked(A, lda, n, work, info, st, &oz);
 }
 
 extern "C" int fmlb_potrs_f64(const double *L, long long lda, int n, const void *work, double *x,

@@ -7,16 +7,20 @@
 // (x = hi + lo): x.y ~ hi.hi + hi.lo + lo.hi, three BF16 MMAs accumulated in
 // FP32 in tensor memory, and every sigma emitted by the epilogue.
 //
-// Structure (one persistent CTA per SM, 192 threads):
+// Structure (one persistent CTA per SM, 320 threads):
 //   warp 0      TMA producer: per k-chunk of 64, four 128 x 64 BF16 tiles
 //               (A hi, A lo, B hi, B lo), 128B-swizzled, into a 3-stage ring;
 //   warp 1      allocates 256 TMEM columns (two 128 x 128 FP32 accumulators)
 //               and one thread issues tcgen05.mma (M=128, N=128, K=16);
-//   warps 2..5  epilogue: tcgen05.ld of their 32-lane quarter, d^2, exp for
-//               every sigma, FP32 stores (and the mirrored tile for
-//               symmetric builds), overlapping the next tile's MMAs.
+//   warps 2..9  epilogue, two warps per 32-lane TMEM quarter (64 columns
+//               each): tcgen05.ld, d^2, release of the accumulator, then exp
+//               for every sigma and streaming FP32 stores: the mirrored tile
+//               (symmetric builds) from registers, the direct tile through a
+//               shared-memory transpose so every store is one coalesced row;
+//               the next tile's MMAs run meanwhile in the other accumulator.
 // Every mbarrier wait is bounded; a wait that runs out records an error code
-// in *status and the CTA winds down instead of hanging.
+// in *status and the CTA winds down instead of hanging, after its own copies
+// and MMAs in flight have finished.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <math.h>
@@ -26,19 +30,26 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "tc_common.cuh"
 
 namespace fmlb {
 namespace {
 
-constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 64, TC_STAGES = 3, TC_THREADS = 192;
+using namespace tc;
+
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 64, TC_STAGES = 3, TC_THREADS = 320;
+constexpr int TC_EPI_WARPS = 8;
 constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 2;          // 16 KB per operand tile
 constexpr int TC_STAGE_BYTES = 4 * TC_TILE_BYTES;          // A hi, A lo, B hi, B lo
 constexpr int TC_TMEM_COLS = 2 * TC_BN;
 constexpr int TC_MAXSIG = 8;
-constexpr size_t kTcSmem = (size_t)TC_STAGES * TC_STAGE_BYTES + 1024 /* align */ + 256;
-constexpr long long kWaitBudget = 4000000000LL;            // clock cycles (~2 s)
+constexpr int TC_PITCH = 33;                               // floats per transposed row
+constexpr int TC_STG_BYTES = TC_EPI_WARPS * 32 * TC_PITCH * 4;
+constexpr size_t kTcSmem =
+    (size_t)TC_STAGES * TC_STAGE_BYTES + TC_STG_BYTES + 1024 /* align */ + 256;
 
-enum TcStatus { TC_OK = 0, TC_TIMEOUT_FULL = 1, TC_TIMEOUT_EMPTY = 2, TC_TIMEOUT_TMEM = 3 };
+enum TcStatus { TC_OK = 0, TC_TIMEOUT_FULL = 1, TC_TIMEOUT_EMPTY = 2, TC_TIMEOUT_TMEM = 3,
+                TC_TIMEOUT_DRAIN = 4 };
 
 struct TcParams {
     float scale[TC_MAXSIG];  // -log2(e) / (2 sigma^2)
@@ -48,45 +59,9 @@ struct TcParams {
     int nk;                  // k-chunks of 64
     int symmetric;
     long long ldk, sstride;  // output row stride and sigma stride (elements)
+    long long budget;        // clock cycles of every mbarrier wait
+    int skip_loads;          // test hook: the producer issues no copies
 };
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Waits for the phase of `bar` with the given parity; false after the budget.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-    if (mbar_try_wait(bar, parity)) return true;
-    const long long t0 = clock64();
-    while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > kWaitBudget) return false;
-    return true;
-}
 
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar,
                                             int x, int y) {
@@ -95,19 +70,6 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, u
         " [%0], [%1, {%3, %4}], [%2];\n" ::"r"(smem_u32(dst)),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
         : "memory");
-}
-
-// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
-// 1024 bytes apart, descriptor version 1 (sm_100).
-__device__ __forceinline__ uint64_t smem_desc_sw128(const void *p) {
-    const uint64_t addr = smem_u32(p);
-    uint64_t d = 0;
-    d |= (addr >> 4) & 0x3FFFull;        // start address
-    d |= (uint64_t)1 << 16;              // leading byte offset (unused for swizzled K-major)
-    d |= (uint64_t)(1024 >> 4) << 32;    // stride byte offset
-    d |= (uint64_t)1 << 46;              // version
-    d |= (uint64_t)2 << 61;              // 128-byte swizzle
-    return d;
 }
 
 // Instruction descriptor, kind::f16: BF16 A and B, FP32 accumulator, both
@@ -121,28 +83,6 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
         " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
         "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t *bar) {
-    asm volatile(
-        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-            smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-        "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
-        "%28, %29, %30, %31}, [%32];\n"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-          "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
-          "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
-          "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
-          "=r"(v[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
 __device__ __forceinline__ void tile_coords(int t, const TcParams &p, int &ta, int &tb) {
@@ -172,13 +112,17 @@ gauss_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constan
     extern __shared__ uint8_t tc_smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~(uintptr_t)1023);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TC_STAGES * TC_STAGE_BYTES);
+    float *stg_all = reinterpret_cast<float *>(smem + TC_STAGES * TC_STAGE_BYTES);
+    uint64_t *bars =
+        reinterpret_cast<uint64_t *>(smem + TC_STAGES * TC_STAGE_BYTES + TC_STG_BYTES);
     uint64_t *full = bars, *empty = bars + TC_STAGES;
     uint64_t *tmem_full = bars + 2 * TC_STAGES, *tmem_empty = tmem_full + 2;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tmem_empty + 2);
+    uint64_t *mma_done = tmem_empty + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mma_done + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ntiles = p.symmetric ? p.ntile_a * (p.ntile_a + 1) / 2 : p.ntile_a * p.ntile_b;
+    const long long budget = p.budget;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_STAGES; ++s) {
@@ -187,32 +131,29 @@ gauss_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constan
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(&tmem_full[a], 1);
-            mbar_init(&tmem_empty[a], 4);
+            mbar_init(&tmem_empty[a], TC_EPI_WARPS);
         }
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        mbar_init(mma_done, 1);
+        mbar_fence_init();
     }
-    if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
-                         smem_u32(tmem_slot)),
-                     "r"(TC_TMEM_COLS));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    if (warp == 1) tmem_alloc(tmem_slot, TC_TMEM_COLS);
+    fence_before_sync();
     __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    fence_after_sync();
     const uint32_t tmem_base = *tmem_slot;
 
     if (warp == 0) {
         // ------------------------------------------------------------ producer
         if (lane == 0) {
-            int stage = 0;
-            uint32_t phase = 0;
+            long long issued = 0;
             bool ok = true;
-            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+            for (int t = blockIdx.x; t < ntiles && ok && !p.skip_loads; t += gridDim.x) {
                 int ta, tb;
                 tile_coords(t, p, ta, tb);
-                for (int kc = 0; kc < p.nk; ++kc) {
-                    if (!mbar_wait(&empty[stage], phase ^ 1)) {
+                for (int kc = 0; kc < p.nk; ++kc, ++issued) {
+                    const int stage = (int)(issued % TC_STAGES);
+                    const uint32_t phase = (uint32_t)((issued / TC_STAGES) & 1);
+                    if (!mbar_wait(&empty[stage], phase ^ 1, budget)) {
                         atomicCAS(status, 0, TC_TIMEOUT_EMPTY);
                         ok = false;
                         break;
@@ -225,41 +166,42 @@ gauss_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constan
                                 tb * TC_BN);
                     tma_load_2d(st + 3 * TC_TILE_BYTES, &mapBlo, &full[stage], kc * TC_BK,
                                 tb * TC_BN);
-                    if (++stage == TC_STAGES) {
-                        stage = 0;
-                        phase ^= 1;
-                    }
                 }
             }
+            // every copy this thread issued has landed before the CTA winds down
+            for (long long l = issued > TC_STAGES ? issued - TC_STAGES : 0; l < issued; ++l)
+                if (!mbar_wait(&full[l % TC_STAGES], (uint32_t)((l / TC_STAGES) & 1), budget))
+                    atomicCAS(status, 0, TC_TIMEOUT_DRAIN);
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------- MMA issuer
         if (lane == 0) {
-            int stage = 0;
-            uint32_t phase = 0;
+            long long consumed = 0;
             int lt = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++lt) {
                 const int acc = lt & 1;
                 const uint32_t acc_phase = (lt >> 1) & 1;
-                if (!mbar_wait(&tmem_empty[acc], acc_phase ^ 1)) {
+                if (!mbar_wait(&tmem_empty[acc], acc_phase ^ 1, budget)) {
                     atomicCAS(status, 0, TC_TIMEOUT_TMEM);
                     break;
                 }
-                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                fence_after_sync();
                 const uint32_t dacc = tmem_base + (uint32_t)(acc * TC_BN);
-                for (int kc = 0; kc < p.nk; ++kc) {
-                    if (!mbar_wait(&full[stage], phase)) {
+                for (int kc = 0; kc < p.nk; ++kc, ++consumed) {
+                    const int stage = (int)(consumed % TC_STAGES);
+                    const uint32_t phase = (uint32_t)((consumed / TC_STAGES) & 1);
+                    if (!mbar_wait(&full[stage], phase, budget)) {
                         atomicCAS(status, 0, TC_TIMEOUT_FULL);
                         ok = false;
                         break;
                     }
-                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                    fence_after_sync();
                     uint8_t *st = smem + stage * TC_STAGE_BYTES;
-                    const uint64_t ahi = smem_desc_sw128(st);
-                    const uint64_t alo = smem_desc_sw128(st + TC_TILE_BYTES);
-                    const uint64_t bhi = smem_desc_sw128(st + 2 * TC_TILE_BYTES);
-                    const uint64_t blo = smem_desc_sw128(st + 3 * TC_TILE_BYTES);
+                    const uint64_t ahi = smem_desc_kmajor(st, 128);
+                    const uint64_t alo = smem_desc_kmajor(st + TC_TILE_BYTES, 128);
+                    const uint64_t bhi = smem_desc_kmajor(st + 2 * TC_TILE_BYTES, 128);
+                    const uint64_t blo = smem_desc_kmajor(st + 3 * TC_TILE_BYTES, 128);
 #pragma unroll
                     for (int k = 0; k < TC_BK / 16; ++k) {
                         // advance 16 BF16 = 32 bytes inside the 128-byte swizzle row
@@ -270,93 +212,96 @@ gauss_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constan
                         mma_bf16(dacc, alo + off, bhi + off, 1u);
                     }
                     mma_commit(&empty[stage]);  // frees the stage once these MMAs finish
-                    if (++stage == TC_STAGES) {
-                        stage = 0;
-                        phase ^= 1;
-                    }
                 }
                 if (!ok) break;
                 mma_commit(&tmem_full[acc]);
             }
+            // every MMA issued has finished before TMEM is released
+            mma_commit(mma_done);
+            if (!mbar_wait(mma_done, 0, budget)) atomicCAS(status, 0, TC_TIMEOUT_DRAIN);
         }
     } else {
         // --------------------------------------------------------------- epilogue
-        const int q = warp & 3;  // TMEM lane quarter this warp may access
-        const int row_local = q * 32 + lane;
-        const bool vec_ok = ((p.ldk & 3) == 0) && ((p.sstride & 3) == 0) &&
-                            ((reinterpret_cast<uintptr_t>(K) & 15) == 0);
+        // Two warps per TMEM lane quarter, 64 columns each. Both 32-column
+        // chunks are drained into registers first and TMEM is released, then
+        // every sigma is written: the mirrored tile straight from registers
+        // (lanes hold consecutive rows: coalesced), the direct tile through a
+        // shared-memory transpose (one coalesced row of 32 floats per store).
+        const int q = warp & 3;
+        const int half = (warp - 2) >> 2;
+        float *stg = stg_all + (warp - 2) * 32 * TC_PITCH;
         int lt = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++lt) {
             int ta, tb;
             tile_coords(t, p, ta, tb);
             const int acc = lt & 1;
             const uint32_t acc_phase = (lt >> 1) & 1;
-            if (!mbar_wait(&tmem_full[acc], acc_phase)) {
+            if (!mbar_wait(&tmem_full[acc], acc_phase, budget)) {
                 atomicCAS(status, 0, TC_TIMEOUT_TMEM);
                 break;
             }
-            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            const int grow = ta * TC_BM + row_local;
+            fence_after_sync();
+            const int row0 = ta * TC_BM + q * 32;           // this warp's first row
+            const int grow = row0 + lane;
+            const int gcol0 = tb * TC_BN + half * 64;       // this warp's first column
             const bool row_ok = grow < p.na;
             const float nr = row_ok ? normA[grow] : 0.0f;
             const bool diag_tile = p.symmetric && ta == tb;
-            for (int c0 = 0; c0 < TC_BN; c0 += 32) {
+            float d2[64];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
                 uint32_t v[32];
-                tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * TC_BN + c0), v);
-                const int gcol0 = tb * TC_BN + c0;
-                float d2[32];
+                tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) +
+                              (uint32_t)(acc * TC_BN + half * 64 + c * 32), v);
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
-                    const int gcol = gcol0 + j;
-                    const float nc = gcol < p.nb ? normB[gcol] : 0.0f;
+                    const int gcol = gcol0 + c * 32 + j;
+                    const float nc = gcol < p.nb ? __ldg(normB + gcol) : 0.0f;
                     float x = fmaxf(nr + nc - 2.0f * __uint_as_float(v[j]), 0.0f);
                     if (diag_tile && gcol == grow) x = 0.0f;  // exact zero distance
-                    d2[j] = x;
-                }
-                if (!row_ok) continue;
-                for (int s = 0; s < p.nsig; ++s) {
-                    const float sc = p.scale[s];
-                    float *Ks = K + s * p.sstride;
-#pragma unroll
-                    for (int j4 = 0; j4 < 32; j4 += 4) {
-                        float kv[4];
-#pragma unroll
-                        for (int i = 0; i < 4; ++i) kv[i] = fast_exp2(d2[j4 + i] * sc);
-                        const int gcol = gcol0 + j4;
-                        // direct tile: on diagonal tiles only the lower triangle (c <= r)
-                        const bool full4 = gcol + 3 < p.nb && (!diag_tile || gcol + 3 <= grow);
-                        if (full4 && vec_ok) {
-                            *reinterpret_cast<float4 *>(Ks + (size_t)grow * p.ldk + gcol) =
-                                make_float4(kv[0], kv[1], kv[2], kv[3]);
-                        } else {
-#pragma unroll
-                            for (int i = 0; i < 4; ++i)
-                                if (gcol + i < p.nb && (!diag_tile || gcol + i <= grow))
-                                    Ks[(size_t)grow * p.ldk + gcol + i] = kv[i];
-                        }
-                        // mirrored tile: lanes hold consecutive rows -> coalesced stores
-                        if (p.symmetric) {
-#pragma unroll
-                            for (int i = 0; i < 4; ++i) {
-                                const int c = gcol + i;
-                                if (c < p.nb && (!diag_tile || c < grow))
-                                    Ks[(size_t)c * p.ldk + grow] = kv[i];
-                            }
-                        }
-                    }
+                    d2[c * 32 + j] = x;
                 }
             }
-            asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+            fence_before_sync();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&tmem_empty[acc]);
+            if (lane == 0) mbar_arrive(&tmem_empty[acc]);  // the next-but-one tile may start
+            for (int s = 0; s < p.nsig; ++s) {
+                const float sc = p.scale[s];
+                float *Ks = K + s * p.sstride;
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const int cb = gcol0 + c * 32;
+                    float kv[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) kv[j] = fast_exp2(d2[c * 32 + j] * sc);
+                    // mirrored tile K[col][row]: lanes write 32 consecutive rows
+                    if (p.symmetric && row_ok) {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const int col = cb + j;
+                            if (col < p.nb && (!diag_tile || col < grow))
+                                __stcs(Ks + (size_t)col * p.ldk + grow, kv[j]);
+                        }
+                    }
+                    // direct tile K[row][col] through the transpose
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) stg[lane * TC_PITCH + j] = kv[j];
+                    __syncwarp();
+                    const int col = cb + lane;
+                    for (int rr = 0; rr < 32; ++rr) {
+                        const int r = row0 + rr;
+                        if (r < p.na && col < p.nb && (!diag_tile || col <= r))
+                            __stcs(Ks + (size_t)r * p.ldk + col, stg[rr * TC_PITCH + lane]);
+                    }
+                    __syncwarp();
+                }
+            }
         }
     }
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    fence_before_sync();
     __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    if (warp == 1)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_base),
-                     "r"(TC_TMEM_COLS));
+    fence_after_sync();
+    if (warp == 1) tmem_dealloc(tmem_base, TC_TMEM_COLS);
 }
 
 // ---- operand preparation ----------------------------------------------------
@@ -400,27 +345,8 @@ __global__ void column_mean_kernel(const double *__restrict__ X, int n, int ldx,
 }
 
 // ---- host: tensor maps --------------------------------------------------------
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
-                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
-                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-    static EncodeTiledFn fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-                cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-    });
-    return fn;
-}
-
 int make_map(CUtensorMap *m, const void *base, int rows, int cols) {
-    EncodeTiledFn fn = encode_fn();
+    EncodeTiledFn fn = encode_tiled_fn();
     if (!fn) {
         set_error("cuTensorMapEncodeTiled is unavailable");
         return FMLB_ECUDA;
@@ -531,6 +457,9 @@ extern "C" int fmlb_gaussian_kernel_tc(const double *A, int na, int lda, const d
     p.symmetric = symmetric ? 1 : 0;
     p.ldk = ldk;
     p.sstride = sigma_stride;
+    const TestHooks hooks = test_hooks();
+    p.budget = hooks.wait_budget;
+    p.skip_loads = hooks.skip_loads;
     static int attr_dev = -1;
     int dev = 0;
     FMLB_TRY(cuda_status(cudaGetDevice(&dev), "fmlb_gaussian_kernel_tc: cudaGetDevice"));

@@ -1,0 +1,483 @@
+// FP64 trailing update C -= P P^T of the Cholesky factorisation on the int8
+// tensor cores: the Ozaki splitting scheme (K. Ozaki, T. Ogita, S. Oishi,
+// S. M. Rump, "Error-free transformations of matrix multiplication by using
+// fast routines of matrix multiplication and its applications", Numer.
+// Algorithms 59, 2012; int8 form: H. Ootomo, K. Ozaki, R. Yokota, "DGEMM on
+// integer matrix multiplication unit", IJHPCA 2024), written for tcgen05.
+//
+// Splitting. Each row r of P (k columns) gets the exponent e_r with
+// max_c |P[r, c]| < 2^e_r and s signed 7-bit digits per entry:
+//     P[r, c] = 2^e_r * sum_{t=1..s} d_t[r, c] 2^(-7 t) + O(2^(e_r - 7 s)),
+//     d_t = trunc(128 * remainder) in [-127, 127],
+// all exact in FP64. The product of two rows keeps the digit pairs (t, u) with
+// t + u <= s + 1, grouped by diagonal q = t + u - 1:
+//     (P P^T)[r, c] ~ 2^(e_r + e_c - 7 (s + 1)) * sum_{q=1..s} D_q 128^(s - q),
+//     D_q = sum_{t + u = q + 1} d_t[r, :] . d_u[c, :]        (exact in int32)
+// s (s + 1) / 2 int8 products in all, every D_q accumulated exactly in its own
+// TMEM accumulator, and combined once, in FP64, by the epilogue (Horner in
+// 128). |d| <= 127 bounds |D_q| by (q + 1) 127^2 k < 2^31 for k <= 16384.
+// The truncation leaves an error of order k 2^(e_r + e_c - 7 s) per entry: at
+// s = 7 about 16x the FP64 rounding bound, at s = 8 below it.
+//
+// Kernel (persistent, one CTA per SM, 320 threads), output tile 128 x 64:
+//   warp 0      TMA producer: per 32-byte k step, the s digit planes of the
+//               128 A rows and 64 B rows (one 3-D box each, 32-byte swizzle)
+//               into a 4-stage ring;
+//   warp 1      allocates 512 TMEM columns (s <= 8 accumulators of 64 int32
+//               columns) and issues tcgen05.mma kind::i8 (M 128, N 64, K 32);
+//   warps 2..9  epilogue, two warps per TMEM lane quarter (32 columns each):
+//               drain the s accumulators into FP64 (Horner), release TMEM to
+//               the next tile's MMAs, scale by the row and column exponents,
+//               and subtract from C through a shared-memory transpose
+//               (coalesced read-modify-write of the lower triangle).
+// Every mbarrier wait is bounded; a wait that runs out stores FMLB_ETIMEDOUT
+// in *info, and every kernel that reads info returns at once.
+#include <math.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "ozaki.cuh"
+#include "tc_common.cuh"
+
+namespace fmlb {
+namespace {
+
+constexpr int OZ_BM = 128, OZ_BN = 64;
+constexpr int OZ_KB = 32;          // int8 k values (bytes) per stage: one MMA K step
+constexpr int OZ_STAGES = 4;
+constexpr int OZ_THREADS = 320;    // 10 warps
+constexpr int OZ_EPI_WARPS = 8;
+constexpr int OZ_TMEM_COLS = 512;
+constexpr int OZ_PITCH = 33;       // doubles per staged row (conflict-free transpose)
+constexpr int OZ_A_PLANE = OZ_BM * OZ_KB;   // 4096 bytes per A digit plane per stage
+constexpr int OZ_B_PLANE = OZ_BN * OZ_KB;   // 2048
+constexpr int OZ_STAGE_STG = OZ_EPI_WARPS * 16 * OZ_PITCH * (int)sizeof(double);
+constexpr int OZ_NONFINITE = 0x7fffffff;    // exponent marking a row with Inf / NaN
+
+constexpr long long kOzDefaultBudget = 4000000000LL;  // clock cycles (~2 s)
+
+struct OzParams {
+    int m;             // rows (= columns) of C
+    int p_row0;        // slice row of C's row 0 (and column 0)
+    int ns;            // digit planes
+    int nkb;           // 32-byte k steps
+    int strip_cols;    // > 0: only the first strip_cols columns
+    int strip_tiles;   // column tiles per row block in strip mode
+    long long ntiles;
+    long long ldc;
+    int exp_bias;      // -7 (ns + 1)
+    int skip_loads;    // test hook: the producer issues no copies
+};
+
+// Instruction descriptor, kind::i8: signed A and B, int32 accumulator, both
+// K-major, M = 128, N = 64.
+constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) |
+                              ((uint32_t)(OZ_BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(kIdescI8), "r"(accumulate));
+}
+
+// Tile t -> (row0, col0): lower triangle of 128 x 64 tiles (row block `by`
+// holds column tiles 0 .. 2 by + 1), or the first strip_tiles column tiles of
+// every row block. False for tiles outside C.
+__device__ __forceinline__ bool oz_tile(long long t, const OzParams &p, int &row0, int &col0) {
+    int by, bx;
+    if (p.strip_tiles > 0) {
+        by = (int)(t / p.strip_tiles);
+        bx = (int)(t % p.strip_tiles);
+        if (bx > 2 * by + 1) return false;
+    } else {
+        by = (int)((sqrt(4.0 * (double)t + 1.0) - 1.0) * 0.5);
+        while ((long long)by * by + by > t) --by;
+        while ((long long)(by + 1) * (by + 1) + (by + 1) <= t) ++by;
+        bx = (int)(t - (long long)by * by - by);
+    }
+    row0 = by * OZ_BM;
+    col0 = bx * OZ_BN;
+    return row0 < p.m && col0 < p.m;
+}
+
+__device__ __forceinline__ void oz_fail(int *info) { atomicCAS(info, 0, FMLB_ETIMEDOUT); }
+
+__global__ void __launch_bounds__(OZ_THREADS, 1)
+ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                  const int *__restrict__ exps, OzParams p, double *__restrict__ C,
+                  int *__restrict__ info, long long budget) {
+    extern __shared__ uint8_t oz_smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>(
+        (reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~(uintptr_t)1023);
+    const int stage_bytes = p.ns * (OZ_A_PLANE + OZ_B_PLANE);
+    double *stg_all = reinterpret_cast<double *>(smem + OZ_STAGES * stage_bytes);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + OZ_STAGES * stage_bytes + OZ_STAGE_STG);
+    uint64_t *full = bars, *empty = bars + OZ_STAGES;
+    uint64_t *tmem_full = bars + 2 * OZ_STAGES, *tmem_empty = tmem_full + 1,
+             *mma_done = tmem_full + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mma_done + 1);
+    __shared__ int abort_cta;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        abort_cta = *(volatile const int *)info != 0;
+        for (int s = 0; s < OZ_STAGES; ++s) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        tc::mbar_init(tmem_full, 1);
+        tc::mbar_init(tmem_empty, OZ_EPI_WARPS);
+        tc::mbar_init(mma_done, 1);
+        tc::mbar_fence_init();
+    }
+    __syncthreads();
+    if (abort_cta) return;  // a failed factorisation: the whole CTA leaves together
+    if (warp == 1) tc::tmem_alloc(tmem_slot, OZ_TMEM_COLS);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer
+        if (lane == 0) {
+            long long issued = 0;
+            bool ok = true;
+            for (long long t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+                int row0, col0;
+                if (!oz_tile(t, p, row0, col0)) continue;
+                for (int kb = 0; kb < p.nkb && !p.skip_loads; ++kb, ++issued) {
+                    const int st = (int)(issued % OZ_STAGES);
+                    const uint32_t ph = (uint32_t)((issued / OZ_STAGES) & 1);
+                    if (!tc::mbar_wait(&empty[st], ph ^ 1, budget)) {
+                        oz_fail(info);
+                        ok = false;
+                        break;
+                    }
+                    uint8_t *sa = smem + st * stage_bytes;
+                    uint8_t *sb = sa + p.ns * OZ_A_PLANE;
+                    tc::mbar_arrive_expect_tx(&full[st], (uint32_t)stage_bytes);
+                    tc::tma_load_3d(sa, &mapA, &full[st], kb * OZ_KB, p.p_row0 + row0, 0);
+                    tc::tma_load_3d(sb, &mapB, &full[st], kb * OZ_KB, p.p_row0 + col0, 0);
+                }
+            }
+            // every copy this thread issued has landed before the CTA winds down
+            for (long long l = std::max(0LL, issued - OZ_STAGES); l < issued; ++l)
+                if (!tc::mbar_wait(&full[l % OZ_STAGES], (uint32_t)((l / OZ_STAGES) & 1), budget))
+                    oz_fail(info);
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            long long consumed = 0;
+            int lt = 0;
+            bool ok = true;
+            for (long long t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+                int row0, col0;
+                if (!oz_tile(t, p, row0, col0)) continue;
+                if (!tc::mbar_wait(tmem_empty, (uint32_t)((lt & 1) ^ 1), budget)) {
+                    oz_fail(info);
+                    break;
+                }
+                tc::fence_after_sync();
+                for (int kb = 0; kb < p.nkb; ++kb, ++consumed) {
+                    const int st = (int)(consumed % OZ_STAGES);
+                    const uint32_t ph = (uint32_t)((consumed / OZ_STAGES) & 1);
+                    if (!tc::mbar_wait(&full[st], ph, budget)) {
+                        oz_fail(info);
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_after_sync();
+                    const uint8_t *sa = smem + st * stage_bytes;
+                    const uint8_t *sb = sa + p.ns * OZ_A_PLANE;
+                    const uint64_t da = tc::smem_desc_kmajor(sa, OZ_KB);
+                    const uint64_t db = tc::smem_desc_kmajor(sb, OZ_KB);
+                    for (int q = 0; q < p.ns; ++q) {
+                        const uint32_t dacc = tmem_base + (uint32_t)(q * OZ_BN);
+                        for (int a = 0; a <= q; ++a) {
+                            const int b = q - a;
+                            // plane offsets in 16-byte units of the descriptor address
+                            mma_i8(dacc, da + (uint64_t)((a * OZ_A_PLANE) >> 4),
+                                   db + (uint64_t)((b * OZ_B_PLANE) >> 4),
+                                   (kb > 0 || a > 0) ? 1u : 0u);
+                        }
+                    }
+                    tc::mma_commit(&empty[st]);  // frees the stage once these MMAs finish
+                }
+                if (!ok) break;
+                tc::mma_commit(tmem_full);
+                ++lt;
+            }
+            // every MMA issued has finished before TMEM is released
+            tc::mma_commit(mma_done);
+            if (!tc::mbar_wait(mma_done, 0, budget)) oz_fail(info);
+        }
+    } else {
+        // --------------------------------------------------------------- epilogue
+        const int qw = warp & 3;            // TMEM lane quarter this warp may read
+        const int half = (warp - 2) >> 2;   // which 32 of the tile's 64 columns
+        double *stg = stg_all + (warp - 2) * 16 * OZ_PITCH;
+        int lt = 0;
+        for (long long t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
+            int row0, col0;
+            if (!oz_tile(t, p, row0, col0)) continue;
+            if (!tc::mbar_wait(tmem_full, (uint32_t)(lt & 1), budget)) {
+                oz_fail(info);
+                break;
+            }
+            tc::fence_after_sync();
+            double acc[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+            for (int q = 0; q < p.ns; ++q) {
+                uint32_t v[32];
+                tc::tmem_ld32(tmem_base + ((uint32_t)(qw * 32) << 16) +
+                                  (uint32_t)(q * OZ_BN + half * 32), v);
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    acc[j] = fma(acc[j], 128.0, (double)(int)v[j]);
+            }
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(tmem_empty);  // the next tile's MMAs may start
+            ++lt;
+            // scale by 2^(e_r + e_c - 7 (s + 1))
+            const int grow = row0 + qw * 32 + lane;
+            const int er = grow < p.m ? exps[p.p_row0 + grow] : 0;
+            const int gcl = col0 + half * 32 + lane;
+            const int ecl = gcl < p.m ? exps[p.p_row0 + gcl] : 0;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const int ec = __shfl_sync(0xffffffffu, ecl, j);
+                acc[j] = (er == OZ_NONFINITE || ec == OZ_NONFINITE)
+                             ? __longlong_as_double(0x7ff8000000000000LL)
+                             : ldexp(acc[j], er + ec + p.exp_bias);
+            }
+            // transpose through shared memory, 16 rows at a time, then a
+            // coalesced read-modify-write of the rows' lower-triangle part
+#pragma unroll
+            for (int hh = 0; hh < 2; ++hh) {
+                if ((lane >> 4) == hh) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) stg[(lane & 15) * OZ_PITCH + j] = acc[j];
+                }
+                __syncwarp();
+                const int c = col0 + half * 32 + lane;
+                for (int rr = 0; rr < 16; ++rr) {
+                    const int r = row0 + qw * 32 + hh * 16 + rr;
+                    if (r < p.m && c < p.m && c <= r && (p.strip_cols == 0 || c < p.strip_cols))
+                        C[(size_t)r * p.ldc + c] -= stg[rr * OZ_PITCH + lane];
+                }
+                __syncwarp();
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (warp == 1) tc::tmem_dealloc(tmem_base, OZ_TMEM_COLS);
+}
+
+// ---- splitting --------------------------------------------------------------
+// One CTA (128 threads) per row of P (rows [0, m), k columns, stride ldp):
+// exps[r] and ns digit planes (row-major, kp >= k columns zero-padded, plane
+// stride pstride bytes). Each thread owns 8 consecutive columns per sweep.
+constexpr int SL_TPB = 128;
+
+__global__ void __launch_bounds__(SL_TPB)
+ozaki_slice_kernel(const double *__restrict__ P, long long ldp, int m, int k, int kp, int ns,
+                   int8_t *__restrict__ planes, long long pstride, long long ldpl,
+                   int *__restrict__ exps, const int *__restrict__ info) {
+    __shared__ double red[SL_TPB / 32];
+    __shared__ int bad_row, abort_cta;
+    const int r = blockIdx.x, tid = threadIdx.x;
+    if (tid == 0) {
+        abort_cta = info && *(volatile const int *)info != 0;
+        bad_row = 0;
+    }
+    __syncthreads();
+    if (abort_cta || r >= m) return;
+    const double *row = P + (size_t)r * ldp;
+    double mx = 0.0;
+    for (int c = tid; c < k; c += SL_TPB) {
+        const double v = row[c];
+        if (!isfinite(v)) bad_row = 1;
+        mx = fmax(mx, fabs(v));
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((tid & 31) == 0) red[tid >> 5] = mx;
+    __syncthreads();
+    mx = fmax(fmax(red[0], red[1]), fmax(red[2], red[3]));
+    int e = 0;
+    if (mx > 0.0) frexp(mx, &e);  // mx = f 2^e, f in [0.5, 1): |P[r, :]| < 2^e
+    if (tid == 0) exps[r] = bad_row ? OZ_NONFINITE : e;
+    for (int c0 = tid * 8; c0 < kp; c0 += SL_TPB * 8) {
+        double x[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int c = c0 + i;
+            const double v = c < k ? row[c] : 0.0;
+            x[i] = (bad_row || !isfinite(v)) ? 0.0 : ldexp(v, -e);
+        }
+        for (int t = 0; t < ns; ++t) {
+            uint64_t word = 0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                x[i] *= 128.0;
+                const double d = trunc(x[i]);
+                x[i] -= d;
+                word |= (uint64_t)(uint8_t)(int8_t)(int)d << (8 * i);
+            }
+            *reinterpret_cast<uint64_t *>(planes + t * pstride + (size_t)r * ldpl + c0) = word;
+        }
+    }
+}
+
+int make_plane_map(CUtensorMap *map, const int8_t *base, int rows, long long ldpl, int kp,
+                   long long pstride, int ns, int box_rows) {
+    tc::EncodeTiledFn fn = tc::encode_tiled_fn();
+    if (!fn) {
+        set_error("cuTensorMapEncodeTiled is unavailable");
+        return FMLB_ECUDA;
+    }
+    FMLB_REQUIRE(((uintptr_t)base % 16) == 0 && ldpl % 16 == 0 && pstride % 16 == 0,
+                 "ozaki: digit planes not 16-byte aligned");
+    const cuuint64_t gdim[3] = {(cuuint64_t)kp, (cuuint64_t)rows, (cuuint64_t)ns};
+    const cuuint64_t gstride[2] = {(cuuint64_t)ldpl, (cuuint64_t)pstride};
+    const cuuint32_t box[3] = {(cuuint32_t)OZ_KB, (cuuint32_t)box_rows, (cuuint32_t)ns};
+    const cuuint32_t estride[3] = {1, 1, 1};
+    CUresult res = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<int8_t *>(base), gdim,
+                      gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (res != CUDA_SUCCESS) {
+        set_error("ozaki: cuTensorMapEncodeTiled failed (%d)", (int)res);
+        return FMLB_ECUDA;
+    }
+    return FMLB_OK;
+}
+
+size_t oz_smem_bytes(int ns) {
+    return (size_t)OZ_STAGES * ns * (OZ_A_PLANE + OZ_B_PLANE) + OZ_STAGE_STG + 128 + 1024;
+}
+
+thread_local tc::TestHooks t_hooks = {0, 0};
+
+}  // namespace
+
+tc::TestHooks tc::test_hooks() {
+    tc::TestHooks h = t_hooks;
+    if (h.wait_budget <= 0) h.wait_budget = kOzDefaultBudget;
+    return h;
+}
+
+int ozaki_split(const double *P, long long ldp, int m, int k, const OzakiSlices &s, const int *info,
+                cudaStream_t st) {
+    if (m <= 0) return FMLB_OK;
+    FMLB_REQUIRE(m <= s.rows && k <= s.kp, "ozaki: panel %d x %d exceeds the slice buffer %d x %d",
+                 m, k, s.rows, s.kp);
+    ozaki_slice_kernel<<<m, SL_TPB, 0, st>>>(P, ldp, m, k, s.kp, s.ns, s.planes, s.pstride,
+                                             s.ldpl, s.exps, info);
+    return launch_status("ozaki_slice_kernel");
+}
+
+int ozaki_syrk(double *C, long long ldc, int m, const OzakiSlices &s, int p_row0, int strip_cols,
+               int *info, cudaStream_t st) {
+    if (m <= 0) return FMLB_OK;
+    FMLB_REQUIRE(s.ns >= 1 && s.ns <= OZAKI_MAX_SLICES, "ozaki: 1..%d slices", OZAKI_MAX_SLICES);
+    FMLB_REQUIRE(s.kp % OZ_KB == 0 && s.kp <= 16384, "ozaki: k must be a multiple of 32, <= 16384");
+    FMLB_REQUIRE(p_row0 >= 0 && p_row0 + m <= s.rows, "ozaki: rows outside the slice buffer");
+    CUtensorMap mA, mB;
+    FMLB_TRY(make_plane_map(&mA, s.planes, s.rows, s.ldpl, s.kp, s.pstride, s.ns, OZ_BM));
+    FMLB_TRY(make_plane_map(&mB, s.planes, s.rows, s.ldpl, s.kp, s.pstride, s.ns, OZ_BN));
+    OzParams p;
+    p.m = m;
+    p.p_row0 = p_row0;
+    p.ns = s.ns;
+    p.nkb = s.kp / OZ_KB;
+    p.strip_cols = strip_cols > 0 ? std::min(strip_cols, m) : 0;
+    const long long Tr = ceil_div(m, OZ_BM);
+    p.strip_tiles = p.strip_cols > 0 ? ceil_div(p.strip_cols, OZ_BN) : 0;
+    p.ntiles = p.strip_tiles ? Tr * p.strip_tiles : Tr * Tr + Tr;
+    p.ldc = ldc;
+    p.exp_bias = -7 * (s.ns + 1);
+    const tc::TestHooks hooks = tc::test_hooks();
+    p.skip_loads = hooks.skip_loads;
+    const size_t smem = oz_smem_bytes(s.ns);
+    static int attr_dev = -1;
+    int dev = 0;
+    FMLB_TRY(cuda_status(cudaGetDevice(&dev), "ozaki: cudaGetDevice"));
+    if (attr_dev != dev) {
+        FMLB_TRY(cuda_status(cudaFuncSetAttribute(ozaki_syrk_kernel,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)oz_smem_bytes(OZAKI_MAX_SLICES)),
+                             "ozaki: smem attribute"));
+        attr_dev = dev;
+    }
+    const int grid = (int)std::min<long long>(p.ntiles, sm_count());
+    ozaki_syrk_kernel<<<grid, OZ_THREADS, smem, st>>>(mA, mB, s.exps, p, C, info,
+                                                       hooks.wait_budget);
+    return launch_status("ozaki_syrk_kernel");
+}
+
+size_t ozaki_slice_bytes(int rows, int kp, int ns) {
+    return (size_t)ns * rows * kp + (size_t)rows * sizeof(int) + 512;
+}
+
+int ozaki_bind(void *ws, int rows, int kp, int ns, OzakiSlices &s) {
+    FMLB_REQUIRE(kp % OZ_KB == 0, "ozaki: padded k must be a multiple of 32");
+    char *p = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(ws) + 255) & ~(uintptr_t)255);
+    s.planes = reinterpret_cast<int8_t *>(p);
+    s.rows = rows;
+    s.kp = kp;
+    s.ns = ns;
+    s.ldpl = kp;
+    s.pstride = (long long)rows * kp;
+    s.exps = reinterpret_cast<int *>(p + (size_t)ns * rows * kp);
+    return FMLB_OK;
+}
+
+}  // namespace fmlb
+
+extern "C" size_t fmlb_syrk_ozaki_workspace_bytes(int m, int k, int nslices) {
+    if (m <= 0 || k <= 0 || nslices <= 0) return 256;
+    const int kp = (k + 31) / 32 * 32;
+    return fmlb::ozaki_slice_bytes(m, kp, nslices);
+}
+
+extern "C" int fmlb_syrk_lower_ozaki(double *C, long long ldc, int m, const double *P,
+                                     long long ldp, int k, int strip_cols, int nslices,
+                                     void *work, size_t ws_bytes, int *info, void *stream) {
+    using namespace fmlb;
+    FMLB_REQUIRE(m >= 0 && k >= 0 && ldc >= m && ldp >= k && strip_cols >= 0,
+                 "fmlb_syrk_lower_ozaki: bad sizes");
+    FMLB_REQUIRE(nslices >= 1 && nslices <= OZAKI_MAX_SLICES,
+                 "fmlb_syrk_lower_ozaki: nslices must be 1..%d", OZAKI_MAX_SLICES);
+    FMLB_REQUIRE(k <= 16384, "fmlb_syrk_lower_ozaki: k=%d above 16384", k);
+    if (m == 0 || k == 0) return FMLB_OK;
+    FMLB_REQUIRE(C && P && info, "fmlb_syrk_lower_ozaki: null pointer");
+    const size_t need = fmlb_syrk_ozaki_workspace_bytes(m, k, nslices);
+    if (!work || ws_bytes < need) {
+        set_error("fmlb_syrk_lower_ozaki: workspace %zu < %zu bytes", ws_bytes, need);
+        return FMLB_ENOMEM;
+    }
+    OzakiSlices s;
+    FMLB_TRY(ozaki_bind(work, m, (k + 31) / 32 * 32, nslices, s));
+    cudaStream_t st = FMLB_STREAM(stream);
+    FMLB_TRY(ozaki_split(P, ldp, m, k, s, info, st));
+    return ozaki_syrk(C, ldc, m, s, 0, strip_cols, info, st);
+}
+
+extern "C" int fmlb_tc_test_hooks(long long wait_cycles, int skip_loads) {
+    using namespace fmlb;
+    FMLB_REQUIRE(wait_cycles >= 0, "fmlb_tc_test_hooks: negative wait budget");
+    t_hooks.wait_budget = wait_cycles;
+    t_hooks.skip_loads = skip_loads ? 1 : 0;
+    return FMLB_OK;
+}

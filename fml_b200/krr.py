@@ -31,8 +31,9 @@ def outer_panel(n):
     return 8 * PANEL if n >= 16384 else 4 * PANEL if n >= 8192 else 2 * PANEL
 
 
-def potrf_launches(n):
-    """Kernel launches of fmlb_potrf_f64 for an n x n matrix (mirrors its loops)."""
+def potrf_launches(n, ozaki=False):
+    """Kernel launches of fmlb_potrf_f64 / fmlb_potrf_ozaki_f64 for an n x n
+    matrix (mirrors their loops)."""
     W = outer_panel(n)
     count = 0
     for K0 in range(0, n, W):
@@ -41,7 +42,7 @@ def potrf_launches(n):
             count += 1 + (1 if n - k0 - PANEL > 0 else 0)  # diagonal block + panel solve
             count += 1 if end - (k0 + PANEL) > 0 else 0     # rest of the outer panel
         if K0 > 0:
-            count += 1                                       # strip of this outer block
+            count += 1 + (1 if ozaki else 0)                 # strip (+ digit split)
     for K0 in range(0, n - W, W):
         count += 1 if n - (K0 + 2 * W) > 0 else 0           # bulk update
     return count
@@ -51,9 +52,18 @@ class KRRPipeline:
     """Preallocated FP64 KRR: ``n_train`` training and ``n_mol - n_train`` test molecules.
 
     The first ``n_train`` molecules of the batch are the training set.
+
+    ``factor="fp64"`` factors on the FP64 tensor cores; ``factor="ozaki"``
+    runs the trailing updates on the int8 tensor cores (``slices`` digit
+    planes) and is followed by ``refine`` double-double refinement steps
+    (default 3 for it, 0 for the FP64 factor). With ``refine`` > 0 the
+    relative residual ||y - (K + lambda I) alpha|| / ||y|| before each step
+    and after the last is kept per sigma in ``resid`` (device, divided by
+    ||y|| by ``relative_residuals``).
     """
 
-    def __init__(self, n_mol, n_train, size, sigmas, lam, kind="gaussian"):
+    def __init__(self, n_mol, n_train, size, sigmas, lam, kind="gaussian", factor="fp64",
+                 slices=7, refine=None):
         lib = _lib.load()
         self.dev = device()
         self.n_mol, self.n_train, self.n_test = n_mol, n_train, n_mol - n_train
@@ -69,8 +79,22 @@ class KRRPipeline:
         n = n_train
         self.X = torch.empty((n_mol, self.d), **f64)
         self.K = torch.empty((self.nsig, n, n), **f64)
-        wb = lib.fmlb_potrf_workspace_bytes(n)
+        if factor not in ("fp64", "ozaki"):
+            raise ValueError("factor must be 'fp64' or 'ozaki'")
+        self.factor, self.slices = factor, int(slices)
+        self.refine = (3 if factor == "ozaki" else 0) if refine is None else int(refine)
+        if factor == "ozaki":
+            wb = lib.fmlb_potrf_ozaki_workspace_bytes(n, self.slices)
+        else:
+            wb = lib.fmlb_potrf_workspace_bytes(n)
         self.work = torch.empty((self.nsig, wb), dtype=torch.uint8, device=self.dev)
+        if self.refine > 0:
+            self.diag = torch.empty((self.nsig, n), **f64)
+            self.alpha_lo = torch.empty((self.nsig, n), **f64)
+            self.ytr = torch.empty(n, **f64)
+            sd = lib.fmlb_krr_refine_dd_scratch_doubles(n)
+            self.scratch = torch.empty((self.nsig, sd), **f64)
+            self.resid = torch.zeros((self.nsig, self.refine + 1), **f64)
         self.info = torch.zeros(self.nsig, dtype=torch.int32, device=self.dev)
         self.alpha = torch.empty((self.nsig, n), **f64)
         self.pred = torch.empty((self.nsig, max(self.n_test, 1)), **f64)
@@ -87,10 +111,19 @@ class KRRPipeline:
     def launches_per_run(self):
         """Kernel launches of one ``run`` (mirrors the loops in the C library)."""
         nblk = -(-self.n_train // PANEL)
-        potrf = potrf_launches(self.n_train)
+        potrf = potrf_launches(self.n_train, self.factor == "ozaki")
         potrs = 2 * nblk
         per_sigma = 1 + potrf + potrs
+        if self.refine > 0:  # diagonal, then per step 3 residual + 2 norm + potrs + update
+            per_sigma += 1 + self.refine * (5 + potrs + 1) + 5
         return 1 + 1 + self.nsig * per_sigma + (2 if self.n_test else 0)
+
+    def relative_residuals(self):
+        """(nsigma, refine + 1) host array of ||r|| / ||y|| (refine > 0 only)."""
+        if self.refine == 0:
+            raise ValueError("the pipeline keeps residuals only with refine > 0")
+        ny = float(torch.linalg.vector_norm(self.ytr))
+        return self.resid.cpu().numpy() / ny
 
     def run_descriptors(self, X, y_train, stream=None):
         """Like ``run`` with the descriptor rows (n_mol, d) given instead of molecules."""
@@ -112,6 +145,9 @@ class KRRPipeline:
         _lib.call(fn, _lib.ptr(self.X), n, d, _lib.ptr(self.X), n, d, d, self._sig_ptr, self.nsig,
                   _lib.ptr(self.K), n, n * n, 1, s)
         main = stream if stream is not None else torch.cuda.current_stream(self.dev)
+        if self.refine > 0:
+            with torch.cuda.stream(main):
+                self.ytr.copy_(y_train)
         self._fork.record(main)
         for k in range(self.nsig):
             Kk = self.K[k]
@@ -119,12 +155,26 @@ class KRRPipeline:
             sk.wait_event(self._fork)
             h = _lib.stream_handle(sk)
             _lib.call("fmlb_add_diagonal_f64", _lib.ptr(Kk), n, n, self.lam, h)
-            _lib.call("fmlb_potrf_f64", _lib.ptr(Kk), n, n, _lib.ptr(self.work[k]),
-                      _lib.ptr(self.info[k:k + 1]), h)
+            if self.refine > 0:
+                _lib.call("fmlb_get_diagonal_f64", _lib.ptr(Kk), n, n, _lib.ptr(self.diag[k]), h)
+            if self.factor == "ozaki":
+                _lib.call("fmlb_potrf_ozaki_f64", _lib.ptr(Kk), n, n, self.slices,
+                          _lib.ptr(self.work[k]), self.work.shape[1],
+                          _lib.ptr(self.info[k:k + 1]), h)
+            else:
+                _lib.call("fmlb_potrf_f64", _lib.ptr(Kk), n, n, _lib.ptr(self.work[k]),
+                          _lib.ptr(self.info[k:k + 1]), h)
             with torch.cuda.stream(sk):
                 self.alpha[k].copy_(y_train)
             _lib.call("fmlb_potrs_f64", _lib.ptr(Kk), n, n, _lib.ptr(self.work[k]),
                       _lib.ptr(self.alpha[k]), h)
+            if self.refine > 0:
+                with torch.cuda.stream(sk):
+                    self.alpha_lo[k].zero_()
+                _lib.call("fmlb_krr_refine_dd", _lib.ptr(Kk), n, n, _lib.ptr(self.diag[k]),
+                          _lib.ptr(self.work[k]), _lib.ptr(self.ytr), _lib.ptr(self.alpha[k]),
+                          _lib.ptr(self.alpha_lo[k]), self.refine, _lib.ptr(self.resid[k]),
+                          _lib.ptr(self.scratch[k]), h)
             self._joins[k].record(sk)
         for ev in self._joins:
             main.wait_event(ev)
@@ -138,11 +188,12 @@ class KRRPipeline:
 
 
 def krr_fit_predict(charges, coords, offsets, y_train, n_train, sigmas, lam, size=23,
-                    kind="gaussian", return_info=False):
+                    kind="gaussian", return_info=False, factor="fp64", slices=7, refine=None):
     """Train on the first ``n_train`` molecules, predict the rest, for every sigma.
 
     Molecules are packed (charges, coords, offsets). Returns (nsigma, n_test)
     predictions (numpy for numpy input, a device tensor for torch input).
+    ``factor``, ``slices`` and ``refine`` as for ``KRRPipeline``.
     """
     off = offsets.cpu().numpy() if isinstance(offsets, torch.Tensor) else np.asarray(offsets)
     n_mol = len(off) - 1
@@ -150,7 +201,8 @@ def krr_fit_predict(charges, coords, offsets, y_train, n_train, sigmas, lam, siz
     r, _ = to_device(coords, torch.float64)
     o, _ = to_device(offsets, torch.int32)
     y, _ = to_device(y_train, torch.float64)
-    pipe = KRRPipeline(n_mol, n_train, size, np.atleast_1d(sigmas), lam, kind)
+    pipe = KRRPipeline(n_mol, n_train, size, np.atleast_1d(sigmas), lam, kind, factor, slices,
+                       refine)
     pred = pipe.run(z, r, o, y)
     out = to_output(pred, as_np)
     if return_info:

@@ -321,6 +321,59 @@ int fmlb_potri_f64(double *A, long long lda, int n, const void *work, double *V,
 int fmlb_syrk_lower_f64(double *C, long long ldc, int m, const double *P, long long ldp, int k,
                         int strip_cols, const int *info, void *stream);
 
+/* FP64-accurate Cholesky factorisation with the trailing updates on the int8
+ * tensor cores, the replacement for LAPACK dpotrf('U') as fcho_solve calls it
+ * (fml/math/fcho_solve.f90:35) when an iterative refinement follows.
+ * Same storage, result layout, workspace prefix (the inverted diagonal blocks
+ * that fmlb_potrs_f64 reads) and info as fmlb_potrf_f64; only the bulk and
+ * strip trailing updates (C -= P P^T with k = the outer panel width) change:
+ * P's rows are split into nslices (1..8) signed 7-bit digit planes with one
+ * power-of-two scale per row, the s(s+1)/2 leading digit products run as
+ * tcgen05.mma kind::i8 with exact int32 accumulation, and the epilogue
+ * combines them in FP64 (the Ozaki scheme). Per update the error is about
+ * 16x the FP64 rounding bound at nslices = 7 and below it at 8.
+ *   work  fmlb_potrf_ozaki_workspace_bytes(n, nslices) bytes
+ *   info  LAPACK-style (> 0: first non-positive pivot); FMLB_ETIMEDOUT (< 0)
+ *         if a bounded device-side wait of the tensor-core kernel gave up. */
+size_t fmlb_potrf_ozaki_workspace_bytes(int n, int nslices);
+int fmlb_potrf_ozaki_f64(double *A, long long lda, int n, int nslices, void *work,
+                         size_t ws_bytes, int *info, void *stream);
+
+/* The int8 emulated trailing update on its own (the step above): C -= P P^T
+ * on the triangle i >= j of the row-major (m, m) C, or its first strip_cols
+ * columns; P is (m, k), k <= 16384. work: fmlb_syrk_ozaki_workspace_bytes
+ * (m, k, nslices) bytes (digit planes and row exponents). info (device):
+ * skipped when non-zero; FMLB_ETIMEDOUT stored on a device-side timeout.
+ * (The LAPACK dsyrk call inside dpotrf, fcho_solve.f90:35.) */
+size_t fmlb_syrk_ozaki_workspace_bytes(int m, int k, int nslices);
+int fmlb_syrk_lower_ozaki(double *C, long long ldc, int m, const double *P, long long ldp, int k,
+                          int strip_cols, int nslices, void *work, size_t ws_bytes, int *info,
+                          void *stream);
+
+/* Test hooks of the tensor-core kernels (fmlb_gaussian_kernel_tc,
+ * fmlb_syrk_lower_ozaki, fmlb_potrf_ozaki_f64) for later launches from the
+ * calling host thread: wait_cycles > 0 sets the clock-cycle limit of every
+ * device-side mbarrier wait (0 restores the default, about 2 s); skip_loads
+ * != 0 makes the TMA producer issue no copies, so the waits run out with
+ * nothing in flight and the kernel reports FMLB_ETIMEDOUT. No reference
+ * counterpart (failure-path testing). */
+int fmlb_tc_test_hooks(long long wait_cycles, int skip_loads);
+
+/* Double-double iterative refinement after an in-place factorisation of
+ * A = K + lambda I (fmlb_potrf_f64 or fmlb_potrf_ozaki_f64), reading K from
+ * the strict upper triangle the factorisation leaves untouched and the
+ * diagonal from `diag` (saved before factoring with fmlb_get_diagonal_f64).
+ * The reference solves once (fml/math/fcho_solve.f90:35-42); this extends it
+ * past the FP64 residual floor. x = x + x_lo is kept in double-double; per
+ * step r = y - A (x + x_lo) in double-double, (x, x_lo) += solve(L, r).
+ * resid (device, iters + 1, may be NULL): ||r||_2 before each step and after
+ * the last. scratch: fmlb_krr_refine_dd_scratch_doubles(n). Deterministic. */
+int fmlb_get_diagonal_f64(const double *A, long long lda, int n, double *diag, void *stream);
+size_t fmlb_krr_refine_dd_scratch_doubles(int n);
+int fmlb_krr_refine_dd(const double *A, long long lda, int n, const double *diag,
+                       const void *work, const double *y, double *x, double *x_lo, int iters,
+                       double *resid, double *scratch, void *stream);
+
 /* FP64 residual and iterative refinement after fmlb_potrf_f64 (the reference
  * solves once, fml/math/fcho_solve.f90:35-42, and leaves the residual to the
  * user). For (K + lambda I) x = y with K full and symmetric (row-major, both

@@ -170,6 +170,22 @@ def laplacian_kernel(A, B, sigma):
     return K
 
 
+def kernels_multi(kind, A, B, sigmas):
+    """Gaussian (kind "gaussian") or Laplacian ("laplacian") kernels for every
+    sigma from one pass over the pairs (fkernels.f90:317-377); each plane is
+    bit-identical to gaussian_kernel / laplacian_kernel at that sigma.
+    Returns (nsigma, na, nb)."""
+    a, b = _rows(A), _rows(B)
+    na, nb, d = a.shape[0], b.shape[0], a.shape[1]
+    sig = np.ascontiguousarray(np.atleast_1d(np.asarray(sigmas, dtype=np.float64)))
+    if not 1 <= len(sig) <= 16:
+        raise ValueError("1..16 sigmas")
+    K = np.empty((len(sig), na, nb))
+    _lib().orc_kernels_multi({"gaussian": 0, "laplacian": 1}[kind], _p(a), na, _p(b), nb, d,
+                             _p(sig), len(sig), _p(K))
+    return K
+
+
 def _ptp_pad(Z, amax):
     out = np.zeros((len(Z), amax, 2))
     for i, z in enumerate(Z):

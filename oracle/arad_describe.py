@@ -43,7 +43,10 @@ def describe(coords, charges, size=30, cut=5.0):
         damp = 1.0 - np.sin(np.pi * d1[None, :] / (2.0 * cut))  # :107-108
         cos_a = np.cos(ang) * damp
         sin_a = np.sin(ang) * damp
-        order = np.argsort(d1, kind="stable")  # :110
+        # :110 with numpy's default sort, as the reference calls it: its order
+        # of exactly equidistant neighbours (not stable above 16 entries) is
+        # part of the descriptor (channels 1-4)
+        order = np.argsort(d1)
         d1s = d1[order]
         keep = np.nonzero(d1s < cut)[0]  # :121
         sel = order[keep]

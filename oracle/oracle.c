@@ -444,6 +444,42 @@ void orc_laplacian_kernel(const double *A, int na, const double *B, int nb, int 
 }
 
 /* ------------------------------------------------------------------------ */
+/* Several sigmas from one pass (fkernels.f90:317-377, the loops above): the  */
+/* pair sum s of each (j, i) is formed once, in the same order as the single- */
+/* sigma routines, and exp(inv_sigma * s) is taken per sigma, so every K_k is  */
+/* bit-identical to orc_gaussian_kernel / orc_laplacian_kernel at sigma_k.     */
+/* kind 0: Gaussian (sum of squares, inv_sigma = -0.5/sigma^2, :334, :341);    */
+/* kind 1: Laplacian (sum of |a - b|, inv_sigma = -1/sigma, :367, :372).       */
+/* K is (nsig, na, nb) row-major.                                              */
+/* ------------------------------------------------------------------------ */
+void orc_kernels_multi(int kind, const double *A, int na, const double *B, int nb, int d,
+                       const double *sigmas, int nsig, double *K)
+{
+    double inv[16];
+    for (int q = 0; q < nsig && q < 16; ++q)
+        inv[q] = kind == 0 ? -0.5 / (sigmas[q] * sigmas[q]) : -1.0 / sigmas[q];
+    const size_t plane = (size_t)na * nb;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < nb; ++i) {
+        const double *b = B + (size_t)i * d;
+        for (int j = 0; j < na; ++j) {
+            const double *a = A + (size_t)j * d;
+            double s = 0.0;
+            if (kind == 0) {
+                for (int k = 0; k < d; ++k) {
+                    double t = a[k] - b[k];
+                    s = s + t * t;
+                }
+            } else {
+                for (int k = 0; k < d; ++k) s = s + fabs(a[k] - b[k]);
+            }
+            for (int q = 0; q < nsig && q < 16; ++q)
+                K[q * plane + (size_t)j * nb + i] = exp(inv[q] * s);
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
 /* ARAD atom-pair distance: farad_kernels.f90:29-90 (atomic_distl2)           */
 /* ------------------------------------------------------------------------ */
 /* x1, x2: one atom's descriptor (5, amax) row-major; s1, s2: sine factors.   */

@@ -86,6 +86,27 @@ def read_xyz(path, charge_table):
     return natoms, symbols, np.array(coords)
 
 
+def tie_molecules():
+    """Molecules whose atoms have exactly equidistant neighbours of different
+    elements: a centre atom plus the 24 signed permutations of (a, b, c) with
+    an even number of minus signs. The squares of a, b, c and their sums are
+    exact in binary, so the 24 centre distances are bit-equal; no vertex has
+    its antipode in the set, so no three atoms are collinear (collinear atoms
+    send arad.py's arccos slightly past +-1, to NaN)."""
+    from itertools import permutations
+    cyc = np.array([1.0, 6.0, 7.0, 8.0, 16.0])
+    mols = []
+    for abc, zc in (((0.75, 1.25, 1.5), 6.0), ((0.5, 1.25, 2.0), 7.0)):
+        pts = [(0.0, 0.0, 0.0)]
+        for perm in permutations(abc):
+            for signs in ((1, 1, 1), (1, -1, -1), (-1, 1, -1), (-1, -1, 1)):
+                pts.append(tuple(s * v for s, v in zip(signs, perm)))
+        r = np.array(pts)
+        z = np.concatenate([[zc], cyc[np.arange(len(r) - 1) % 5]])
+        mols.append((z, r))
+    return mols
+
+
 def main():
     arad_mod = _load_module("ref_arad", os.path.join(REF, "fml/arad.py"))
     data_mod = _load_module("ref_data", os.path.join(REF, "fml/data.py"))
@@ -120,6 +141,16 @@ def main():
         a = arad_mod.ARAD(maxMolSize=23, maxAts=23, cut=cut)
         arad["syn_s23_c%g" % cut] = np.stack(
             [a.describe(syn.molecule(i)[1], syn.molecule(i)[0]) for i in range(syn.nmol)])
+
+    # ---- exact ties: equidistant neighbours of different elements ---------
+    # arad.py:110 sorts neighbour distances with numpy's default argsort, which
+    # is not stable above 16 elements; these molecules have many exact ties.
+    ties = tie_molecules()
+    for size, cut in ((30, 5.0), (30, 1e6)):
+        a = arad_mod.ARAD(maxMolSize=size, maxAts=size, cut=cut)
+        arad["ties_s%d_c%g" % (size, cut)] = np.stack([a.describe(r, z) for z, r in ties])
+    tie_off = np.zeros(len(ties) + 1, dtype=np.int32)
+    np.cumsum([len(z) for z, _ in ties], out=tie_off[1:])
 
     # ---- sorted Coulomb matrices from representations.py ------------------
     rep_path = os.path.join(REF, "fml/representations/representations.py")
@@ -202,6 +233,8 @@ def main():
         **{"arad_" + k: v for k, v in arad.items()},
         **{"cm_" + k: v for k, v in cm.items()},
         **{"lcm_" + k: v for k, v in lcm.items()},
+        ties_charges=np.concatenate([z for z, _ in ties]),
+        ties_coords=np.concatenate([r for _, r in ties]), ties_offsets=tie_off,
         syn11_charges=syn.charges, syn11_coords=syn.coords, syn11_offsets=syn.offsets,
         syn12_charges=syn_cm.charges, syn12_coords=syn_cm.coords,
         syn12_offsets=syn_cm.offsets,

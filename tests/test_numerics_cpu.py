@@ -32,3 +32,52 @@ def test_fp32_cholesky_breaks_down_where_fp64_succeeds(oracle_mod, cm_kernel_inp
     _, info64 = lapack.dpotrf(A, lower=1)
     assert info64 == 0
     assert info32 > 0
+
+
+def _blocked_cholesky(A, W, nslices):
+    """Right-looking blocked Cholesky whose trailing updates are the int8
+    (Ozaki) emulation with ``nslices`` digit planes (0: exact FP64 products),
+    diagonal blocks and panel solves in FP64 - the structure of
+    fmlb_potrf_ozaki_f64. None on breakdown."""
+    import scipy.linalg as sla
+    import ozaki_emulation as emu
+    L = np.tril(A).copy()
+    n = len(A)
+    for K0 in range(0, n, W):
+        K1 = min(K0 + W, n)
+        try:
+            L[K0:K1, K0:K1] = np.linalg.cholesky(L[K0:K1, K0:K1])
+        except np.linalg.LinAlgError:
+            return None
+        if K1 < n:
+            L[K1:, K0:K1] = sla.solve_triangular(L[K0:K1, K0:K1], L[K1:, K0:K1].T, lower=True).T
+            P = L[K1:, K0:K1]
+            L[K1:, K1:] -= np.tril(P @ P.T if nslices == 0 else emu.product(P, nslices))
+    return np.tril(L)
+
+
+@pytest.mark.parametrize("sigma", [100.0, 1600.0])
+def test_ozaki_slices_needed_for_fp64_refined_accuracy(oracle_mod, cm_kernel_inputs, sigma):
+    """Why fmlb_potrf_ozaki_f64 defaults to 7 digit planes: on these kernels
+    at lambda = 1e-8 a factor from 7 planes, refined three times with FP64
+    residuals, reaches the residual of the FP64 factor refined the same way,
+    while 4 planes leave it orders of magnitude above (or break down)."""
+    import scipy.linalg as sla
+    X = cm_kernel_inputs
+    A = oracle_mod.gaussian_kernel(X.T, X.T, sigma) + 1e-8 * np.eye(len(X))
+    y = np.random.default_rng(0).standard_normal(len(X))
+
+    def refined_residual(L):
+        def solve(v):
+            return sla.solve_triangular(L.T, sla.solve_triangular(L, v, lower=True), lower=False)
+        x = solve(y)
+        for _ in range(3):
+            x = x + solve(y - A @ x)
+        return np.linalg.norm(y - A @ x) / np.linalg.norm(y)
+
+    r64 = refined_residual(_blocked_cholesky(A, 256, 0))
+    L7 = _blocked_cholesky(A, 256, 7)
+    assert L7 is not None
+    assert refined_residual(L7) <= 4 * r64
+    L4 = _blocked_cholesky(A, 256, 4)
+    assert L4 is None or refined_residual(L4) > 100 * r64

@@ -143,3 +143,31 @@ def test_gaussian_laplacian_oracle_cross_checked_by_scipy(golden, oracle_mod):
         np.testing.assert_allclose(oracle_mod.laplacian_kernel(A, B, sigma),
                                    np.exp(-cdist(A.T, B.T, "cityblock") / sigma),
                                    rtol=1e-12, atol=1e-300)
+
+
+def test_multi_sigma_oracle_bit_identical_to_single_sigma(golden, oracle_mod):
+    """kernels_multi (used by the headline-pipeline parity test) forms each
+    pair sum once and must give, bit for bit, the single-sigma restatements."""
+    X = golden["cm_syn_s23"]
+    A, B = X[:33].T, X[33:].T
+    sig = [50.0, 724.0, 3000.0]
+    for kind, single in (("gaussian", oracle_mod.gaussian_kernel),
+                         ("laplacian", oracle_mod.laplacian_kernel)):
+        K = oracle_mod.kernels_multi(kind, A, B, sig)
+        for q, s in enumerate(sig):
+            np.testing.assert_array_equal(K[q], single(A, B, s))
+
+
+@pytest.mark.parametrize("cut", [5.0, 1e6])
+def test_arad_describe_oracle_keeps_reference_tie_order(golden, oracle_mod, cut):
+    """Exactly equidistant neighbours of different elements (25 atoms, ties of
+    up to 24): arad.py:110 sorts with numpy's default (non-stable above 16
+    entries) argsort, and the oracle reproduces its order. Channels 0-2
+    (distances, neighbour PTP row/column) are bit-equal; channels 3-4 agree to
+    rounding."""
+    g = golden
+    d = oracle_mod.arad_descriptors(g["ties_charges"], g["ties_coords"], g["ties_offsets"], 30,
+                                    cut)
+    ref = g["arad_ties_s30_c%g" % cut]
+    np.testing.assert_array_equal(d[:, :, :3, :], ref[:, :, :3, :])
+    np.testing.assert_allclose(d, ref, rtol=0, atol=1e-14)

@@ -93,6 +93,42 @@ def test_arad_descriptors_vs_oracle(oracle_mod, cut, nmax):
     np.testing.assert_allclose(d, ref, rtol=1e-12, atol=1e-13)
 
 
+def _canonical_neighbours(D):
+    """Neighbour columns of every atom's (5, size) block sorted by all five
+    channels: equal for two descriptors that differ only in the order of
+    exactly equidistant neighbours."""
+    out = np.empty_like(D)
+    for m in range(D.shape[0]):
+        for a in range(D.shape[1]):
+            blk = D[m, a]
+            order = np.lexsort(np.round(blk[::-1], 12))
+            out[m, a] = blk[:, order]
+    return out
+
+
+@pytest.mark.parametrize("cut", [5.0, 1e6])
+def test_arad_descriptors_exact_ties_vs_reference(golden, cut):
+    """Molecules with exactly equidistant neighbours of different elements.
+    The reference orders such ties by numpy's default argsort (arad.py:110,
+    not stable above 16 entries); the kernel orders them by atom index. The
+    descriptors agree as sets of neighbour records (1e-13), and the ARAD
+    kernels built from them agree to 1e-12, since the kernel sums over all
+    neighbour pairs."""
+    g = golden
+    d = fml_b200.generate_arad_descriptors(g["ties_charges"], g["ties_coords"], g["ties_offsets"],
+                                           size=30, cut=cut)
+    ref = g["arad_ties_s30_c%g" % cut]
+    np.testing.assert_array_equal(d[:, :, 0, :], ref[:, :, 0, :])   # sorted distances
+    np.testing.assert_allclose(_canonical_neighbours(d), _canonical_neighbours(ref), rtol=0,
+                               atol=1e-13)
+    off = g["ties_offsets"]
+    Z = [list(g["ties_charges"][off[i]:off[i + 1]]) for i in range(len(off) - 1)]
+    sig = [0.1, 1.0, 5.0]
+    K = fml_b200.get_atomic_symmetric_kernels_arad(d, Z, sig)
+    Kref = fml_b200.get_atomic_symmetric_kernels_arad(ref, Z, sig)
+    np.testing.assert_allclose(K, Kref, rtol=1e-12, atol=0)
+
+
 def test_arad_unknown_element_raises():
     with pytest.raises(KeyError):
         fml_b200.generate_arad_descriptors(np.array([1.0, 0.0]), np.random.rand(2, 3), [0, 2])
