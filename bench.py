@@ -54,6 +54,18 @@ def parse():
     p.add_argument("--sigmas", default="100,400,1600")
     p.add_argument("--lam", type=float, default=1e-8)
     p.add_argument("--seed", type=int, default=2)
+    p.add_argument("--factor", default="ozaki", choices=["ozaki", "fp64"],
+                   help="factorisation of the headline step: 'ozaki' (trailing updates on "
+                        "the int8 tensor cores, then double-double refinement) or 'fp64' "
+                        "(FP64 tensor cores, no refinement)")
+    p.add_argument("--slices", type=int, default=7, help="digit planes of the int8 factor")
+    p.add_argument("--refine", type=int, default=None,
+                   help="double-double refinement steps (default 3 with the int8 factor, 0 "
+                        "with the FP64 one)")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the measurements reported beside the headline (FP64-factor "
+                        "path, Laplacian and lambda=1e-6 legs, mixed kernels, batched, "
+                        "serving)")
     p.add_argument("--cpu-ntrain", type=int, default=4096)
     p.add_argument("--cpu-ntest", type=int, default=1024)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -61,7 +73,7 @@ def parse():
     p.add_argument("--stages", nargs="?", const="all", default=None,
                    help="time each hot-path kernel on its own (one JSON line per stage); "
                         "'arad' times only the ARAD kernels, 'build' only the descriptors "
-                        "and kernel-matrix builds")
+                        "and kernel-matrix builds, 'factor' only the factorisations")
     p.add_argument("--workload", default="krr",
                    choices=["krr", "batched", "serving", "small", "arad"],
                    help="krr: the large-N KRR step (default, the headline line); batched: "
@@ -88,6 +100,18 @@ def workload_name(a, nsig):
     return ("gaussian KRR on sorted Coulomb matrices: N_train=%d, N_test=%d, nmax=%d (d=%d), "
             "sigma=%s, lambda=%g, FP64" % (a.ntrain, a.ntest, a.nmax, a.nmax * (a.nmax + 1) // 2,
                                           a.sigmas, a.lam))
+
+
+def refine_steps(a):
+    return (3 if a.factor == "ozaki" else 0) if a.refine is None else a.refine
+
+
+def factor_name(a):
+    if a.factor == "ozaki":
+        return ("int8 tensor-core (Ozaki, %d digit planes) trailing updates + %d double-double "
+                "refinement steps" % (a.slices, refine_steps(a)))
+    return "FP64 tensor-core factorisation" + (
+        " + %d double-double refinement steps" % refine_steps(a) if refine_steps(a) else "")
 
 
 # ---------------------------------------------------------------------------
@@ -192,23 +216,34 @@ def run_reference(a):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def measure_syrk(pipe, torch, lib_call, ptr, stream):
-    """Per-launch timing of the dominant kernel (FP64 trailing update) over the
+def measure_syrk(pipe, torch, lib_call, ptr, stream, factor="fp64", slices=7):
+    """Per-launch timing of the dominant kernel (the trailing update) over the
     launch sequence of one factorisation (the strip of each next outer block
     and the bulk past it, with k = the outer panel width), on the pipeline's K
-    buffer."""
+    buffer. factor "ozaki" times fmlb_syrk_lower_ozaki (digit split + int8
+    tensor-core update per launch), "fp64" fmlb_syrk_lower_f64."""
+    from fml_b200 import _lib
     from fml_b200.krr import outer_panel
     n = pipe.n_train
     W = outer_panel(n)
     K = pipe.K[0]
     evs = []
     flops = 0.0
+    if factor == "ozaki":
+        lib = _lib.load()
+        ws = torch.empty(lib.fmlb_syrk_ozaki_workspace_bytes(n, W, slices), dtype=torch.uint8,
+                         device=K.device)
+        info = torch.zeros(1, dtype=torch.int32, device=K.device)
 
     def timed(Cv, m, Pv, strip):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        lib_call("fmlb_syrk_lower_f64", ptr(Cv), n, m, ptr(Pv), n, W, strip, None, stream)
+        if factor == "ozaki":
+            lib_call("fmlb_syrk_lower_ozaki", ptr(Cv), n, m, ptr(Pv), n, W, strip, slices,
+                     ptr(ws), ws.numel(), ptr(info), stream)
+        else:
+            lib_call("fmlb_syrk_lower_f64", ptr(Cv), n, m, ptr(Pv), n, W, strip, None, stream)
         e1.record()
         evs.append((e0, e1))
 
@@ -226,6 +261,29 @@ def measure_syrk(pipe, torch, lib_call, ptr, stream):
     torch.cuda.synchronize()
     ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
     return flops, ms, len(evs)
+
+
+def measure_int8_peak(torch):
+    """Dense int8 tensor-core throughput of a library GEMM (torch._int_mm,
+    cuBLASLt) at 8192^3, best of 4; None if unavailable."""
+    try:
+        n = 8192
+        a = torch.randint(-127, 127, (n, n), dtype=torch.int8, device="cuda")
+        b = torch.randint(-127, 127, (n, n), dtype=torch.int8, device="cuda")
+        torch._int_mm(a, b)
+        best = 1e30
+        for _ in range(4):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        del a, b
+        return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+    except Exception:  # noqa: BLE001 - a missing library path only loses the figure
+        return None
 
 
 def measure_dgemm_peak(torch):
@@ -262,7 +320,6 @@ def run_ours(a):
     import torch
     import torch.distributed as dist
 
-    import fml_b200
     from fml_b200 import _lib, krr, synthetic
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -282,8 +339,9 @@ def run_ours(a):
     r = torch.from_numpy(b.coords).to(dev)
     o = torch.from_numpy(b.offsets).to(dev)
     y = torch.from_numpy(np.ascontiguousarray(b.energies[:a.ntrain])).to(dev)
-    pipe = krr.KRRPipeline(n_mol, a.ntrain, a.nmax, sigmas, a.lam)
-    stream = torch.cuda.current_stream()
+    nref = refine_steps(a)
+    pipe = krr.KRRPipeline(n_mol, a.ntrain, a.nmax, sigmas, a.lam, factor=a.factor,
+                           slices=a.slices, refine=nref)
 
     for _ in range(a.warmup):
         pipe.run(z, r, o, y)
@@ -344,51 +402,61 @@ def run_ours(a):
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(nsig * a.ntest * 8),
                "ms_per_step": ems, "api": "fml_b200.krr.KRRPipeline.run on host-pinned inputs"}
 
-    # relative residual ||y - (K + lambda I) alpha|| / ||y|| of every sigma, in FP64 on
-    # the device (fmlb_krr_refine_f64), with K rebuilt after the timed region (the
-    # factorisation overwrote it), before and after one FP64 refinement step
-    resid, resid_ir = {}, {}
-    n_tr, d_cm = a.ntrain, pipe.d
-    lib = _lib.load()
-    Kr = torch.empty((n_tr, n_tr), dtype=torch.float64, device=dev)
-    scratch = torch.empty(lib.fmlb_krr_refine_scratch_doubles(n_tr), dtype=torch.float64,
-                          device=dev)
-    rn = torch.empty(2, dtype=torch.float64, device=dev)
-    hs = _lib.stream_handle()
-    ynorm = float(np.linalg.norm(b.energies[:n_tr]))
-    for k, s in enumerate(sigmas):
-        sp, keep = _lib.host_doubles([s])
-        _lib.call("fmlb_gaussian_kernel_f64", _lib.ptr(pipe.X), n_tr, d_cm, _lib.ptr(pipe.X), n_tr,
-                  d_cm, d_cm, sp, 1, _lib.ptr(Kr), n_tr, n_tr * n_tr, 1, hs)
-        xk = pipe.alpha[k].clone()
-        _lib.call("fmlb_krr_refine_f64", _lib.ptr(Kr), n_tr, n_tr, a.lam, _lib.ptr(pipe.K[k]),
-                  n_tr, _lib.ptr(pipe.work[k]), _lib.ptr(y), _lib.ptr(xk), 1, _lib.ptr(rn),
-                  _lib.ptr(scratch), hs)
-        r0, r1 = rn.cpu().numpy()
-        resid[str(s)] = float(r0 / ynorm)
-        resid_ir[str(s)] = float(r1 / ynorm)
-        del keep
-    del Kr, scratch
+    # relative residuals ||y - (K + lambda I) alpha|| / ||y|| in double-double
+    # (K from the strict upper triangle the factorisation leaves in place)
+    if nref > 0:
+        rr = pipe.relative_residuals()
+        residuals = {str(s): [float(v) for v in rr[k]] for k, s in enumerate(sigmas)}
+        res_key = "relative_residual_per_refinement_step"
+    else:
+        rr = pipe.residual_now()
+        residuals = {str(s): float(rr[k]) for k, s in enumerate(sigmas)}
+        res_key = "relative_residual"
 
-    # dominant kernel: FP64 trailing update of the factorisation
-    flops, syrk_ms, nl = measure_syrk(pipe, torch, _lib.call, _lib.ptr, _lib.stream_handle())
-    peak = measure_dgemm_peak(torch)
-    achieved = flops / (syrk_ms * 1e-3) / 1e12
+    # dominant kernel: the trailing update of the factorisation
+    flops, syrk_ms, nl = measure_syrk(pipe, torch, _lib.call, _lib.ptr, _lib.stream_handle(),
+                                      a.factor, a.slices)
+    dgemm = measure_dgemm_peak(torch)
+    fp64_equiv = flops / (syrk_ms * 1e-3) / 1e12
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "syrk_update_f64_traffic.json")
+    if a.factor == "ozaki":
+        nprod = a.slices * (a.slices + 1) // 2
+        int8_peak = measure_int8_peak(torch)
+        peaks = _measured_peaks()
+        peak, peak_src = int8_peak, "torch._int_mm (cuBLASLt int8) 8192^3 measured in this run"
+        if peak is None:
+            peak = 2.0 * peaks["bf16_tflops"]
+            peak_src = "2 x measured dense bf16 (MEASURED_PEAKS.json): no int8 GEMM measured"
+        achieved = flops * nprod / (syrk_ms * 1e-3) / 1e12
+        tpath = os.path.join(ROOT, "profiles", "ozaki_syrk_traffic.json")
+        roofline = {"bound": "tensor", "pipe": "int8 tensor cores (tcgen05.mma kind::i8)",
+                    "kernel": "ozaki_syrk_kernel (int8 emulated FP64 trailing update, %d "
+                              "digit products per FP64 product; timing includes the digit "
+                              "split)" % nprod,
+                    "achieved": achieved, "peak": peak, "unit": "TOPS (int8)",
+                    "frac": achieved / peak, "peak_source": peak_src,
+                    "fp64_equivalent_tflops": fp64_equiv, "dgemm_tflops_measured": dgemm,
+                    "fp64_equivalent_vs_dgemm": fp64_equiv / dgemm}
+    else:
+        tpath = os.path.join(ROOT, "profiles", "syrk_update_f64_traffic.json")
+        roofline = {"bound": "tensor", "pipe": "FP64 DMMA (mma.sync m8n8k4 f64)",
+                    "kernel": "syrk_dmma_kernel (FP64 trailing update)",
+                    "achieved": fp64_equiv, "peak": dgemm, "unit": "TFLOP/s",
+                    "frac": fp64_equiv / dgemm,
+                    "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json "
+                                   "holds no FP64 figure)"}
     if os.path.exists(tpath):
         try:
             traffic = json.load(open(tpath)).get("bytes_per_launch")
         except (OSError, ValueError):
             traffic = None
-    roofline = {"bound": "tensor", "pipe": "FP64 DMMA (mma.sync m8n8k4 f64)",
-                "kernel": "syrk_dmma_kernel (FP64 trailing update)",
-                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json "
-                               "holds no FP64 figure)",
-                "traffic": traffic, "launches": nl, "avg_launch_ms": syrk_ms / nl,
-                "share_of_step": syrk_ms * nsig / ms,
-                "algorithmic_flops_per_launch": flops / nl}
+    roofline.update({"traffic": traffic, "launches": nl, "avg_launch_ms": syrk_ms / nl,
+                     "share_of_step": syrk_ms * nsig / ms,
+                     "algorithmic_fp64_flops_per_launch": flops / nl})
+
+    extras = None
+    if rank == 0 and world == 1 and not a.no_extras:
+        extras = headline_extras(a, torch, pipe, b, sigmas, dev, z, r, o, y, pred, ms)
 
     cpu = None
     if rank == 0 and not a.no_cpu_baseline:
@@ -399,29 +467,234 @@ def run_ours(a):
         dt = time.perf_counter() - t0
         cpu = {"value": entries_per_step(a.cpu_ntrain, a.cpu_ntest, nsig) / dt, "unit": UNIT,
                "cores": _CORES, "kind": "port",
-               "sample": "N_train=%d, N_test=%d, same sigmas/lambda, one step of %.1f s"
-                         % (a.cpu_ntrain, a.cpu_ntest, dt)}
+               "sample": "N_train=%d, N_test=%d, same sigmas/lambda, one step of %.1f s; the "
+                         "port's cost per entry grows with N (kernels ~N^2 d, factorisation "
+                         "~N^3), so entries/s at N_train=%d is lower still"
+                         % (a.cpu_ntrain, a.cpu_ntest, dt, a.ntrain)}
 
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64",
+            "vs_baseline": None, "dtype": "f64" if a.factor == "fp64" else
+            "f64 (int8 tensor-core emulated trailing updates, double-double refinement)",
             "data": "synthetic seeded molecules (fml_b200/synthetic.py)",
             "config": {"workload": workload_name(a, nsig), "n_train": a.ntrain,
                        "n_test": a.ntest, "sigmas": sigmas, "lambda": a.lam,
+                       "factorisation": factor_name(a),
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (each K is %.1f GB)"
                              % (a.ntrain ** 2 * 8 / 1e9)},
             "solves_per_s": world * nsig / (ms * 1e-3),
-            "mae": mae, "potrf_info": [int(v) for v in info],
-            "relative_residual": resid,
-            "relative_residual_after_1_fp64_refinement": resid_ir,
+            "mae": mae, "potrf_info": [int(v) for v in info], res_key: residuals,
             "clocks": clocks, "e2e": e2e, "gpu_launches": pipe.launches_per_run() * a.steps,
-            "roofline": roofline, "cpu_baseline": cpu,
+            "roofline": roofline, "cpu_baseline": cpu, "extras": extras,
         }))
     if world > 1:
         dist.destroy_process_group()
+
+
+def _guarded(out, name, fn):
+    """Runs one extra measurement; a failure is recorded, not raised."""
+    t0 = time.perf_counter()
+    try:
+        res = fn()
+    except Exception as e:  # noqa: BLE001 - the headline line must still print
+        res = {"error": repr(e)[:400]}
+    res["wall_s"] = time.perf_counter() - t0
+    out[name] = res
+
+
+def headline_extras(a, torch, pipe, b, sigmas, dev, z, r, o, y, pred, ms_head):
+    """Measurements reported beside the headline, outside its timed region."""
+    from fml_b200 import _lib, krr
+
+    out = {}
+    yt = b.energies[a.ntrain:]
+    n_mol = a.ntrain + a.ntest
+    per_step = entries_per_step(a.ntrain, a.ntest, len(sigmas))
+
+    def time_pipe(p, steps=2):
+        p.run(z, r, o, y)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            p.run(z, r, o, y)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def leg(kind, lam, factor, refine):
+        p = krr.KRRPipeline(n_mol, a.ntrain, a.nmax, sigmas, lam, kind, factor=factor,
+                            slices=a.slices, refine=refine)
+        ms = time_pipe(p, 1)
+        pr = p.pred[:, :a.ntest].cpu().numpy()
+        res = p.residual_now()
+        d = {"kind": kind, "lambda": lam, "factor": factor, "refine": refine, "ms_per_step": ms,
+             "entries_per_s": per_step / (ms * 1e-3),
+             "solves_per_s": len(sigmas) / (ms * 1e-3),
+             "info": [int(v) for v in p.info.cpu().numpy()],
+             "mae": {str(s): float(np.abs(pr[k] - yt).mean()) for k, s in enumerate(sigmas)},
+             "relative_residual": {str(s): float(res[k]) for k, s in enumerate(sigmas)}}
+        return d, pr, p
+
+    if a.factor != "fp64":
+        def fp64_path():
+            d, pr, p = leg("gaussian", a.lam, "fp64", 0)
+            del p
+            ms_fp = d["ms_per_step"]
+            d["headline_speedup_vs_fp64_factor_path"] = ms_fp / ms_head
+            d["max_rel_pred_diff_headline_vs_fp64"] = {
+                str(s): float(np.abs(pred[k] - pr[k]).max() / np.abs(pr[k]).max())
+                for k, s in enumerate(sigmas)}
+            d["rel_mae_diff_headline_vs_fp64"] = {
+                str(s): float(abs(np.abs(pred[k] - yt).mean() - np.abs(pr[k] - yt).mean())
+                              / np.abs(pr[k] - yt).mean()) for k, s in enumerate(sigmas)}
+            return d
+        _guarded(out, "plain_fp64_factor_path", fp64_path)
+        torch.cuda.empty_cache()
+
+    nref = refine_steps(a)
+
+    def lap():
+        d, _, p = leg("laplacian", a.lam, a.factor, nref)
+        del p
+        return d
+    _guarded(out, "laplacian_leg", lap)
+    torch.cuda.empty_cache()
+
+    def lam6():
+        d, _, p = leg("gaussian", 1e-6, a.factor, nref)
+        del p
+        return d
+    _guarded(out, "lambda_1e-06_leg", lam6)
+    torch.cuda.empty_cache()
+
+    def mixed():
+        return mixed_kernel_builds(a, torch, pipe, sigmas, dev)
+    _guarded(out, "mixed_precision_kernel_builds", mixed)
+    torch.cuda.empty_cache()
+
+    def batched():
+        return batched_once(a, torch)
+    _guarded(out, "batched_256_problems", batched)
+    torch.cuda.empty_cache()
+
+    def serving():
+        return serving_once(a, torch)
+    _guarded(out, "serving_one_rate", serving)
+    torch.cuda.empty_cache()
+    return out
+
+
+def mixed_kernel_builds(a, torch, pipe, sigmas, dev):
+    """The tcgen05 BF16x3 Gaussian and the FP32 Laplacian builds of the
+    training kernels (all sigmas, symmetric, FP32 out) at N_train, with their
+    max-abs error against the FP64 builds on the leading 8192 x 8192 block.
+    Neither can feed the lambda = 1e-8 factorisation: its entries carry
+    ~1e-4 absolute error, four orders above lambda."""
+    from fml_b200 import _lib
+    lib = _lib.load()
+    P, st = _lib.ptr, _lib.stream_handle()
+    n, L, ns = a.ntrain, pipe.d, len(sigmas)
+    X = pipe.X[:n]
+    sp, keep = _lib.host_doubles(sigmas)
+    peaks = _measured_peaks()
+    K32 = torch.empty((ns, n, n), dtype=torch.float32, device=dev)
+    mu = torch.empty(L, dtype=torch.float64, device=dev)
+    ws = torch.empty(lib.fmlb_tc_operand_bytes(n, L), dtype=torch.uint8, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def tc():
+        _lib.call("fmlb_column_mean_f64", P(X), n, L, L, P(mu), st)
+        _lib.call("fmlb_gaussian_kernel_tc", P(X), n, L, P(X), n, L, L, P(mu), sp, ns, P(K32), n,
+                  n * n, 1, P(ws), ws.numel(), P(status), st)
+    ms_tc = _time(torch, tc, reps=3)
+    nb = min(n, 8192)
+    Kd = torch.empty((ns, nb, nb), dtype=torch.float64, device=dev)
+    _lib.call("fmlb_gaussian_kernel_f64", P(X), nb, L, P(X), nb, L, L, sp, ns, P(Kd), nb, nb * nb,
+              1, st)
+    err_tc = _max_abs_diff(torch, K32[:, :nb, :nb], Kd)
+    ms_l = _time(torch, lambda: _lib.call("fmlb_laplacian_kernel_f32", P(X), n, L, P(X), n, L, L,
+                                          sp, ns, P(K32), n, n * n, 1, st), reps=2)
+    _lib.call("fmlb_laplacian_kernel_f64", P(X), nb, L, P(X), nb, L, L, sp, ns, P(Kd), nb, nb * nb,
+              1, st)
+    err_l = _max_abs_diff(torch, K32[:, :nb, :nb], Kd)
+    del keep
+    wbytes = 4.0 * n * n * ns
+    return {"n": n, "sigmas": sigmas, "error_sample": "leading %d x %d block" % (nb, nb),
+            "gaussian_bf16x3_tcgen05": {
+                "ms": ms_tc, "entries_per_s": n * n * ns / (ms_tc * 1e-3),
+                "hbm_write_gbs": wbytes / ms_tc / 1e6,
+                "hbm_write_frac_of_measured_copy": wbytes / ms_tc / 1e6 / peaks["hbm_gbs"],
+                "max_abs_err_vs_fp64": err_tc, "status": int(status.item())},
+            "laplacian_fp32": {"ms": ms_l, "entries_per_s": n * n * ns / (ms_l * 1e-3),
+                               "max_abs_err_vs_fp64": err_l}}
+
+
+def batched_once(a, torch):
+    """The 256-problem batched workload (default tile configuration, no
+    autotuning): one captured pass replayed twice after a warm-up."""
+    from fml_b200 import autotune
+    from fml_b200.batched import BatchedKRR
+    probs, kinds, ytest, nt = batched_problems(a.nprob)
+    bk = BatchedKRR(probs, split_threshold=autotune.DEFAULT["split_threshold"],
+                    grid=autotune.DEFAULT["grid"])
+    g = bk.capture()
+    g.replay()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(2):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 2
+    info = bk.infos()
+    preds = bk.predictions()
+    mae = [float(np.mean(np.abs(p - yt))) for p, yt in zip(preds, ytest)]
+    ns = np.array([len(p.y) for p in probs])
+    entries = float(np.sum(ns.astype(np.float64) ** 2 + nt * ns))
+    del g
+    return {"problems": a.nprob, "ms_per_pass": ms, "solves_per_s": a.nprob / (ms * 1e-3),
+            "kernel_entries_per_s": entries / (ms * 1e-3),
+            "cholesky_failures": int((info != 0).sum()), "median_mae": float(np.median(mae)),
+            "config": "default split threshold / grid (autotuning off here)"}
+
+
+def serving_once(a, torch):
+    """The serving loop at one offered rate: 16 resident models (8 CM, 8 ARAD)
+    with n_train log-spaced 2000..8192 (the full configuration goes to 32768:
+    bench.py --workload serving), 100 Poisson requests at 200 req/s."""
+    from fml_b200 import synthetic
+    from fml_b200.serving import KRRServer, latency_summary
+    size = 29
+    srv = KRRServer(hbm_budget=150e9, max_inflight=8, max_batch_molecules=1024)
+    specs = serving_models(8192, size)
+    for m, kind, bb, sigma, lam in specs:
+        srv.add_model(m, kind, bb.charges, bb.coords, bb.offsets, bb.energies, sigma, lam,
+                      size=size)
+    srv.reserve()
+    train_sizes = [bb.nmol for _, _, bb, _, _ in specs]
+    pool = synthetic.generate(20000, nmax=size, seed=4000)
+    warm = serving_requests(16, 1e6, pool, 16, 3999, train_sizes, retrain_frac=0.0)
+    for k, q in enumerate(warm):
+        q.model = k
+    srv.serve(warm, realtime=False)
+    reqs = serving_requests(100, 200.0, pool, 16, 4000, train_sizes, retrain_frac=0.02)
+    wall = srv.serve(reqs, realtime=True)
+    preds = [q for q in reqs if not q.retrain]
+    res = latency_summary(reqs)
+    res.update({"offered_req_per_s": 200.0, "requests": len(reqs),
+                "molecules_per_s": sum(q.nmol for q in preds) / wall,
+                "cm": latency_summary([q for q in preds if q.model < 8]),
+                "arad": latency_summary([q for q in preds if q.model >= 8]),
+                "models": "16 (8 CM-Gaussian, 8 ARAD), n_train 2000..8192"})
+    del srv
+    return res
 
 
 # ---------------------------------------------------------------------------
@@ -487,6 +760,8 @@ def run_stages(a):
 
     if a.stages == "arad":
         return run_arad_stage(a, torch, lib, st, P)
+    if a.stages == "factor":
+        return run_factor_stages(a, torch, lib, st, P, emit)
     # --- descriptors ---------------------------------------------------------
     b = synthetic.generate(40960, nmax=29, seed=2)
     z = torch.from_numpy(b.charges).to(dev)
@@ -618,6 +893,80 @@ def run_stages(a):
     del keep
     out += run_arad_stage(a, torch, lib, st, P)
     return out
+
+
+def run_factor_stages(a, torch, lib, st, P, emit):
+    """The factorisations alone at N = --ntrain on the Gaussian kernel of the
+    sorted CMs (sigma = last of --sigmas, lambda = --lam): FP64 and int8
+    (Ozaki) factors, and one bulk trailing update of each kind (m = N - 1024,
+    k = 1024)."""
+    from fml_b200 import _lib, synthetic
+    dev = torch.device("cuda", 0)
+    n = a.ntrain
+    b = synthetic.generate(n, nmax=a.nmax, seed=2)
+    L = a.nmax * (a.nmax + 1) // 2
+    z = torch.from_numpy(b.charges).to(dev)
+    r = torch.from_numpy(b.coords).to(dev)
+    o = torch.from_numpy(b.offsets).to(dev)
+    X = torch.empty((n, L), dtype=torch.float64, device=dev)
+    _lib.call("fmlb_coulomb_matrices", P(z), P(r), P(o), n, a.nmax, P(X), L, None, 0, None, None,
+              st)
+    sig = [float(v) for v in a.sigmas.split(",")][-1]
+    one, keep = _lib.host_doubles([sig])
+    K = torch.empty((n, n), dtype=torch.float64, device=dev)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    dgemm = measure_dgemm_peak(torch)
+    w64 = torch.empty(lib.fmlb_potrf_workspace_bytes(n), dtype=torch.uint8, device=dev)
+    woz = torch.empty(lib.fmlb_potrf_ozaki_workspace_bytes(n, a.slices), dtype=torch.uint8,
+                      device=dev)
+
+    def build():
+        _lib.call("fmlb_gaussian_kernel_f64", P(X), n, L, P(X), n, L, L, one, 1, P(K), n, n * n,
+                  1, st)
+        _lib.call("fmlb_add_diagonal_f64", P(K), n, n, a.lam, st)
+
+    for name in ("fp64", "ozaki"):
+        tms = []
+        for _ in range(3):
+            build()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            if name == "fp64":
+                _lib.call("fmlb_potrf_f64", P(K), n, n, P(w64), P(info), st)
+            else:
+                _lib.call("fmlb_potrf_ozaki_f64", P(K), n, n, a.slices, P(woz), woz.numel(),
+                          P(info), st)
+            e1.record()
+            torch.cuda.synchronize()
+            tms.append(e0.elapsed_time(e1))
+        ms = float(np.median(tms[1:]))
+        fl = n ** 3 / 3.0
+        emit({"stage": "potrf_" + name, "config": "N=%d, sigma=%g, lambda=%g" % (n, sig, a.lam),
+              "ms": ms, "fp64_equivalent_tflops": fl / ms / 1e9, "dgemm_tflops": dgemm,
+              "info": int(info.item())})
+    # one bulk update of each kind: C = K[1024:, 1024:], P = K[1024:, :1024]
+    m, k = n - 1024, 1024
+    Cv, Pv = K[1024:, 1024:], K[1024:, :1024]
+    ws = torch.empty(lib.fmlb_syrk_ozaki_workspace_bytes(m, k, a.slices), dtype=torch.uint8,
+                     device=dev)
+    info.zero_()
+    fl = 2.0 * k * m * (m + 1) / 2
+    ms = _time(torch, lambda: _lib.call("fmlb_syrk_lower_f64", P(Cv), n, m, P(Pv), n, k, 0, None,
+                                        st), reps=3)
+    emit({"stage": "syrk_fp64", "config": "m=%d, k=%d" % (m, k), "ms": ms,
+          "tflops": fl / ms / 1e9, "frac_of_dgemm": fl / ms / 1e9 / dgemm})
+    ms = _time(torch, lambda: _lib.call("fmlb_syrk_lower_ozaki", P(Cv), n, m, P(Pv), n, k, 0,
+                                        a.slices, P(ws), ws.numel(), P(info), st), reps=3)
+    nprod = a.slices * (a.slices + 1) // 2
+    int8 = measure_int8_peak(torch)
+    emit({"stage": "syrk_ozaki", "config": "m=%d, k=%d, %d digit planes (%d int8 products)"
+          % (m, k, a.slices, nprod), "ms": ms, "fp64_equivalent_tflops": fl / ms / 1e9,
+          "int8_tops": fl * nprod / ms / 1e9, "int8_peak_tops_measured": int8,
+          "frac_of_int8_peak": (fl * nprod / ms / 1e9 / int8) if int8 else None,
+          "vs_dgemm": fl / ms / 1e9 / dgemm, "info": int(info.item())})
+    del keep
+    return []
 
 
 def run_arad_stage(a, torch, lib, st, P):

@@ -6,9 +6,11 @@
 // CUDA-core kernel (the L1 distance is not a contraction): 128 x 128 output
 // tile per 256-thread CTA, FP64 descriptors converted to FP32 while staged
 // through shared memory in k-chunks of 32, 8 x 8 outputs per thread (2 FP32
-// instructions per term), every sigma emitted from one pass; symmetric builds
-// compute the tiles on or below the diagonal and write the mirror through a
-// shared-memory transpose.
+// instructions per term; operands fetched as float4), every sigma emitted
+// from one pass. The next k-chunk's global loads are issued into registers
+// before the current chunk is computed, so their latency hides under the
+// arithmetic. Symmetric builds compute the tiles on or below the diagonal and
+// write the mirror through a shared-memory transpose.
 #include <math.h>
 
 #include <algorithm>
@@ -54,25 +56,37 @@ laplacian_f32_kernel(const double *__restrict__ A, int na, int lda, const double
 #pragma unroll
         for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
 
-    // loader: 32 consecutive k of one row per warp, 8 rows per pass
+    // loader: 32 consecutive k of one row per warp, 8 rows per pass; the
+    // chunk is held in registers (converted) until the previous one is done
     const int lk = threadIdx.x & 31, lr = threadIdx.x >> 5;
-    for (int k0 = 0; k0 < d; k0 += LK) {
+    float pa[LB / 8], pb[LB / 8];
+    auto fetch = [&](int k0) {
         const int k = k0 + lk;
-#pragma unroll 4
+#pragma unroll
         for (int r = 0; r < LB / 8; ++r) {
             const int rr = lr + 8 * r;
             const int ra = row0 + rr, rb = col0 + rr;
-            As[lk][rr] = (ra < na && k < d) ? (float)A[(size_t)ra * lda + k] : 0.0f;
-            Bs[lk][rr] = (rb < nb && k < d) ? (float)B[(size_t)rb * ldb + k] : 0.0f;
+            pa[r] = (ra < na && k < d) ? (float)A[(size_t)ra * lda + k] : 0.0f;
+            pb[r] = (rb < nb && k < d) ? (float)B[(size_t)rb * ldb + k] : 0.0f;
+        }
+    };
+    fetch(0);
+    for (int k0 = 0; k0 < d; k0 += LK) {
+#pragma unroll
+        for (int r = 0; r < LB / 8; ++r) {
+            As[lk][lr + 8 * r] = pa[r];
+            Bs[lk][lr + 8 * r] = pb[r];
         }
         __syncthreads();
-#pragma unroll 1
+        if (k0 + LK < d) fetch(k0 + LK);  // in flight during the arithmetic below
+#pragma unroll 2
         for (int kk = 0; kk < LK; ++kk) {
-            float a[8], b[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) a[i] = As[kk][ty + 16 * i];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) b[j] = Bs[kk][tx + 16 * j];
+            const float4 a0 = *reinterpret_cast<const float4 *>(&As[kk][ty * 8]);
+            const float4 a1 = *reinterpret_cast<const float4 *>(&As[kk][ty * 8 + 4]);
+            const float4 b0 = *reinterpret_cast<const float4 *>(&Bs[kk][tx * 8]);
+            const float4 b1 = *reinterpret_cast<const float4 *>(&Bs[kk][tx * 8 + 4]);
+            const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
             for (int i = 0; i < 8; ++i)
 #pragma unroll
@@ -86,7 +100,7 @@ laplacian_f32_kernel(const double *__restrict__ A, int na, int lda, const double
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) T[ty + 16 * i][tx + 16 * j] = acc[i][j];
+        for (int j = 0; j < 8; ++j) T[ty * 8 + i][tx * 8 + j] = acc[i][j];
     __syncthreads();
     const bool mirror = symmetric && by > bx;
     for (int s = 0; s < nsig; ++s) {

@@ -88,12 +88,14 @@ class KRRPipeline:
         else:
             wb = lib.fmlb_potrf_workspace_bytes(n)
         self.work = torch.empty((self.nsig, wb), dtype=torch.uint8, device=self.dev)
+        # the diagonal of K + lambda I is kept for the residual: the factor
+        # overwrites it, K's strict upper triangle stays in place
+        self.diag = torch.empty((self.nsig, n), **f64)
+        self.ytr = torch.empty(n, **f64)
+        self.scratch = None
         if self.refine > 0:
-            self.diag = torch.empty((self.nsig, n), **f64)
             self.alpha_lo = torch.empty((self.nsig, n), **f64)
-            self.ytr = torch.empty(n, **f64)
-            sd = lib.fmlb_krr_refine_dd_scratch_doubles(n)
-            self.scratch = torch.empty((self.nsig, sd), **f64)
+            self._alloc_scratch()
             self.resid = torch.zeros((self.nsig, self.refine + 1), **f64)
         self.info = torch.zeros(self.nsig, dtype=torch.int32, device=self.dev)
         self.alpha = torch.empty((self.nsig, n), **f64)
@@ -114,16 +116,40 @@ class KRRPipeline:
         potrf = potrf_launches(self.n_train, self.factor == "ozaki")
         potrs = 2 * nblk
         per_sigma = 1 + potrf + potrs
-        if self.refine > 0:  # diagonal, then per step 3 residual + 2 norm + potrs + update
-            per_sigma += 1 + self.refine * (5 + potrs + 1) + 5
+        per_sigma += 1  # the kept diagonal
+        if self.refine > 0:  # per step 3 residual + 2 norm + potrs + update, final residual
+            per_sigma += self.refine * (5 + potrs + 1) + 5
         return 1 + 1 + self.nsig * per_sigma + (2 if self.n_test else 0)
 
+    def _alloc_scratch(self):
+        sd = _lib.load().fmlb_krr_refine_dd_scratch_doubles(self.n_train)
+        self.scratch = torch.empty((self.nsig, sd), dtype=torch.float64, device=self.dev)
+
     def relative_residuals(self):
-        """(nsigma, refine + 1) host array of ||r|| / ||y|| (refine > 0 only)."""
+        """(nsigma, refine + 1) host array of ||r|| / ||y|| before each
+        refinement step and after the last (refine > 0 only)."""
         if self.refine == 0:
             raise ValueError("the pipeline keeps residuals only with refine > 0")
         ny = float(torch.linalg.vector_norm(self.ytr))
         return self.resid.cpu().numpy() / ny
+
+    def residual_now(self):
+        """(nsigma,) host array: ||y - (K + lambda I) alpha|| / ||y|| of the
+        current weights, formed in double-double from the factored buffers
+        (K's strict upper triangle and the kept diagonal)."""
+        if self.scratch is None:
+            self._alloc_scratch()
+        n = self.n_train
+        out = torch.empty((self.nsig, 1), dtype=torch.float64, device=self.dev)
+        st = _lib.stream_handle()
+        for k in range(self.nsig):
+            lo = self.alpha_lo[k] if self.refine > 0 else torch.zeros(n, dtype=torch.float64,
+                                                                      device=self.dev)
+            _lib.call("fmlb_krr_refine_dd", _lib.ptr(self.K[k]), n, n, _lib.ptr(self.diag[k]),
+                      _lib.ptr(self.work[k]), _lib.ptr(self.ytr), _lib.ptr(self.alpha[k]),
+                      _lib.ptr(lo), 0, _lib.ptr(out[k]), _lib.ptr(self.scratch[k]), st)
+        ny = float(torch.linalg.vector_norm(self.ytr))
+        return out[:, 0].cpu().numpy() / ny
 
     def run_descriptors(self, X, y_train, stream=None):
         """Like ``run`` with the descriptor rows (n_mol, d) given instead of molecules."""
@@ -145,9 +171,8 @@ class KRRPipeline:
         _lib.call(fn, _lib.ptr(self.X), n, d, _lib.ptr(self.X), n, d, d, self._sig_ptr, self.nsig,
                   _lib.ptr(self.K), n, n * n, 1, s)
         main = stream if stream is not None else torch.cuda.current_stream(self.dev)
-        if self.refine > 0:
-            with torch.cuda.stream(main):
-                self.ytr.copy_(y_train)
+        with torch.cuda.stream(main):
+            self.ytr.copy_(y_train)
         self._fork.record(main)
         for k in range(self.nsig):
             Kk = self.K[k]
@@ -155,8 +180,7 @@ class KRRPipeline:
             sk.wait_event(self._fork)
             h = _lib.stream_handle(sk)
             _lib.call("fmlb_add_diagonal_f64", _lib.ptr(Kk), n, n, self.lam, h)
-            if self.refine > 0:
-                _lib.call("fmlb_get_diagonal_f64", _lib.ptr(Kk), n, n, _lib.ptr(self.diag[k]), h)
+            _lib.call("fmlb_get_diagonal_f64", _lib.ptr(Kk), n, n, _lib.ptr(self.diag[k]), h)
             if self.factor == "ozaki":
                 _lib.call("fmlb_potrf_ozaki_f64", _lib.ptr(Kk), n, n, self.slices,
                           _lib.ptr(self.work[k]), self.work.shape[1],

@@ -434,6 +434,25 @@ def test_gaussian_tc_symmetric_exact(oracle_mod, cm_large):
         assert np.abs(K[k] - ref).max() <= 2e-4
 
 
+def test_gaussian_tc_wait_timeout_reports_and_recovers(oracle_mod, cm_large):
+    """Every mbarrier wait of the tcgen05 kernel is bounded. With the test hook
+    set (waits of 20000 cycles, the TMA producer issues no copies) the MMA and
+    epilogue waits run out with nothing in flight: the call raises FmlbError
+    (FMLB_ETIMEDOUT) and the context stays usable, so the next call matches
+    the oracle."""
+    from fml_b200 import _lib
+    A = cm_large[:300].T
+    try:
+        _lib.call("fmlb_tc_test_hooks", 20000, 1)
+        with pytest.raises(_lib.FmlbError) as err:
+            fml_b200.gaussian_kernel(A, A, [400.0], precision="bf16x3")
+    finally:
+        _lib.call("fmlb_tc_test_hooks", 0, 0)
+    assert err.value.code == _lib.FMLB_ETIMEDOUT
+    K = fml_b200.gaussian_kernel(A, A, [400.0], precision="bf16x3")
+    assert np.abs(K[0] - oracle_mod.gaussian_kernel(A, A, 400.0)).max() <= 2e-4
+
+
 @pytest.mark.parametrize("m,strip", [(300, 128), (100, 128), (257, 64)])
 def test_syrk_lower_strip(m, strip):
     """strip_cols > 0 updates only the first strip_cols columns of the lower triangle."""
