@@ -594,6 +594,83 @@ __device__ __forceinline__ void fast_item_band(FastSmem &sm, int p, int j1, floa
     }
 }
 
+// Two passes per work item: lane = one record of pass p and one of pass
+// p + 1 (the next 32 records in r order), against the record pairs of atom j1
+// of J in the union of the two passes' windows. Each J record pair is loaded
+// once for four neighbour-pair evaluations, and the item set-up is shared by
+// two passes. Terms outside a record's own window are masked to exactly zero,
+// so every lane sums the same non-zero terms in the same order as
+// fast_item_band and the fixed-point sums are unchanged.
+__device__ __forceinline__ void fast_item_band2(FastSmem &sm, int p, int j1, float maxg2s,
+                                                float wd) {
+    const int lane = threadIdx.x & 31;
+    const bool two = p + 1 < sm.npassI;
+    const float4 u0 = sm.recI[p * 32 + lane];
+    const int meta0 = sm.metaI[p * 32 + lane];
+    const float4 u1 = two ? sm.recI[(p + 1) * 32 + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const int meta1 = two ? sm.metaI[(p + 1) * 32 + lane] : 0;
+    const float2 *ptrow0 = sm.pt + ((meta0 >> 16) & 0xff) * FC_PTS;
+    const float2 *ptrow1 = sm.pt + ((meta1 >> 16) & 0xff) * FC_PTS;
+    const float2 nux0 = make_float2(-u0.x, -u0.x), uy0 = make_float2(u0.y, u0.y),
+                 uz0 = make_float2(u0.z, u0.z), uw0 = make_float2(u0.w, u0.w);
+    const float2 nux1 = make_float2(-u1.x, -u1.x), uy1 = make_float2(u1.y, u1.y),
+                 uz1 = make_float2(u1.z, u1.z), uw1 = make_float2(u1.w, u1.w);
+    const int beg = sm.offJ[j1], end = sm.offJ[j1 + 1];
+    const float lo = sm.passLo[p] - wd, hi = sm.passHi[two ? p + 1 : p] + wd;
+    bool below = false, before = false;
+    if (beg + lane < end) {
+        const float4 A = sm.J.p.a[beg + lane];
+        below = !(A.y > lo);
+        before = A.x < hi;
+    }
+    const int mb = beg + __popc(__ballot_sync(0xffffffffu, below));
+    const int me = beg + __popc(__ballot_sync(0xffffffffu, before));
+    float2 acc0 = make_float2(0.0f, 0.0f), acc1 = make_float2(0.0f, 0.0f);
+#pragma unroll 2
+    for (int m = mb; m < me; ++m) {
+        const float4 A = sm.J.p.a[m];
+        const float4 B = sm.J.p.b[m];
+        const int k = sm.J.p.k[m];
+        const float2 st0 = ptrow0[k], st1 = ptrow1[k];
+        const float2 rj = make_float2(A.x, A.y), xj = make_float2(A.z, A.w);
+        const float2 cj = make_float2(B.x, B.y), sj = make_float2(B.z, B.w);
+        {
+            const float2 dr = __fadd2_rn(rj, nux0);
+            const float2 t = __fmul2_rn(dr, dr);
+            float e0, e1;
+            asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e0) : "f"(-t.x));
+            asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e1) : "f"(-t.y));
+            const float2 g = __ffma2_rn(sj, uw0, __ffma2_rn(cj, uz0, __fmul2_rn(xj, uy0)));
+            const float2 win = make_float2(set_lt(t.x, maxg2s), set_lt(t.y, maxg2s));
+            const float2 eg = __fmul2_rn(__fmul2_rn(make_float2(e0, e1), st0), win);
+            acc0 = __ffma2_rn(eg, g, acc0);
+        }
+        {
+            const float2 dr = __fadd2_rn(rj, nux1);
+            const float2 t = __fmul2_rn(dr, dr);
+            float e0, e1;
+            asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e0) : "f"(-t.x));
+            asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e1) : "f"(-t.y));
+            const float2 g = __ffma2_rn(sj, uw1, __ffma2_rn(cj, uz1, __fmul2_rn(xj, uy1)));
+            const float2 win = make_float2(set_lt(t.x, maxg2s), set_lt(t.y, maxg2s));
+            const float2 eg = __fmul2_rn(__fmul2_rn(make_float2(e0, e1), st1), win);
+            acc1 = __ffma2_rn(eg, g, acc1);
+        }
+    }
+    if ((meta0 >> 24) & 1) {
+        const long long f = __float2ll_rn((acc0.x + acc0.y) * 4294967296.0f);
+        if (f)
+            atomicAdd(reinterpret_cast<unsigned long long *>(&sm.S.q[(meta0 & 0xff) * FC_SS + j1]),
+                      (unsigned long long)f);
+    }
+    if ((meta1 >> 24) & 1) {
+        const long long f = __float2ll_rn((acc1.x + acc1.y) * 4294967296.0f);
+        if (f)
+            atomicAdd(reinterpret_cast<unsigned long long *>(&sm.S.q[(meta1 & 0xff) * FC_SS + j1]),
+                      (unsigned long long)f);
+    }
+}
+
 // Work item (pass p, atom j1): the segment sums of the pass against j1 are
 // added into S[i1][j1] by each segment's last lane (an atom split across two
 // passes contributes two partial sums; two terms commute, so the result does
@@ -640,8 +717,9 @@ __device__ __forceinline__ void fast_pair_sums(FastSmem &sm, int nJ, float maxg2
         // skip margin slightly wider than the window: only records whose every
         // term is masked are skipped
         const float wd = sqrtf(maxg2s) * 1.0001f;
-        for (int it = warp; it < items; it += FC_WARPS)
-            fast_item_band(sm, it / nJ, it % nJ, maxg2s, wd);
+        const int items2 = ((sm.npassI + 1) >> 1) * nJ;
+        for (int it = warp; it < items2; it += FC_WARPS)
+            fast_item_band2(sm, 2 * (it / nJ), it % nJ, maxg2s, wd);
     } else {
         for (int it = warp; it < items; it += FC_WARPS) fast_item(sm, it / nJ, it % nJ, maxg2s);
     }
