@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--sigmas", default="100,400,1600")
     p.add_argument("--lam", type=float, default=1e-8)
     p.add_argument("--seed", type=int, default=2)
-    p.add_argument("--factor", default="ozaki", choices=["ozaki", "fp64"],
+    p.add_argument("--factor", default="fp64", choices=["ozaki", "fp64"],
                    help="factorisation of the headline step: 'ozaki' (trailing updates on "
                         "the int8 tensor cores, then double-double refinement) or 'fp64' "
                         "(FP64 tensor cores, no refinement)")
