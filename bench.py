@@ -60,7 +60,7 @@ def parse():
                         "(FP64 tensor cores, no refinement)")
     p.add_argument("--slices", type=int, default=7, help="digit planes of the int8 factor")
     p.add_argument("--refine", type=int, default=None,
-                   help="double-double refinement steps (default 3 with the int8 factor, 0 "
+                   help="double-double refinement steps (default 2 with the int8 factor, 0 "
                         "with the FP64 one)")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the measurements reported beside the headline (FP64-factor "
@@ -103,7 +103,7 @@ def workload_name(a, nsig):
 
 
 def refine_steps(a):
-    return (3 if a.factor == "ozaki" else 0) if a.refine is None else a.refine
+    return (2 if a.factor == "ozaki" else 0) if a.refine is None else a.refine
 
 
 def factor_name(a):

@@ -91,7 +91,7 @@ def cho_solve(A, y, strict=False, refine=None, return_residuals=False, factor="f
     Extensions (the reference solves once with LAPACK):
 
     * ``factor="ozaki"`` factors on the int8 tensor cores (``slices`` digit
-      planes, 1..8) and refines; ``refine`` then defaults to 3 steps and the
+      planes, 1..8) and refines; ``refine`` then defaults to 2 steps and the
       residual to double-double.
     * ``refine`` > 0 adds that many iterative-refinement steps on the device
       (r = y - A x, x += solve(r)); ``residual="fp64"`` (the default for the
@@ -108,7 +108,7 @@ def cho_solve(A, y, strict=False, refine=None, return_residuals=False, factor="f
     if factor not in ("fp64", "ozaki"):
         raise ValueError("factor must be 'fp64' or 'ozaki'")
     if refine is None:
-        refine = 3 if factor == "ozaki" else 0
+        refine = 2 if factor == "ozaki" else 0
     if residual is None:
         residual = "dd" if factor == "ozaki" else "fp64"
     if refine < 0:

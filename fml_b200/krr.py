@@ -56,7 +56,7 @@ class KRRPipeline:
     ``factor="fp64"`` factors on the FP64 tensor cores; ``factor="ozaki"``
     runs the trailing updates on the int8 tensor cores (``slices`` digit
     planes) and is followed by ``refine`` double-double refinement steps
-    (default 3 for it, 0 for the FP64 factor). With ``refine`` > 0 the
+    (default 2 for it, 0 for the FP64 factor). With ``refine`` > 0 the
     relative residual ||y - (K + lambda I) alpha|| / ||y|| before each step
     and after the last is kept per sigma in ``resid`` (device, divided by
     ||y|| by ``relative_residuals``).
@@ -82,7 +82,7 @@ class KRRPipeline:
         if factor not in ("fp64", "ozaki"):
             raise ValueError("factor must be 'fp64' or 'ozaki'")
         self.factor, self.slices = factor, int(slices)
-        self.refine = (3 if factor == "ozaki" else 0) if refine is None else int(refine)
+        self.refine = (2 if factor == "ozaki" else 0) if refine is None else int(refine)
         if factor == "ozaki":
             wb = lib.fmlb_potrf_ozaki_workspace_bytes(n, self.slices)
         else:
