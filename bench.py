@@ -58,7 +58,7 @@ def parse():
                    help="factorisation of the headline step: 'ozaki' (trailing updates on "
                         "the int8 tensor cores, then double-double refinement) or 'fp64' "
                         "(FP64 tensor cores, no refinement)")
-    p.add_argument("--slices", type=int, default=7, help="digit planes of the int8 factor")
+    p.add_argument("--slices", type=int, default=6, help="digit planes of the int8 factor")
     p.add_argument("--refine", type=int, default=None,
                    help="double-double refinement steps (default 2 with the int8 factor, 0 "
                         "with the FP64 one)")

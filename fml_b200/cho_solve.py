@@ -45,12 +45,12 @@ def _upper_as_rowmajor_lower(A):
     return t, True
 
 
-def potrf(Ad, n, factor="fp64", slices=7):
+def potrf(Ad, n, factor="fp64", slices=6):
     """In-place factorisation of a device (n, n) tensor; returns (work, info).
 
     factor="fp64": FP64 tensor-core trailing updates (DMMA);
     factor="ozaki": trailing updates on the int8 tensor cores with ``slices``
-    7-bit digit planes per entry (the Ozaki scheme), to be followed by
+    8-bit digit planes per entry (the Ozaki scheme), to be followed by
     iterative refinement.
     """
     lib = _lib.load()
@@ -85,7 +85,7 @@ def _check_info(info, strict):
 
 
 def cho_solve(A, y, strict=False, refine=None, return_residuals=False, factor="fp64",
-              slices=7, residual=None):
+              slices=6, residual=None):
     """Solve A x = y for symmetric positive-definite A.
 
     Extensions (the reference solves once with LAPACK):

@@ -25,6 +25,7 @@
 #include <cuda_bf16.h>
 #include <math.h>
 #include <stdint.h>
+#include <string.h>
 
 #include <algorithm>
 #include <mutex>
@@ -37,14 +38,17 @@ namespace {
 
 using namespace tc;
 
-constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 64, TC_STAGES = 3, TC_THREADS = 320;
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 64, TC_STAGES = 2, TC_THREADS = 320;
 constexpr int TC_EPI_WARPS = 8;
 constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 2;          // 16 KB per operand tile
 constexpr int TC_STAGE_BYTES = 4 * TC_TILE_BYTES;          // A hi, A lo, B hi, B lo
 constexpr int TC_TMEM_COLS = 2 * TC_BN;
 constexpr int TC_MAXSIG = 8;
 constexpr int TC_PITCH = 33;                               // floats per transposed row
-constexpr int TC_STG_BYTES = TC_EPI_WARPS * 32 * TC_PITCH * 4;
+constexpr int TC_BOX_FLOATS = 32 * 32;                     // one 32 x 32 FP32 store box
+constexpr int TC_WARP_STG = 2 * TC_BOX_FLOATS;             // direct + mirrored box per warp
+static_assert(32 * TC_PITCH <= TC_WARP_STG, "the transposed fallback tile fits the boxes");
+constexpr int TC_STG_BYTES = TC_EPI_WARPS * TC_WARP_STG * 4;
 constexpr size_t kTcSmem =
     (size_t)TC_STAGES * TC_STAGE_BYTES + TC_STG_BYTES + 1024 /* align */ + 256;
 
@@ -61,6 +65,7 @@ struct TcParams {
     long long ldk, sstride;  // output row stride and sigma stride (elements)
     long long budget;        // clock cycles of every mbarrier wait
     int skip_loads;          // test hook: the producer issues no copies
+    int tma_store;           // K is written by TMA bulk-tensor stores (aligned K)
 };
 
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar,
@@ -98,6 +103,26 @@ __device__ __forceinline__ void tile_coords(int t, const TcParams &p, int &ta, i
     }
 }
 
+// 3-D tiled TMA store of a shared-memory box (bulk async-group completion).
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, const void *src, int x, int y,
+                                             int z) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];\n" ::"l"(
+            reinterpret_cast<uint64_t>(map)),
+        "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n"); }
+__device__ __forceinline__ void bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() {
+    asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+
 __device__ __forceinline__ float fast_exp2(float x) {
     float y;
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -107,8 +132,9 @@ __device__ __forceinline__ float fast_exp2(float x) {
 __global__ void __launch_bounds__(TC_THREADS, 1)
 gauss_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
                 const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
-                const float *__restrict__ normA, const float *__restrict__ normB, TcParams p,
-                float *__restrict__ K, int *__restrict__ status) {
+                const __grid_constant__ CUtensorMap mapK, const float *__restrict__ normA,
+                const float *__restrict__ normB, TcParams p, float *__restrict__ K,
+                int *__restrict__ status) {
     extern __shared__ uint8_t tc_smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -229,7 +255,8 @@ gauss_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constan
         // shared-memory transpose (one coalesced row of 32 floats per store).
         const int q = warp & 3;
         const int half = (warp - 2) >> 2;
-        float *stg = stg_all + (warp - 2) * 32 * TC_PITCH;
+        float *stg = stg_all + (warp - 2) * TC_WARP_STG;  // 1024-byte aligned boxes
+        float *dbox = stg, *mbox = stg + TC_BOX_FLOATS;
         int lt = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++lt) {
             int ta, tb;
@@ -265,6 +292,7 @@ gauss_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constan
             fence_before_sync();
             __syncwarp();
             if (lane == 0) mbar_arrive(&tmem_empty[acc]);  // the next-but-one tile may start
+            const bool tma = p.tma_store && !diag_tile;
             for (int s = 0; s < p.nsig; ++s) {
                 const float sc = p.scale[s];
                 float *Ks = K + s * p.sstride;
@@ -274,29 +302,57 @@ gauss_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constan
                     float kv[32];
 #pragma unroll
                     for (int j = 0; j < 32; ++j) kv[j] = fast_exp2(d2[c * 32 + j] * sc);
-                    // mirrored tile K[col][row]: lanes write 32 consecutive rows
-                    if (p.symmetric && row_ok) {
+                    // the boxes are free once the previous stores have read them
+                    if (lane == 0) bulk_wait_read();
+                    __syncwarp();
+                    if (tma) {
+                        // direct box K[row0 + r][cb + j], row r = lane, 128-byte
+                        // swizzle: 16-byte chunk j4 of row r at chunk j4 ^ (r & 7)
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            const int col = cb + j;
-                            if (col < p.nb && (!diag_tile || col < grow))
-                                __stcs(Ks + (size_t)col * p.ldk + grow, kv[j]);
+                        for (int j4 = 0; j4 < 8; ++j4)
+                            *reinterpret_cast<float4 *>(dbox + lane * 32 + ((j4 ^ (lane & 7)) << 2)) =
+                                make_float4(kv[4 * j4], kv[4 * j4 + 1], kv[4 * j4 + 2],
+                                            kv[4 * j4 + 3]);
+                        // mirrored box K[cb + j][row0 + lane]: row j, column lane
+                        if (p.symmetric) {
+#pragma unroll
+                            for (int j = 0; j < 32; ++j)
+                                mbox[j * 32 + (((lane >> 2) ^ (j & 7)) << 2) + (lane & 3)] = kv[j];
                         }
-                    }
-                    // direct tile K[row][col] through the transpose
+                        fence_proxy_async();
+                        __syncwarp();
+                        if (lane == 0) {  // boxes wholly outside K are not issued
+                            if (row0 < p.na && cb < p.nb) tma_store_3d(&mapK, dbox, cb, row0, s);
+                            if (p.symmetric && row0 < p.nb && cb < p.na)
+                                tma_store_3d(&mapK, mbox, row0, cb, s);
+                            bulk_commit();
+                        }
+                    } else {
+                        // mirrored tile K[col][row]: lanes write 32 consecutive rows
+                        if (p.symmetric && row_ok) {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) stg[lane * TC_PITCH + j] = kv[j];
-                    __syncwarp();
-                    const int col = cb + lane;
-                    for (int rr = 0; rr < 32; ++rr) {
-                        const int r = row0 + rr;
-                        if (r < p.na && col < p.nb && (!diag_tile || col <= r))
-                            __stcs(Ks + (size_t)r * p.ldk + col, stg[rr * TC_PITCH + lane]);
+                            for (int j = 0; j < 32; ++j) {
+                                const int col = cb + j;
+                                if (col < p.nb && (!diag_tile || col < grow))
+                                    __stcs(Ks + (size_t)col * p.ldk + grow, kv[j]);
+                            }
+                        }
+                        // direct tile K[row][col] through the transpose
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) stg[lane * TC_PITCH + j] = kv[j];
+                        __syncwarp();
+                        const int col = cb + lane;
+                        for (int rr = 0; rr < 32; ++rr) {
+                            const int r = row0 + rr;
+                            if (r < p.na && col < p.nb && (!diag_tile || col <= r))
+                                __stcs(Ks + (size_t)r * p.ldk + col, stg[rr * TC_PITCH + lane]);
+                        }
+                        __syncwarp();
                     }
-                    __syncwarp();
                 }
             }
         }
+        if (lane == 0) bulk_wait_all();  // every store of this warp is complete
     }
     fence_before_sync();
     __syncthreads();
@@ -460,6 +516,25 @@ extern "C" int fmlb_gaussian_kernel_tc(const double *A, int na, int lda, const d
     const TestHooks hooks = test_hooks();
     p.budget = hooks.wait_budget;
     p.skip_loads = hooks.skip_loads;
+    // K written by TMA stores when its rows and sigma planes start on 16 bytes
+    CUtensorMap mK;
+    memset(&mK, 0, sizeof mK);
+    p.tma_store = ((uintptr_t)K % 16 == 0) && (ldk % 4 == 0) &&
+                  (nsigma == 1 || sigma_stride % 4 == 0) && ldk * 4 < (1LL << 40) &&
+                  (long long)sigma_stride * 4 < (1LL << 40);
+    if (p.tma_store) {
+        EncodeTiledFn fn = encode_tiled_fn();
+        const cuuint64_t gdim[3] = {(cuuint64_t)nb, (cuuint64_t)na, (cuuint64_t)nsigma};
+        const cuuint64_t gstride[2] = {(cuuint64_t)ldk * 4,
+                                       (cuuint64_t)(nsigma > 1 ? sigma_stride : (long long)na * ldk) * 4};
+        const cuuint32_t box[3] = {32, 32, 1};
+        const cuuint32_t estride[3] = {1, 1, 1};
+        if (!fn || fn(&mK, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, K, gdim, gstride, box, estride,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                      CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            p.tma_store = 0;  // the per-element store path needs no map
+    }
     static int attr_dev = -1;
     int dev = 0;
     FMLB_TRY(cuda_status(cudaGetDevice(&dev), "fmlb_gaussian_kernel_tc: cudaGetDevice"));
@@ -474,7 +549,7 @@ extern "C" int fmlb_gaussian_kernel_tc(const double *A, int na, int lda, const d
                                        : (long long)p.ntile_a * p.ntile_b;
     FMLB_REQUIRE(ntiles < (1LL << 31), "fmlb_gaussian_kernel_tc: too many tiles");
     const int grid = (int)std::min<long long>(ntiles, sm_count());
-    gauss_tc_kernel<<<grid, TC_THREADS, kTcSmem, st>>>(mAhi, mAlo, mBhi, mBlo, va.norms, vb.norms,
+    gauss_tc_kernel<<<grid, TC_THREADS, kTcSmem, st>>>(mAhi, mAlo, mBhi, mBlo, mK, va.norms, vb.norms,
                                                        p, K, status);
     return launch_status("gauss_tc_kernel");
 }

@@ -6,18 +6,21 @@
 // integer matrix multiplication unit", IJHPCA 2024), written for tcgen05.
 //
 // Splitting. Each row r of P (k columns) gets the exponent e_r with
-// max_c |P[r, c]| < 2^e_r and s signed 7-bit digits per entry:
-//     P[r, c] = 2^e_r * sum_{t=1..s} d_t[r, c] 2^(-7 t) + O(2^(e_r - 7 s)),
-//     d_t = trunc(128 * remainder) in [-127, 127],
-// all exact in FP64. The product of two rows keeps the digit pairs (t, u) with
-// t + u <= s + 1, grouped by diagonal q = t + u - 1:
-//     (P P^T)[r, c] ~ 2^(e_r + e_c - 7 (s + 1)) * sum_{q=1..s} D_q 128^(s - q),
+// max_c |P[r, c]| < 2^e_r, so x = P[r, c] 2^-(e_r + 1) lies in (-1/2, 1/2),
+// and s base-256 digits by repeated flooring, all exact in FP64:
+//     d_1 = floor(256 x)             in [-128, 127]   (signed 8-bit)
+//     d_t = floor(256 rem_{t-1})     in [0, 255]      (unsigned 8-bit), t > 1
+//     P[r, c] = 2^(e_r + 1) sum_t d_t 256^-t + O(2^(e_r + 1 - 8 s)).
+// The product of two rows keeps the digit pairs (t, u) with t + u <= s + 1,
+// grouped by diagonal q = t + u - 1:
+//     (P P^T)[r, c] ~ 2^(e_r + e_c + 2 - 8 (s + 1)) sum_{q=1..s} D_q 256^(s - q),
 //     D_q = sum_{t + u = q + 1} d_t[r, :] . d_u[c, :]        (exact in int32)
-// s (s + 1) / 2 int8 products in all, every D_q accumulated exactly in its own
-// TMEM accumulator, and combined once, in FP64, by the epilogue (Horner in
-// 128). |d| <= 127 bounds |D_q| by (q + 1) 127^2 k < 2^31 for k <= 16384.
-// The truncation leaves an error of order k 2^(e_r + e_c - 7 s) per entry: at
-// s = 7 about 16x the FP64 rounding bound, at s = 8 below it.
+// s (s + 1) / 2 int8 products in all (each MMA declares which operand is the
+// signed leading digit), every D_q accumulated exactly in its own TMEM
+// accumulator and combined once, in FP64, by the epilogue (Horner in 256).
+// |d_t d_u| <= 255^2 bounds |D_q| by (q + 1) 255^2 k < 2^31 for k <= 4096.
+// The truncation leaves an error of order k 2^(e_r + e_c + 2 - 8 s) per
+// entry: at s = 6 about 16x the FP64 rounding bound, at s = 7 below it.
 //
 // Kernel (persistent, one CTA per SM, 320 threads), output tile 128 x 64:
 //   warp 0      TMA producer: per 32-byte k step, the s digit planes of the
@@ -67,21 +70,25 @@ struct OzParams {
     int strip_tiles;   // column tiles per row block in strip mode
     long long ntiles;
     long long ldc;
-    int exp_bias;      // -7 (ns + 1)
+    int exp_bias;      // 2 - 8 (ns + 1)
     int skip_loads;    // test hook: the producer issues no copies
 };
 
-// Instruction descriptor, kind::i8: signed A and B, int32 accumulator, both
-// K-major, M = 128, N = 64.
-constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) |
-                              ((uint32_t)(OZ_BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+// Instruction descriptor, kind::i8: int32 accumulator, both operands K-major,
+// M = 128, N = 64; A (B) is signed 8-bit when it holds the leading digit
+// plane, unsigned otherwise.
+constexpr uint32_t kIdescI8 =
+    (2u << 4) | ((uint32_t)(OZ_BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+__device__ __forceinline__ uint32_t idesc_i8(int a, int b) {
+    return kIdescI8 | (a == 0 ? (1u << 7) : 0u) | (b == 0 ? (1u << 10) : 0u);
+}
 
 __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                       uint32_t accumulate) {
+                                       uint32_t idesc, uint32_t accumulate) {
     asm volatile(
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
         " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(kIdescI8), "r"(accumulate));
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
 // Tile t -> (row0, col0): lower triangle of 128 x 64 tiles (row block `by`
@@ -203,7 +210,7 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constan
                             const int b = q - a;
                             // plane offsets in 16-byte units of the descriptor address
                             mma_i8(dacc, da + (uint64_t)((a * OZ_A_PLANE) >> 4),
-                                   db + (uint64_t)((b * OZ_B_PLANE) >> 4),
+                                   db + (uint64_t)((b * OZ_B_PLANE) >> 4), idesc_i8(a, b),
                                    (kb > 0 || a > 0) ? 1u : 0u);
                         }
                     }
@@ -240,13 +247,13 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constan
                                   (uint32_t)(q * OZ_BN + half * 32), v);
 #pragma unroll
                 for (int j = 0; j < 32; ++j)
-                    acc[j] = fma(acc[j], 128.0, (double)(int)v[j]);
+                    acc[j] = fma(acc[j], 256.0, (double)(int)v[j]);
             }
             tc::fence_before_sync();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(tmem_empty);  // the next tile's MMAs may start
             ++lt;
-            // scale by 2^(e_r + e_c - 7 (s + 1))
+            // scale by 2^(e_r + e_c + 2 - 8 (s + 1))
             const int grow = row0 + qw * 32 + lane;
             const int er = grow < p.m ? exps[p.p_row0 + grow] : 0;
             const int gcl = col0 + half * 32 + lane;
@@ -323,16 +330,16 @@ ozaki_slice_kernel(const double *__restrict__ P, long long ldp, int m, int k, in
         for (int i = 0; i < 8; ++i) {
             const int c = c0 + i;
             const double v = c < k ? row[c] : 0.0;
-            x[i] = (bad_row || !isfinite(v)) ? 0.0 : ldexp(v, -e);
+            x[i] = (bad_row || !isfinite(v)) ? 0.0 : ldexp(v, -(e + 1));  // in (-1/2, 1/2)
         }
         for (int t = 0; t < ns; ++t) {
             uint64_t word = 0;
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                x[i] *= 128.0;
-                const double d = trunc(x[i]);
+                x[i] *= 256.0;
+                const double d = floor(x[i]);  // [-128, 127] first, then [0, 255]
                 x[i] -= d;
-                word |= (uint64_t)(uint8_t)(int8_t)(int)d << (8 * i);
+                word |= (uint64_t)((uint32_t)(int)d & 0xffu) << (8 * i);
             }
             *reinterpret_cast<uint64_t *>(planes + t * pstride + (size_t)r * ldpl + c0) = word;
         }
@@ -391,7 +398,7 @@ int ozaki_syrk(double *C, long long ldc, int m, const OzakiSlices &s, int p_row0
                int *info, cudaStream_t st) {
     if (m <= 0) return FMLB_OK;
     FMLB_REQUIRE(s.ns >= 1 && s.ns <= OZAKI_MAX_SLICES, "ozaki: 1..%d slices", OZAKI_MAX_SLICES);
-    FMLB_REQUIRE(s.kp % OZ_KB == 0 && s.kp <= 16384, "ozaki: k must be a multiple of 32, <= 16384");
+    FMLB_REQUIRE(s.kp % OZ_KB == 0 && s.kp <= 4096, "ozaki: k must be a multiple of 32, <= 4096");
     FMLB_REQUIRE(p_row0 >= 0 && p_row0 + m <= s.rows, "ozaki: rows outside the slice buffer");
     CUtensorMap mA, mB;
     FMLB_TRY(make_plane_map(&mA, s.planes, s.rows, s.ldpl, s.kp, s.pstride, s.ns, OZ_BM));
@@ -406,7 +413,7 @@ int ozaki_syrk(double *C, long long ldc, int m, const OzakiSlices &s, int p_row0
     p.strip_tiles = p.strip_cols > 0 ? ceil_div(p.strip_cols, OZ_BN) : 0;
     p.ntiles = p.strip_tiles ? Tr * p.strip_tiles : Tr * Tr + Tr;
     p.ldc = ldc;
-    p.exp_bias = -7 * (s.ns + 1);
+    p.exp_bias = 2 - 8 * (s.ns + 1);
     const tc::TestHooks hooks = tc::test_hooks();
     p.skip_loads = hooks.skip_loads;
     const size_t smem = oz_smem_bytes(s.ns);
@@ -459,7 +466,7 @@ extern "C" int fmlb_syrk_lower_ozaki(double *C, long long ldc, int m, const doub
                  "fmlb_syrk_lower_ozaki: bad sizes");
     FMLB_REQUIRE(nslices >= 1 && nslices <= OZAKI_MAX_SLICES,
                  "fmlb_syrk_lower_ozaki: nslices must be 1..%d", OZAKI_MAX_SLICES);
-    FMLB_REQUIRE(k <= 16384, "fmlb_syrk_lower_ozaki: k=%d above 16384", k);
+    FMLB_REQUIRE(k <= 4096, "fmlb_syrk_lower_ozaki: k=%d above 4096", k);
     if (m == 0 || k == 0) return FMLB_OK;
     FMLB_REQUIRE(C && P && info, "fmlb_syrk_lower_ozaki: null pointer");
     const size_t need = fmlb_syrk_ozaki_workspace_bytes(m, k, nslices);

@@ -63,7 +63,7 @@ class KRRPipeline:
     """
 
     def __init__(self, n_mol, n_train, size, sigmas, lam, kind="gaussian", factor="fp64",
-                 slices=7, refine=None):
+                 slices=6, refine=None):
         lib = _lib.load()
         self.dev = device()
         self.n_mol, self.n_train, self.n_test = n_mol, n_train, n_mol - n_train
@@ -212,7 +212,7 @@ class KRRPipeline:
 
 
 def krr_fit_predict(charges, coords, offsets, y_train, n_train, sigmas, lam, size=23,
-                    kind="gaussian", return_info=False, factor="fp64", slices=7, refine=None):
+                    kind="gaussian", return_info=False, factor="fp64", slices=6, refine=None):
     """Train on the first ``n_train`` molecules, predict the rest, for every sigma.
 
     Molecules are packed (charges, coords, offsets). Returns (nsigma, n_test)

@@ -58,10 +58,11 @@ def _blocked_cholesky(A, W, nslices):
 
 @pytest.mark.parametrize("sigma", [100.0, 1600.0])
 def test_ozaki_slices_needed_for_fp64_refined_accuracy(oracle_mod, cm_kernel_inputs, sigma):
-    """Why fmlb_potrf_ozaki_f64 defaults to 7 digit planes: on these kernels
-    at lambda = 1e-8 a factor from 7 planes, refined three times with FP64
-    residuals, reaches the residual of the FP64 factor refined the same way,
-    while 4 planes leave it orders of magnitude above (or break down)."""
+    """Why fmlb_potrf_ozaki_f64 defaults to 6 digit planes (8 bits each): on
+    these kernels at lambda = 1e-8 a factor from 6 planes, refined three times
+    with FP64 residuals, reaches the residual of the FP64 factor refined the
+    same way, while 4 planes leave it orders of magnitude above (or break
+    down)."""
     import scipy.linalg as sla
     X = cm_kernel_inputs
     A = oracle_mod.gaussian_kernel(X.T, X.T, sigma) + 1e-8 * np.eye(len(X))
@@ -76,8 +77,8 @@ def test_ozaki_slices_needed_for_fp64_refined_accuracy(oracle_mod, cm_kernel_inp
         return np.linalg.norm(y - A @ x) / np.linalg.norm(y)
 
     r64 = refined_residual(_blocked_cholesky(A, 256, 0))
-    L7 = _blocked_cholesky(A, 256, 7)
-    assert L7 is not None
-    assert refined_residual(L7) <= 4 * r64
+    L6 = _blocked_cholesky(A, 256, 6)
+    assert L6 is not None
+    assert refined_residual(L6) <= 4 * r64
     L4 = _blocked_cholesky(A, 256, 4)
     assert L4 is None or refined_residual(L4) > 100 * r64

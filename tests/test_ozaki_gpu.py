@@ -3,7 +3,7 @@ factorisation built on it, through the C ABI.
 
 * fmlb_syrk_lower_ozaki against a numpy statement of the same arithmetic
   (tests/ozaki_emulation.py): bit-exact; against the exact FP64 product:
-  within the scheme's bound k (s + 3) 2^(e_r + e_c - 7 s) per entry.
+  within the scheme's bound k (s + 3) 2^(e_r + e_c + 2 - 8 s) per entry.
 * fmlb_potrf_ozaki_f64 + double-double refinement against LAPACK
   (fcho_solve.f90:35-42 calls dpotrf/dpotrs) at n = 16500, which crosses the
   1024-wide outer panels, kappa ~ 1e11: refined relative residual below
@@ -51,8 +51,8 @@ def _panel(rng, m, k):
     return P
 
 
-@pytest.mark.parametrize("m,k,s,strip", [(700, 1024, 7, 0), (300, 256, 8, 0), (517, 96, 3, 0),
-                                         (1000, 512, 6, 256), (5, 64, 1, 0), (130, 1024, 7, 0),
+@pytest.mark.parametrize("m,k,s,strip", [(700, 1024, 6, 0), (300, 256, 8, 0), (517, 96, 3, 0),
+                                         (1000, 512, 7, 256), (5, 64, 1, 0), (130, 4096, 6, 0),
                                          (1, 32, 8, 0)])
 def test_syrk_ozaki_bit_exact_vs_emulation(m, k, s, strip):
     rng = np.random.default_rng(m + k + s)
@@ -67,7 +67,8 @@ def test_syrk_ozaki_bit_exact_vs_emulation(m, k, s, strip):
     if strip:
         mask[:, strip:] = False
     err = np.abs(out - exact)[mask]
-    bound = (emu.error_bound(P, s) + 1e-15 * np.abs(P) @ np.abs(P).T + 1e-15 * np.abs(C))[mask]
+    # plus the FP64 rounding of the combination and of numpy's own product
+    bound = (emu.error_bound(P, s) + 1e-14 * np.abs(P) @ np.abs(P).T + 1e-15 * np.abs(C))[mask]
     assert (err <= bound).all()
     np.testing.assert_array_equal(out[~mask], C[~mask])  # untouched outside the update
 
@@ -113,7 +114,7 @@ def cm_gaussian_16500():
     return K, b.energies
 
 
-@pytest.mark.parametrize("slices", [7, 8])
+@pytest.mark.parametrize("slices", [6, 7])
 def test_potrf_ozaki_refined_solve_vs_lapack(cm_gaussian_16500, slices):
     A, y = cm_gaussian_16500
     x, res = fml_b200.cho_solve(A, y, factor="ozaki", slices=slices, refine=4,

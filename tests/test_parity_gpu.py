@@ -411,7 +411,8 @@ def cm_large(oracle_mod):
     return oracle_mod.coulomb_matrices(b.charges, b.coords, b.offsets, 29)
 
 
-@pytest.mark.parametrize("na,nb", [(300, 300), (130, 257), (1, 129), (600, 1)])
+@pytest.mark.parametrize("na,nb", [(300, 300), (130, 257), (1, 129), (600, 1), (333, 64),
+                                   (129, 516)])
 def test_gaussian_tc_vs_fp64(oracle_mod, cm_large, na, nb):
     A = cm_large[:na].T
     B = cm_large[-nb:].T
@@ -423,8 +424,11 @@ def test_gaussian_tc_vs_fp64(oracle_mod, cm_large, na, nb):
         assert np.abs(K[k] - ref).max() <= 2e-4, (s, np.abs(K[k] - ref).max())
 
 
-def test_gaussian_tc_symmetric_exact(oracle_mod, cm_large):
-    A = cm_large[:517].T
+@pytest.mark.parametrize("n", [517, 300, 640])
+def test_gaussian_tc_symmetric_exact(oracle_mod, cm_large, n):
+    """n = 517: per-element stores (rows not 16-byte aligned); 300 and 640:
+    TMA bulk-tensor stores of the off-diagonal tiles, partial and whole."""
+    A = cm_large[:n].T
     sig = [100.0, 1600.0]
     K = fml_b200.gaussian_kernel(A, A, sig, precision="bf16x3")
     for k, s in enumerate(sig):
