@@ -11,10 +11,12 @@ namespace fmlb {
 constexpr int OZAKI_MAX_SLICES = 8;
 
 // Digit planes of a panel: ns planes of rows x kp int8 (row stride ldpl,
-// plane stride pstride bytes) and one exponent per row.
+// plane stride pstride bytes), one exponent and one zero-point digit sum per
+// row.
 struct OzakiSlices {
     int8_t *planes = nullptr;
     int *exps = nullptr;
+    double *rsum = nullptr;
     int rows = 0, kp = 0, ns = 0;
     long long ldpl = 0, pstride = 0;
 };

@@ -8,26 +8,37 @@
 // Splitting. Each row r of P (k columns) gets the exponent e_r with
 // max_c |P[r, c]| < 2^e_r, so x = P[r, c] 2^-(e_r + 1) lies in (-1/2, 1/2),
 // and s base-256 digits by repeated flooring, all exact in FP64:
-//     d_1 = floor(256 x)             in [-128, 127]   (signed 8-bit)
-//     d_t = floor(256 rem_{t-1})     in [0, 255]      (unsigned 8-bit), t > 1
-//     P[r, c] = 2^(e_r + 1) sum_t d_t 256^-t + O(2^(e_r + 1 - 8 s)).
-// The product of two rows keeps the digit pairs (t, u) with t + u <= s + 1,
+//     d_1 = floor(256 x) in [-128, 127];  u_t = floor(256 rem_{t-1}) in [0, 255]
+// stored as signed bytes with a zero point: v_t = u_t - 128 in [-128, 127], so
+//     x = xt + c + rho,   xt = d_1 / 256 + sum_{t>1} v_t 256^-t,
+//     c = 128 sum_{t=2..s} 256^-t,   0 <= rho < 256^-s.
+// With c' = c + 256^-s / 2 the error x - (xt + c') is zero-mean, and so are
+// the dropped digit products below (v_t is centred), which keeps the errors
+// of the k-term sums from adding up coherently. Then, summing over k,
+//     x_r . x_c ~ xt_r . xt_c + c' (S_r + S_c) + k c'^2,   S_r = sum_k xt_r,k,
+// and the product of two rows keeps the digit pairs (t, u) with t + u <= s + 1,
 // grouped by diagonal q = t + u - 1:
-//     (P P^T)[r, c] ~ 2^(e_r + e_c + 2 - 8 (s + 1)) sum_{q=1..s} D_q 256^(s - q),
-//     D_q = sum_{t + u = q + 1} d_t[r, :] . d_u[c, :]        (exact in int32)
-// s (s + 1) / 2 int8 products in all (each MMA declares which operand is the
-// signed leading digit), every D_q accumulated exactly in its own TMEM
-// accumulator and combined once, in FP64, by the epilogue (Horner in 256).
-// |d_t d_u| <= 255^2 bounds |D_q| by (q + 1) 255^2 k < 2^31 for k <= 4096.
-// The truncation leaves an error of order k 2^(e_r + e_c + 2 - 8 s) per
-// entry: at s = 6 about 16x the FP64 rounding bound, at s = 7 below it.
+//     xt_r . xt_c ~ 256^-(s + 1) sum_{q=1..s} D_q 256^(s - q),
+//     D_q = sum_{t + u = q + 1} dig_t[r, :] . dig_u[c, :]       (exact in int32)
+// s (s + 1) / 2 signed int8 products in all, every D_q accumulated exactly in
+// its own TMEM accumulator and combined once, in FP64, by the epilogue
+// (Horner in 256), which adds the zero-point terms and scales by
+// 2^(e_r + e_c + 2). |dig| <= 128 bounds |D_q| by (q + 1) 2^14 k < 2^31 for
+// k <= 8192. Six planes carry the accuracy of seven truncated 7-bit ones
+// (21 products instead of 28); the error of one entry stays below
+// k (s + 3) 2^(e_r + e_c + 2 - 8 s).
 //
 // Kernel (persistent, one CTA per SM, 320 threads), output tile 128 x 64:
 //   warp 0      TMA producer: per 32-byte k step, the s digit planes of the
 //               128 A rows and 64 B rows (one 3-D box each, 32-byte swizzle)
-//               into a 4-stage ring;
+//               into a ring as deep as shared memory allows (5 stages at
+//               s = 6, at most 8);
 //   warp 1      allocates 512 TMEM columns (s <= 8 accumulators of 64 int32
-//               columns) and issues tcgen05.mma kind::i8 (M 128, N 64, K 32);
+//               columns) and issues tcgen05.mma kind::i8 (M 128, N 64, K 32).
+//               For s <= 6 it first copies the k step's A planes into TMEM
+//               (tcgen05.cp, two buffers after the accumulators), so each of
+//               the s (s + 1) / 2 products reads only its B plane from shared
+//               memory: shared-memory operand traffic halves;
 //   warps 2..9  epilogue, two warps per TMEM lane quarter (32 columns each):
 //               drain the s accumulators into FP64 (Horner), release TMEM to
 //               the next tile's MMAs, scale by the row and column exponents,
@@ -49,7 +60,7 @@ namespace {
 
 constexpr int OZ_BM = 128, OZ_BN = 64;
 constexpr int OZ_KB = 32;          // int8 k values (bytes) per stage: one MMA K step
-constexpr int OZ_STAGES = 4;
+constexpr int OZ_MAX_STAGES = 8;  // the ring depth is set per launch from shared memory
 constexpr int OZ_THREADS = 320;    // 10 warps
 constexpr int OZ_EPI_WARPS = 8;
 constexpr int OZ_TMEM_COLS = 512;
@@ -60,6 +71,11 @@ constexpr int OZ_STAGE_STG = OZ_EPI_WARPS * 16 * OZ_PITCH * (int)sizeof(double);
 constexpr int OZ_NONFINITE = 0x7fffffff;    // exponent marking a row with Inf / NaN
 
 constexpr long long kOzDefaultBudget = 4000000000LL;  // clock cycles (~2 s)
+constexpr int OZ_SMEM_LIMIT = 232448 - 64;  // opt-in shared memory per CTA, less static
+constexpr int OZ_BAR_BYTES = (2 * OZ_MAX_STAGES + 3) * 8 + 8;
+constexpr int OZ_A_TMEM_MAX = 6;            // planes that fit A in TMEM twice beside D
+constexpr int OZ_A_TMEM_COL = OZ_A_TMEM_MAX * OZ_BN;  // 384: A buffers after 6 accumulators
+static_assert(OZ_A_TMEM_COL + 2 * OZ_A_TMEM_MAX * 8 <= OZ_TMEM_COLS, "A buffers fit TMEM");
 
 struct OzParams {
     int m;             // rows (= columns) of C
@@ -70,18 +86,19 @@ struct OzParams {
     int strip_tiles;   // column tiles per row block in strip mode
     long long ntiles;
     long long ldc;
-    int exp_bias;      // 2 - 8 (ns + 1)
+    int exp_bias;      // -8 (ns + 1)
+    double zp_c;       // c' (zero point of the digit planes)
+    double zp_kc2;     // kp c'^2
     int skip_loads;    // test hook: the producer issues no copies
+    int stages;        // depth of the operand ring
+    int a_tmem;        // A planes copied to TMEM once per k step (ns <= 6)
 };
 
-// Instruction descriptor, kind::i8: int32 accumulator, both operands K-major,
-// M = 128, N = 64; A (B) is signed 8-bit when it holds the leading digit
-// plane, unsigned otherwise.
-constexpr uint32_t kIdescI8 =
-    (2u << 4) | ((uint32_t)(OZ_BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
-__device__ __forceinline__ uint32_t idesc_i8(int a, int b) {
-    return kIdescI8 | (a == 0 ? (1u << 7) : 0u) | (b == 0 ? (1u << 10) : 0u);
-}
+// Instruction descriptor, kind::i8: signed A and B, int32 accumulator, both
+// K-major, M = 128, N = 64.
+constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) |
+                              ((uint32_t)(OZ_BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+__device__ __forceinline__ uint32_t idesc_i8(int, int) { return kIdescI8; }
 
 __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
                                        uint32_t idesc, uint32_t accumulate) {
@@ -89,6 +106,22 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
         " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+// The same MMA with A (128 rows x 32 bytes) read from TMEM columns at a_tmem.
+__device__ __forceinline__ void mma_i8_ta(uint32_t tmem_d, uint32_t a_tmem, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+// Copies a 128-row x 32-byte shared-memory tile (matrix descriptor sdesc) into
+// the 8 TMEM columns at taddr, row i to lane i; ordered before the MMAs this
+// thread issues after it.
+__device__ __forceinline__ void tmem_cp_128x256b(uint32_t taddr, uint64_t sdesc) {
+    asm volatile("tcgen05.cp.cta_group::1.128x256b [%0], %1;\n" ::"r"(taddr), "l"(sdesc));
 }
 
 // Tile t -> (row0, col0): lower triangle of 128 x 64 tiles (row block `by`
@@ -115,16 +148,18 @@ __device__ __forceinline__ void oz_fail(int *info) { atomicCAS(info, 0, FMLB_ETI
 
 __global__ void __launch_bounds__(OZ_THREADS, 1)
 ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
-                  const int *__restrict__ exps, OzParams p, double *__restrict__ C,
+                  const int *__restrict__ exps, const double *__restrict__ rsum, OzParams p,
+                  double *__restrict__ C,
                   int *__restrict__ info, long long budget) {
     extern __shared__ uint8_t oz_smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~(uintptr_t)1023);
     const int stage_bytes = p.ns * (OZ_A_PLANE + OZ_B_PLANE);
-    double *stg_all = reinterpret_cast<double *>(smem + OZ_STAGES * stage_bytes);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + OZ_STAGES * stage_bytes + OZ_STAGE_STG);
-    uint64_t *full = bars, *empty = bars + OZ_STAGES;
-    uint64_t *tmem_full = bars + 2 * OZ_STAGES, *tmem_empty = tmem_full + 1,
+    const int nst = p.stages;
+    double *stg_all = reinterpret_cast<double *>(smem + nst * stage_bytes);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + nst * stage_bytes + OZ_STAGE_STG);
+    uint64_t *full = bars, *empty = bars + OZ_MAX_STAGES;
+    uint64_t *tmem_full = bars + 2 * OZ_MAX_STAGES, *tmem_empty = tmem_full + 1,
              *mma_done = tmem_full + 2;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mma_done + 1);
     __shared__ int abort_cta;
@@ -132,7 +167,7 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constan
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
         abort_cta = *(volatile const int *)info != 0;
-        for (int s = 0; s < OZ_STAGES; ++s) {
+        for (int s = 0; s < nst; ++s) {
             tc::mbar_init(&full[s], 1);
             tc::mbar_init(&empty[s], 1);
         }
@@ -158,8 +193,8 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constan
                 int row0, col0;
                 if (!oz_tile(t, p, row0, col0)) continue;
                 for (int kb = 0; kb < p.nkb && !p.skip_loads; ++kb, ++issued) {
-                    const int st = (int)(issued % OZ_STAGES);
-                    const uint32_t ph = (uint32_t)((issued / OZ_STAGES) & 1);
+                    const int st = (int)(issued % nst);
+                    const uint32_t ph = (uint32_t)((issued / nst) & 1);
                     if (!tc::mbar_wait(&empty[st], ph ^ 1, budget)) {
                         oz_fail(info);
                         ok = false;
@@ -173,8 +208,8 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constan
                 }
             }
             // every copy this thread issued has landed before the CTA winds down
-            for (long long l = std::max(0LL, issued - OZ_STAGES); l < issued; ++l)
-                if (!tc::mbar_wait(&full[l % OZ_STAGES], (uint32_t)((l / OZ_STAGES) & 1), budget))
+            for (long long l = std::max(0LL, issued - (long long)nst); l < issued; ++l)
+                if (!tc::mbar_wait(&full[l % nst], (uint32_t)((l / nst) & 1), budget))
                     oz_fail(info);
         }
     } else if (warp == 1) {
@@ -192,8 +227,8 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constan
                 }
                 tc::fence_after_sync();
                 for (int kb = 0; kb < p.nkb; ++kb, ++consumed) {
-                    const int st = (int)(consumed % OZ_STAGES);
-                    const uint32_t ph = (uint32_t)((consumed / OZ_STAGES) & 1);
+                    const int st = (int)(consumed % nst);
+                    const uint32_t ph = (uint32_t)((consumed / nst) & 1);
                     if (!tc::mbar_wait(&full[st], ph, budget)) {
                         oz_fail(info);
                         ok = false;
@@ -204,6 +239,26 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constan
                     const uint8_t *sb = sa + p.ns * OZ_A_PLANE;
                     const uint64_t da = tc::smem_desc_kmajor(sa, OZ_KB);
                     const uint64_t db = tc::smem_desc_kmajor(sb, OZ_KB);
+                    if (p.a_tmem) {
+                        // A planes to TMEM once (double-buffered by k step), then every
+                        // product reads A there and only B from shared memory
+                        const uint32_t abuf = tmem_base + (uint32_t)(OZ_A_TMEM_COL +
+                                                                     (consumed & 1) * p.ns * 8);
+                        for (int a = 0; a < p.ns; ++a)
+                            tmem_cp_128x256b(abuf + (uint32_t)(a * 8),
+                                             da + (uint64_t)((a * OZ_A_PLANE) >> 4));
+                        for (int q = 0; q < p.ns; ++q) {
+                            const uint32_t dacc = tmem_base + (uint32_t)(q * OZ_BN);
+                            for (int a = 0; a <= q; ++a) {
+                                const int b = q - a;
+                                mma_i8_ta(dacc, abuf + (uint32_t)(a * 8),
+                                          db + (uint64_t)((b * OZ_B_PLANE) >> 4), idesc_i8(a, b),
+                                          (kb > 0 || a > 0) ? 1u : 0u);
+                            }
+                        }
+                        tc::mma_commit(&empty[st]);
+                        continue;
+                    }
                     for (int q = 0; q < p.ns; ++q) {
                         const uint32_t dacc = tmem_base + (uint32_t)(q * OZ_BN);
                         for (int a = 0; a <= q; ++a) {
@@ -253,17 +308,25 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constan
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(tmem_empty);  // the next tile's MMAs may start
             ++lt;
-            // scale by 2^(e_r + e_c + 2 - 8 (s + 1))
+            // (acc 256^-(s+1) + c' (S_r + S_c) + k c'^2) 2^(e_r + e_c + 2), the
+            // operations in a fixed order with no contraction
             const int grow = row0 + qw * 32 + lane;
             const int er = grow < p.m ? exps[p.p_row0 + grow] : 0;
+            const double sr = grow < p.m ? rsum[p.p_row0 + grow] : 0.0;
             const int gcl = col0 + half * 32 + lane;
             const int ecl = gcl < p.m ? exps[p.p_row0 + gcl] : 0;
+            const double scl = gcl < p.m ? rsum[p.p_row0 + gcl] : 0.0;
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
                 const int ec = __shfl_sync(0xffffffffu, ecl, j);
+                const double sc = __shfl_sync(0xffffffffu, scl, j);
+                const double core =
+                    __dadd_rn(__dadd_rn(ldexp(acc[j], p.exp_bias),
+                                        __dmul_rn(p.zp_c, __dadd_rn(sr, sc))),
+                              p.zp_kc2);
                 acc[j] = (er == OZ_NONFINITE || ec == OZ_NONFINITE)
                              ? __longlong_as_double(0x7ff8000000000000LL)
-                             : ldexp(acc[j], er + ec + p.exp_bias);
+                             : ldexp(core, er + ec + 2);
             }
             // transpose through shared memory, 16 rows at a time, then a
             // coalesced read-modify-write of the rows' lower-triangle part
@@ -292,15 +355,19 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constan
 
 // ---- splitting --------------------------------------------------------------
 // One CTA (128 threads) per row of P (rows [0, m), k columns, stride ldp):
-// exps[r] and ns digit planes (row-major, kp >= k columns zero-padded, plane
-// stride pstride bytes). Each thread owns 8 consecutive columns per sweep.
+// exps[r], ns digit planes (row-major, kp >= k columns zero-padded, plane
+// stride pstride bytes) and the row sum rsum[r] = S_r of the zero-point
+// digits (per-plane integer sums, combined in FP64 in plane order). Each
+// thread owns 8 consecutive columns per sweep.
 constexpr int SL_TPB = 128;
 
 __global__ void __launch_bounds__(SL_TPB)
 ozaki_slice_kernel(const double *__restrict__ P, long long ldp, int m, int k, int kp, int ns,
                    int8_t *__restrict__ planes, long long pstride, long long ldpl,
-                   int *__restrict__ exps, const int *__restrict__ info) {
+                   int *__restrict__ exps, double *__restrict__ rsum,
+                   const int *__restrict__ info) {
     __shared__ double red[SL_TPB / 32];
+    __shared__ int tsum[OZAKI_MAX_SLICES][SL_TPB / 32];
     __shared__ int bad_row, abort_cta;
     const int r = blockIdx.x, tid = threadIdx.x;
     if (tid == 0) {
@@ -324,6 +391,9 @@ ozaki_slice_kernel(const double *__restrict__ P, long long ldp, int m, int k, in
     int e = 0;
     if (mx > 0.0) frexp(mx, &e);  // mx = f 2^e, f in [0.5, 1): |P[r, :]| < 2^e
     if (tid == 0) exps[r] = bad_row ? OZ_NONFINITE : e;
+    int psum[OZAKI_MAX_SLICES];
+#pragma unroll
+    for (int t = 0; t < OZAKI_MAX_SLICES; ++t) psum[t] = 0;
     for (int c0 = tid * 8; c0 < kp; c0 += SL_TPB * 8) {
         double x[8];
 #pragma unroll
@@ -332,17 +402,37 @@ ozaki_slice_kernel(const double *__restrict__ P, long long ldp, int m, int k, in
             const double v = c < k ? row[c] : 0.0;
             x[i] = (bad_row || !isfinite(v)) ? 0.0 : ldexp(v, -(e + 1));  // in (-1/2, 1/2)
         }
-        for (int t = 0; t < ns; ++t) {
+#pragma unroll
+        for (int t = 0; t < OZAKI_MAX_SLICES; ++t) {
+            if (t >= ns) break;
             uint64_t word = 0;
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
                 x[i] *= 256.0;
-                const double d = floor(x[i]);  // [-128, 127] first, then [0, 255]
+                const double d = floor(x[i]);       // [-128, 127] first, then [0, 255]
                 x[i] -= d;
-                word |= (uint64_t)((uint32_t)(int)d & 0xffu) << (8 * i);
+                const int v = (int)d - (t ? 128 : 0);  // zero point of the lower planes
+                psum[t] += v;
+                word |= (uint64_t)((uint32_t)v & 0xffu) << (8 * i);
             }
             *reinterpret_cast<uint64_t *>(planes + t * pstride + (size_t)r * ldpl + c0) = word;
         }
+    }
+#pragma unroll
+    for (int t = 0; t < OZAKI_MAX_SLICES; ++t) {
+        int v = psum[t];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((tid & 31) == 0) tsum[t][tid >> 5] = v;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double sr = 0.0;
+        for (int t = 0; t < ns; ++t) {
+            const int tt = tsum[t][0] + tsum[t][1] + tsum[t][2] + tsum[t][3];
+            sr = __dadd_rn(sr, ldexp((double)tt, -8 * (t + 1)));
+        }
+        rsum[r] = sr;
     }
 }
 
@@ -370,8 +460,16 @@ int make_plane_map(CUtensorMap *map, const int8_t *base, int rows, long long ldp
     return FMLB_OK;
 }
 
+// Deepest operand ring (<= OZ_MAX_STAGES) whose shared memory fits a CTA.
+int oz_stages(int ns) {
+    const int sb = ns * (OZ_A_PLANE + OZ_B_PLANE);
+    const int room = OZ_SMEM_LIMIT - OZ_STAGE_STG - OZ_BAR_BYTES - 1024;
+    return std::max(2, std::min(OZ_MAX_STAGES, room / sb));
+}
+
 size_t oz_smem_bytes(int ns) {
-    return (size_t)OZ_STAGES * ns * (OZ_A_PLANE + OZ_B_PLANE) + OZ_STAGE_STG + 128 + 1024;
+    return (size_t)oz_stages(ns) * ns * (OZ_A_PLANE + OZ_B_PLANE) + OZ_STAGE_STG + OZ_BAR_BYTES +
+           1024;
 }
 
 thread_local tc::TestHooks t_hooks = {0, 0};
@@ -390,7 +488,7 @@ int ozaki_split(const double *P, long long ldp, int m, int k, const OzakiSlices 
     FMLB_REQUIRE(m <= s.rows && k <= s.kp, "ozaki: panel %d x %d exceeds the slice buffer %d x %d",
                  m, k, s.rows, s.kp);
     ozaki_slice_kernel<<<m, SL_TPB, 0, st>>>(P, ldp, m, k, s.kp, s.ns, s.planes, s.pstride,
-                                             s.ldpl, s.exps, info);
+                                             s.ldpl, s.exps, s.rsum, info);
     return launch_status("ozaki_slice_kernel");
 }
 
@@ -398,7 +496,7 @@ int ozaki_syrk(double *C, long long ldc, int m, const OzakiSlices &s, int p_row0
                int *info, cudaStream_t st) {
     if (m <= 0) return FMLB_OK;
     FMLB_REQUIRE(s.ns >= 1 && s.ns <= OZAKI_MAX_SLICES, "ozaki: 1..%d slices", OZAKI_MAX_SLICES);
-    FMLB_REQUIRE(s.kp % OZ_KB == 0 && s.kp <= 4096, "ozaki: k must be a multiple of 32, <= 4096");
+    FMLB_REQUIRE(s.kp % OZ_KB == 0 && s.kp <= 8192, "ozaki: k must be a multiple of 32, <= 8192");
     FMLB_REQUIRE(p_row0 >= 0 && p_row0 + m <= s.rows, "ozaki: rows outside the slice buffer");
     CUtensorMap mA, mB;
     FMLB_TRY(make_plane_map(&mA, s.planes, s.rows, s.ldpl, s.kp, s.pstride, s.ns, OZ_BM));
@@ -413,9 +511,15 @@ int ozaki_syrk(double *C, long long ldc, int m, const OzakiSlices &s, int p_row0
     p.strip_tiles = p.strip_cols > 0 ? ceil_div(p.strip_cols, OZ_BN) : 0;
     p.ntiles = p.strip_tiles ? Tr * p.strip_tiles : Tr * Tr + Tr;
     p.ldc = ldc;
-    p.exp_bias = 2 - 8 * (s.ns + 1);
+    p.exp_bias = -8 * (s.ns + 1);
+    double zc = ldexp(1.0, -8 * s.ns - 1);  // half an ulp of the last digit
+    for (int t = 2; t <= s.ns; ++t) zc += ldexp(128.0, -8 * t);
+    p.zp_c = zc;
+    p.zp_kc2 = (double)s.kp * zc * zc;
     const tc::TestHooks hooks = tc::test_hooks();
     p.skip_loads = hooks.skip_loads;
+    p.stages = oz_stages(s.ns);
+    p.a_tmem = s.ns <= OZ_A_TMEM_MAX ? 1 : 0;
     const size_t smem = oz_smem_bytes(s.ns);
     static int attr_dev = -1;
     int dev = 0;
@@ -423,18 +527,18 @@ int ozaki_syrk(double *C, long long ldc, int m, const OzakiSlices &s, int p_row0
     if (attr_dev != dev) {
         FMLB_TRY(cuda_status(cudaFuncSetAttribute(ozaki_syrk_kernel,
                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                  (int)oz_smem_bytes(OZAKI_MAX_SLICES)),
+                                                  OZ_SMEM_LIMIT),
                              "ozaki: smem attribute"));
         attr_dev = dev;
     }
     const int grid = (int)std::min<long long>(p.ntiles, sm_count());
-    ozaki_syrk_kernel<<<grid, OZ_THREADS, smem, st>>>(mA, mB, s.exps, p, C, info,
+    ozaki_syrk_kernel<<<grid, OZ_THREADS, smem, st>>>(mA, mB, s.exps, s.rsum, p, C, info,
                                                        hooks.wait_budget);
     return launch_status("ozaki_syrk_kernel");
 }
 
 size_t ozaki_slice_bytes(int rows, int kp, int ns) {
-    return (size_t)ns * rows * kp + (size_t)rows * sizeof(int) + 512;
+    return (size_t)ns * rows * kp + (size_t)rows * (sizeof(int) + sizeof(double)) + 512;
 }
 
 int ozaki_bind(void *ws, int rows, int kp, int ns, OzakiSlices &s) {
@@ -446,7 +550,8 @@ int ozaki_bind(void *ws, int rows, int kp, int ns, OzakiSlices &s) {
     s.ns = ns;
     s.ldpl = kp;
     s.pstride = (long long)rows * kp;
-    s.exps = reinterpret_cast<int *>(p + (size_t)ns * rows * kp);
+    s.rsum = reinterpret_cast<double *>(p + (size_t)ns * rows * kp);  // 8-byte aligned: kp % 32 == 0
+    s.exps = reinterpret_cast<int *>(s.rsum + rows);
     return FMLB_OK;
 }
 
@@ -466,7 +571,7 @@ extern "C" int fmlb_syrk_lower_ozaki(double *C, long long ldc, int m, const doub
                  "fmlb_syrk_lower_ozaki: bad sizes");
     FMLB_REQUIRE(nslices >= 1 && nslices <= OZAKI_MAX_SLICES,
                  "fmlb_syrk_lower_ozaki: nslices must be 1..%d", OZAKI_MAX_SLICES);
-    FMLB_REQUIRE(k <= 4096, "fmlb_syrk_lower_ozaki: k=%d above 4096", k);
+    FMLB_REQUIRE(k <= 8192, "fmlb_syrk_lower_ozaki: k=%d above 8192", k);
     if (m == 0 || k == 0) return FMLB_OK;
     FMLB_REQUIRE(C && P && info, "fmlb_syrk_lower_ozaki: null pointer");
     const size_t need = fmlb_syrk_ozaki_workspace_bytes(m, k, nslices);

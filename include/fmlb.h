@@ -328,11 +328,12 @@ int fmlb_syrk_lower_f64(double *C, long long ldc, int m, const double *P, long l
  * that fmlb_potrs_f64 reads) and info as fmlb_potrf_f64; only the bulk and
  * strip trailing updates (C -= P P^T with k = the outer panel width) change:
  * P's rows are split into nslices (1..8) 8-bit digit planes (a signed leading
- * digit, unsigned lower ones) with one power-of-two scale per row, the
- * s(s+1)/2 leading digit products run as tcgen05.mma kind::i8 with exact
- * int32 accumulation, and the epilogue combines them in FP64 (the Ozaki
- * scheme). Per update the error is about 16x the FP64 rounding bound at
- * nslices = 6 and below it at 7.
+ * digit, lower digits stored around a zero point) with one power-of-two
+ * scale per row, the s(s+1)/2 leading digit products run as tcgen05.mma
+ * kind::i8 with exact int32 accumulation, and the epilogue combines them in
+ * FP64 and adds the zero-point terms (the Ozaki scheme). Six planes give the
+ * accuracy of seven truncated 7-bit planes; seven or eight are below the
+ * FP64 rounding bound.
  *   work  fmlb_potrf_ozaki_workspace_bytes(n, nslices) bytes
  *   info  LAPACK-style (> 0: first non-positive pivot); FMLB_ETIMEDOUT (< 0)
  *         if a bounded device-side wait of the tensor-core kernel gave up. */
@@ -342,7 +343,7 @@ int fmlb_potrf_ozaki_f64(double *A, long long lda, int n, int nslices, void *wor
 
 /* The int8 emulated trailing update on its own (the step above): C -= P P^T
  * on the triangle i >= j of the row-major (m, m) C, or its first strip_cols
- * columns; P is (m, k), k <= 4096. work: fmlb_syrk_ozaki_workspace_bytes
+ * columns; P is (m, k), k <= 8192. work: fmlb_syrk_ozaki_workspace_bytes
  * (m, k, nslices) bytes (digit planes and row exponents). info (device):
  * skipped when non-zero; FMLB_ETIMEDOUT stored on a device-side timeout.
  * (The LAPACK dsyrk call inside dpotrf, fcho_solve.f90:35.) */
