@@ -28,7 +28,8 @@
 // (21 products instead of 28); the error of one entry stays below
 // k (s + 3) 2^(e_r + e_c + 2 - 8 s).
 //
-// Kernel (persistent, one CTA per SM, 320 threads), output tile 128 x 64:
+// Kernel (one CTA per SM at a time, four tiles per CTA, 320 threads), output
+// tile 128 x 64:
 //   warp 0      TMA producer: per 32-byte k step, the s digit planes of the
 //               128 A rows and 64 B rows (one 3-D box each, 32-byte swizzle)
 //               into a ring as deep as shared memory allows (5 stages at
@@ -531,7 +532,11 @@ int ozaki_syrk(double *C, long long ldc, int m, const OzakiSlices &s, int p_row0
                              "ozaki: smem attribute"));
         attr_dev = dev;
     }
-    const int grid = (int)std::min<long long>(p.ntiles, sm_count());
+    // four tiles per CTA: CTAs retire while the update runs, so the
+    // factorisation's high-priority panel chain gets SMs (a persistent grid
+    // held every SM until the update ended and serialised the lookahead)
+    const int grid = (int)std::min<long long>(
+        p.ntiles, std::max<long long>(sm_count(), (p.ntiles + 3) / 4));
     ozaki_syrk_kernel<<<grid, OZ_THREADS, smem, st>>>(mA, mB, s.exps, s.rsum, p, C, info,
                                                        hooks.wait_budget);
     return launch_status("ozaki_syrk_kernel");
