@@ -9,6 +9,8 @@
 // max_c |P[r, c]| < 2^e_r, so x = P[r, c] 2^-(e_r + 1) lies in (-1/2, 1/2),
 // and s base-256 digits by repeated flooring, all exact in FP64:
 //     d_1 = floor(256 x) in [-128, 127];  u_t = floor(256 rem_{t-1}) in [0, 255]
+// (a remainder 1 - |tiny| that rounds to 1.0 after a leading -1 is carried
+// back into the digit, so every remainder stays in [0, 1))
 // stored as signed bytes with a zero point: v_t = u_t - 128 in [-128, 127], so
 //     x = xt + c + rho,   xt = d_1 / 256 + sum_{t>1} v_t 256^-t,
 //     c = 128 sum_{t=2..s} 256^-t,   0 <= rho < 256^-s.
@@ -35,11 +37,7 @@
 //               into a ring as deep as shared memory allows (5 stages at
 //               s = 6, at most 8);
 //   warp 1      allocates 512 TMEM columns (s <= 8 accumulators of 64 int32
-//               columns) and issues tcgen05.mma kind::i8 (M 128, N 64, K 32).
-//               For s <= 6 it first copies the k step's A planes into TMEM
-//               (tcgen05.cp, two buffers after the accumulators), so each of
-//               the s (s + 1) / 2 products reads only its B plane from shared
-//               memory: shared-memory operand traffic halves;
+//               columns) and issues tcgen05.mma kind::i8 (M 128, N 64, K 32);
 //   warps 2..9  epilogue, two warps per TMEM lane quarter (32 columns each):
 //               drain the s accumulators into FP64 (Horner), release TMEM to
 //               the next tile's MMAs, scale by the row and column exponents,
@@ -74,9 +72,6 @@ constexpr int OZ_NONFINITE = 0x7fffffff;    // exponent marking a row with Inf /
 constexpr long long kOzDefaultBudget = 4000000000LL;  // clock cycles (~2 s)
 constexpr int OZ_SMEM_LIMIT = 232448 - 64;  // opt-in shared memory per CTA, less static
 constexpr int OZ_BAR_BYTES = (2 * OZ_MAX_STAGES + 3) * 8 + 8;
-constexpr int OZ_A_TMEM_MAX = 6;            // planes that fit A in TMEM twice beside D
-constexpr int OZ_A_TMEM_COL = OZ_A_TMEM_MAX * OZ_BN;  // 384: A buffers after 6 accumulators
-static_assert(OZ_A_TMEM_COL + 2 * OZ_A_TMEM_MAX * 8 <= OZ_TMEM_COLS, "A buffers fit TMEM");
 
 struct OzParams {
     int m;             // rows (= columns) of C
@@ -92,7 +87,6 @@ struct OzParams {
     double zp_kc2;     // kp c'^2
     int skip_loads;    // test hook: the producer issues no copies
     int stages;        // depth of the operand ring
-    int a_tmem;        // A planes copied to TMEM once per k step (ns <= 6)
 };
 
 // Instruction descriptor, kind::i8: signed A and B, int32 accumulator, both
@@ -107,22 +101,6 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
         " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-
-// The same MMA with A (128 rows x 32 bytes) read from TMEM columns at a_tmem.
-__device__ __forceinline__ void mma_i8_ta(uint32_t tmem_d, uint32_t a_tmem, uint64_t bdesc,
-                                          uint32_t idesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-        " tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p;\n}\n" ::"r"(tmem_d),
-        "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-
-// Copies a 128-row x 32-byte shared-memory tile (matrix descriptor sdesc) into
-// the 8 TMEM columns at taddr, row i to lane i; ordered before the MMAs this
-// thread issues after it.
-__device__ __forceinline__ void tmem_cp_128x256b(uint32_t taddr, uint64_t sdesc) {
-    asm volatile("tcgen05.cp.cta_group::1.128x256b [%0], %1;\n" ::"r"(taddr), "l"(sdesc));
 }
 
 // Tile t -> (row0, col0): lower triangle of 128 x 64 tiles (row block `by`
@@ -240,26 +218,6 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constan
                     const uint8_t *sb = sa + p.ns * OZ_A_PLANE;
                     const uint64_t da = tc::smem_desc_kmajor(sa, OZ_KB);
                     const uint64_t db = tc::smem_desc_kmajor(sb, OZ_KB);
-                    if (p.a_tmem) {
-                        // A planes to TMEM once (double-buffered by k step), then every
-                        // product reads A there and only B from shared memory
-                        const uint32_t abuf = tmem_base + (uint32_t)(OZ_A_TMEM_COL +
-                                                                     (consumed & 1) * p.ns * 8);
-                        for (int a = 0; a < p.ns; ++a)
-                            tmem_cp_128x256b(abuf + (uint32_t)(a * 8),
-                                             da + (uint64_t)((a * OZ_A_PLANE) >> 4));
-                        for (int q = 0; q < p.ns; ++q) {
-                            const uint32_t dacc = tmem_base + (uint32_t)(q * OZ_BN);
-                            for (int a = 0; a <= q; ++a) {
-                                const int b = q - a;
-                                mma_i8_ta(dacc, abuf + (uint32_t)(a * 8),
-                                          db + (uint64_t)((b * OZ_B_PLANE) >> 4), idesc_i8(a, b),
-                                          (kb > 0 || a > 0) ? 1u : 0u);
-                            }
-                        }
-                        tc::mma_commit(&empty[st]);
-                        continue;
-                    }
                     for (int q = 0; q < p.ns; ++q) {
                         const uint32_t dacc = tmem_base + (uint32_t)(q * OZ_BN);
                         for (int a = 0; a <= q; ++a) {
@@ -410,8 +368,14 @@ ozaki_slice_kernel(const double *__restrict__ P, long long ldp, int m, int k, in
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
                 x[i] *= 256.0;
-                const double d = floor(x[i]);       // [-128, 127] first, then [0, 255]
+                double d = floor(x[i]);             // [-128, 127] first, then [0, 255]
                 x[i] -= d;
+                // a tiny negative leading value gives d = -1 and a remainder
+                // 1 - |x| that rounds to 1.0: carry it back into the digit
+                if (x[i] >= 1.0) {
+                    x[i] -= 1.0;
+                    d += 1.0;
+                }
                 const int v = (int)d - (t ? 128 : 0);  // zero point of the lower planes
                 psum[t] += v;
                 word |= (uint64_t)((uint32_t)v & 0xffu) << (8 * i);
@@ -520,7 +484,6 @@ int ozaki_syrk(double *C, long long ldc, int m, const OzakiSlices &s, int p_row0
     const tc::TestHooks hooks = tc::test_hooks();
     p.skip_loads = hooks.skip_loads;
     p.stages = oz_stages(s.ns);
-    p.a_tmem = s.ns <= OZ_A_TMEM_MAX ? 1 : 0;
     const size_t smem = oz_smem_bytes(s.ns);
     static int attr_dev = -1;
     int dev = 0;

@@ -28,6 +28,9 @@ def split(P, nslices, kp=None):
         x = x * 256.0
         d = np.floor(x)
         x = x - d
+        up = x >= 1.0  # 1 - |tiny| rounded to 1.0 after a leading -1: carry
+        x = np.where(up, x - 1.0, x)
+        d = np.where(up, d + 1.0, d)
         digits.append(d - (128.0 if t else 0.0))
     zc = np.ldexp(1.0, -8 * nslices - 1)
     for t in range(2, nslices + 1):

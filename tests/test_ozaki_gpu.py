@@ -73,6 +73,28 @@ def test_syrk_ozaki_bit_exact_vs_emulation(m, k, s, strip):
     np.testing.assert_array_equal(out[~mask], C[~mask])  # untouched outside the update
 
 
+def test_syrk_ozaki_tiny_negative_entries():
+    """Rows with one dominant entry and tiny negative ones (the shape of a
+    Cholesky factor of a nearly diagonal kernel matrix): a tiny negative
+    value has leading digit -1 and a remainder that rounds to 1.0, which must
+    be carried instead of overflowing the next digit. Bit-exact against the
+    emulation and within the scheme's bound of the exact product."""
+    rng = np.random.default_rng(8)
+    m, k = 400, 1024
+    P = -np.abs(rng.standard_normal((m, k))) * np.ldexp(1.0, rng.integers(-80, -40, size=(m, k)))
+    P[np.arange(m), rng.integers(0, k, size=m)] = rng.uniform(0.5, 0.99, size=m)
+    P[:, 7] = -1e-300
+    C = np.eye(m) + 1e-3 * rng.standard_normal((m, m))
+    for s in (6, 7):
+        out, info = _syrk_gpu(C, P, s)
+        assert info == 0
+        np.testing.assert_array_equal(out, emu.syrk_lower(C, P, s))
+        low = np.tril(np.ones((m, m), dtype=bool))
+        err = np.abs(out - (C - P @ P.T))[low]
+        bound = (emu.error_bound(P, s) + 1e-14 * np.abs(P) @ np.abs(P).T + 1e-15 * np.abs(C))[low]
+        assert (err <= bound).all()
+
+
 def test_syrk_ozaki_nonfinite_rows_propagate():
     rng = np.random.default_rng(3)
     P = rng.standard_normal((200, 128))
