@@ -57,7 +57,8 @@
 namespace fmlb {
 namespace {
 
-constexpr int OZ_BM = 128, OZ_BN = 64;
+constexpr int OZ_BM = 128, OZ_BN = 128;
+constexpr int OZ_PASS_Q = 4;      // diagonals (accumulators of 128 columns) per pass
 constexpr int OZ_KB = 32;          // int8 k values (bytes) per stage: one MMA K step
 constexpr int OZ_MAX_STAGES = 8;  // the ring depth is set per launch from shared memory
 constexpr int OZ_THREADS = 320;    // 10 warps
@@ -65,7 +66,7 @@ constexpr int OZ_EPI_WARPS = 8;
 constexpr int OZ_TMEM_COLS = 512;
 constexpr int OZ_PITCH = 33;       // doubles per staged row (conflict-free transpose)
 constexpr int OZ_A_PLANE = OZ_BM * OZ_KB;   // 4096 bytes per A digit plane per stage
-constexpr int OZ_B_PLANE = OZ_BN * OZ_KB;   // 2048
+constexpr int OZ_B_PLANE = OZ_BN * OZ_KB;   // 4096
 constexpr int OZ_STAGE_STG = OZ_EPI_WARPS * 16 * OZ_PITCH * (int)sizeof(double);
 constexpr int OZ_NONFINITE = 0x7fffffff;    // exponent marking a row with Inf / NaN
 
@@ -83,6 +84,7 @@ struct OzParams {
     long long ntiles;
     long long ldc;
     int exp_bias;      // -8 (ns + 1)
+    int npass;         // 1 (ns <= 4) or 2: diagonals [0, 4) then [4, ns)
     double zp_c;       // c' (zero point of the digit planes)
     double zp_kc2;     // kp c'^2
     int skip_loads;    // test hook: the producer issues no copies
@@ -103,20 +105,20 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
-// Tile t -> (row0, col0): lower triangle of 128 x 64 tiles (row block `by`
-// holds column tiles 0 .. 2 by + 1), or the first strip_tiles column tiles of
-// every row block. False for tiles outside C.
+// Tile t -> (row0, col0): lower triangle of 128 x 128 tiles (row block `by`
+// holds column tiles 0 .. by), or the first strip_tiles column tiles of every
+// row block. False for tiles outside C.
 __device__ __forceinline__ bool oz_tile(long long t, const OzParams &p, int &row0, int &col0) {
     int by, bx;
     if (p.strip_tiles > 0) {
         by = (int)(t / p.strip_tiles);
         bx = (int)(t % p.strip_tiles);
-        if (bx > 2 * by + 1) return false;
+        if (bx > by) return false;
     } else {
-        by = (int)((sqrt(4.0 * (double)t + 1.0) - 1.0) * 0.5);
-        while ((long long)by * by + by > t) --by;
-        while ((long long)(by + 1) * (by + 1) + (by + 1) <= t) ++by;
-        bx = (int)(t - (long long)by * by - by);
+        by = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+        while ((long long)by * (by + 1) / 2 > t) --by;
+        while ((long long)(by + 1) * (by + 2) / 2 <= t) ++by;
+        bx = (int)(t - (long long)by * (by + 1) / 2);
     }
     row0 = by * OZ_BM;
     col0 = bx * OZ_BN;
@@ -125,15 +127,20 @@ __device__ __forceinline__ bool oz_tile(long long t, const OzParams &p, int &row
 
 __device__ __forceinline__ void oz_fail(int *info) { atomicCAS(info, 0, FMLB_ETIMEDOUT); }
 
+// Pass q0..q1 of the diagonals needs the digit planes 0..q1-1.
+__device__ __forceinline__ void oz_pass(const OzParams &p, int ps, int &q0, int &q1) {
+    q0 = ps * OZ_PASS_Q;
+    q1 = min(p.ns, q0 + OZ_PASS_Q);
+}
+
 __global__ void __launch_bounds__(OZ_THREADS, 1)
-ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapLo, const __grid_constant__ CUtensorMap mapHi,
                   const int *__restrict__ exps, const double *__restrict__ rsum, OzParams p,
-                  double *__restrict__ C,
-                  int *__restrict__ info, long long budget) {
+                  double *__restrict__ C, int *__restrict__ info, long long budget) {
     extern __shared__ uint8_t oz_smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~(uintptr_t)1023);
-    const int stage_bytes = p.ns * (OZ_A_PLANE + OZ_B_PLANE);
+    const int stage_bytes = p.ns * (OZ_A_PLANE + OZ_B_PLANE);  // B planes after ns A planes
     const int nst = p.stages;
     double *stg_all = reinterpret_cast<double *>(smem + nst * stage_bytes);
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + nst * stage_bytes + OZ_STAGE_STG);
@@ -171,19 +178,24 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constan
             for (long long t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
                 int row0, col0;
                 if (!oz_tile(t, p, row0, col0)) continue;
-                for (int kb = 0; kb < p.nkb && !p.skip_loads; ++kb, ++issued) {
-                    const int st = (int)(issued % nst);
-                    const uint32_t ph = (uint32_t)((issued / nst) & 1);
-                    if (!tc::mbar_wait(&empty[st], ph ^ 1, budget)) {
-                        oz_fail(info);
-                        ok = false;
-                        break;
+                for (int ps = 0; ps < p.npass && ok; ++ps) {
+                    int q0, q1;
+                    oz_pass(p, ps, q0, q1);
+                    const CUtensorMap *map = q1 == p.ns ? &mapHi : &mapLo;  // q1 planes
+                    for (int kb = 0; kb < p.nkb && !p.skip_loads; ++kb, ++issued) {
+                        const int st = (int)(issued % nst);
+                        const uint32_t ph = (uint32_t)((issued / nst) & 1);
+                        if (!tc::mbar_wait(&empty[st], ph ^ 1, budget)) {
+                            oz_fail(info);
+                            ok = false;
+                            break;
+                        }
+                        uint8_t *sa = smem + st * stage_bytes;
+                        uint8_t *sb = sa + p.ns * OZ_A_PLANE;
+                        tc::mbar_arrive_expect_tx(&full[st], (uint32_t)(q1 * (OZ_A_PLANE + OZ_B_PLANE)));
+                        tc::tma_load_3d(sa, map, &full[st], kb * OZ_KB, p.p_row0 + row0, 0);
+                        tc::tma_load_3d(sb, map, &full[st], kb * OZ_KB, p.p_row0 + col0, 0);
                     }
-                    uint8_t *sa = smem + st * stage_bytes;
-                    uint8_t *sb = sa + p.ns * OZ_A_PLANE;
-                    tc::mbar_arrive_expect_tx(&full[st], (uint32_t)stage_bytes);
-                    tc::tma_load_3d(sa, &mapA, &full[st], kb * OZ_KB, p.p_row0 + row0, 0);
-                    tc::tma_load_3d(sb, &mapB, &full[st], kb * OZ_KB, p.p_row0 + col0, 0);
                 }
             }
             // every copy this thread issued has landed before the CTA winds down
@@ -195,44 +207,48 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constan
         // ------------------------------------------------------------- MMA issuer
         if (lane == 0) {
             long long consumed = 0;
-            int lt = 0;
+            int lp = 0;  // passes issued
             bool ok = true;
             for (long long t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
                 int row0, col0;
                 if (!oz_tile(t, p, row0, col0)) continue;
-                if (!tc::mbar_wait(tmem_empty, (uint32_t)((lt & 1) ^ 1), budget)) {
-                    oz_fail(info);
-                    break;
-                }
-                tc::fence_after_sync();
-                for (int kb = 0; kb < p.nkb; ++kb, ++consumed) {
-                    const int st = (int)(consumed % nst);
-                    const uint32_t ph = (uint32_t)((consumed / nst) & 1);
-                    if (!tc::mbar_wait(&full[st], ph, budget)) {
+                for (int ps = 0; ps < p.npass; ++ps, ++lp) {
+                    int q0, q1;
+                    oz_pass(p, ps, q0, q1);
+                    if (!tc::mbar_wait(tmem_empty, (uint32_t)((lp & 1) ^ 1), budget)) {
                         oz_fail(info);
                         ok = false;
                         break;
                     }
                     tc::fence_after_sync();
-                    const uint8_t *sa = smem + st * stage_bytes;
-                    const uint8_t *sb = sa + p.ns * OZ_A_PLANE;
-                    const uint64_t da = tc::smem_desc_kmajor(sa, OZ_KB);
-                    const uint64_t db = tc::smem_desc_kmajor(sb, OZ_KB);
-                    for (int q = 0; q < p.ns; ++q) {
-                        const uint32_t dacc = tmem_base + (uint32_t)(q * OZ_BN);
-                        for (int a = 0; a <= q; ++a) {
-                            const int b = q - a;
-                            // plane offsets in 16-byte units of the descriptor address
-                            mma_i8(dacc, da + (uint64_t)((a * OZ_A_PLANE) >> 4),
-                                   db + (uint64_t)((b * OZ_B_PLANE) >> 4), idesc_i8(a, b),
-                                   (kb > 0 || a > 0) ? 1u : 0u);
+                    for (int kb = 0; kb < p.nkb; ++kb, ++consumed) {
+                        const int st = (int)(consumed % nst);
+                        const uint32_t ph = (uint32_t)((consumed / nst) & 1);
+                        if (!tc::mbar_wait(&full[st], ph, budget)) {
+                            oz_fail(info);
+                            ok = false;
+                            break;
                         }
+                        tc::fence_after_sync();
+                        const uint8_t *sa = smem + st * stage_bytes;
+                        const uint8_t *sb = sa + p.ns * OZ_A_PLANE;
+                        const uint64_t da = tc::smem_desc_kmajor(sa, OZ_KB);
+                        const uint64_t db = tc::smem_desc_kmajor(sb, OZ_KB);
+                        for (int q = q0; q < q1; ++q) {
+                            const uint32_t dacc = tmem_base + (uint32_t)((q - q0) * OZ_BN);
+                            for (int a = 0; a <= q; ++a) {
+                                const int b = q - a;
+                                // plane offsets in 16-byte units of the descriptor address
+                                mma_i8(dacc, da + (uint64_t)((a * OZ_A_PLANE) >> 4),
+                                       db + (uint64_t)((b * OZ_B_PLANE) >> 4), idesc_i8(a, b),
+                                       (kb > 0 || a > 0) ? 1u : 0u);
+                            }
+                        }
+                        tc::mma_commit(&empty[st]);  // frees the stage once these MMAs finish
                     }
-                    tc::mma_commit(&empty[st]);  // frees the stage once these MMAs finish
+                    if (!ok) break;
+                    tc::mma_commit(tmem_full);
                 }
-                if (!ok) break;
-                tc::mma_commit(tmem_full);
-                ++lt;
             }
             // every MMA issued has finished before TMEM is released
             tc::mma_commit(mma_done);
@@ -240,69 +256,101 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constan
         }
     } else {
         // --------------------------------------------------------------- epilogue
-        const int qw = warp & 3;            // TMEM lane quarter this warp may read
-        const int half = (warp - 2) >> 2;   // which 32 of the tile's 64 columns
+        // Two warps per TMEM lane quarter, 64 columns (two chunks of 32) each.
+        // Per pass and chunk: drain the pass's accumulators into FP64 (Horner
+        // in 256), scale, and subtract from C through a shared-memory transpose
+        // (coalesced read-modify-write, the 16 rows' loads in flight at once).
+        // TMEM is released after the second chunk's drain, so the next pass's
+        // MMAs overlap that chunk's read-modify-write.
+        const int qw = warp & 3;
+        const int half = (warp - 2) >> 2;
         double *stg = stg_all + (warp - 2) * 16 * OZ_PITCH;
-        int lt = 0;
-        for (long long t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
+        int lp = 0;
+        bool ok = true;
+        for (long long t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
             int row0, col0;
             if (!oz_tile(t, p, row0, col0)) continue;
-            if (!tc::mbar_wait(tmem_full, (uint32_t)(lt & 1), budget)) {
-                oz_fail(info);
-                break;
-            }
-            tc::fence_after_sync();
-            double acc[32];
-#pragma unroll
-            for (int j = 0; j < 32; ++j) acc[j] = 0.0;
-            for (int q = 0; q < p.ns; ++q) {
-                uint32_t v[32];
-                tc::tmem_ld32(tmem_base + ((uint32_t)(qw * 32) << 16) +
-                                  (uint32_t)(q * OZ_BN + half * 32), v);
-#pragma unroll
-                for (int j = 0; j < 32; ++j)
-                    acc[j] = fma(acc[j], 256.0, (double)(int)v[j]);
-            }
-            tc::fence_before_sync();
-            __syncwarp();
-            if (lane == 0) tc::mbar_arrive(tmem_empty);  // the next tile's MMAs may start
-            ++lt;
-            // (acc 256^-(s+1) + c' (S_r + S_c) + k c'^2) 2^(e_r + e_c + 2), the
-            // operations in a fixed order with no contraction
             const int grow = row0 + qw * 32 + lane;
             const int er = grow < p.m ? exps[p.p_row0 + grow] : 0;
             const double sr = grow < p.m ? rsum[p.p_row0 + grow] : 0.0;
-            const int gcl = col0 + half * 32 + lane;
-            const int ecl = gcl < p.m ? exps[p.p_row0 + gcl] : 0;
-            const double scl = gcl < p.m ? rsum[p.p_row0 + gcl] : 0.0;
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                const int ec = __shfl_sync(0xffffffffu, ecl, j);
-                const double sc = __shfl_sync(0xffffffffu, scl, j);
-                const double core =
-                    __dadd_rn(__dadd_rn(ldexp(acc[j], p.exp_bias),
-                                        __dmul_rn(p.zp_c, __dadd_rn(sr, sc))),
-                              p.zp_kc2);
-                acc[j] = (er == OZ_NONFINITE || ec == OZ_NONFINITE)
-                             ? __longlong_as_double(0x7ff8000000000000LL)
-                             : ldexp(core, er + ec + 2);
-            }
-            // transpose through shared memory, 16 rows at a time, then a
-            // coalesced read-modify-write of the rows' lower-triangle part
-#pragma unroll
-            for (int hh = 0; hh < 2; ++hh) {
-                if ((lane >> 4) == hh) {
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) stg[(lane & 15) * OZ_PITCH + j] = acc[j];
+            for (int ps = 0; ps < p.npass; ++ps, ++lp) {
+                int q0, q1;
+                oz_pass(p, ps, q0, q1);
+                const bool last = ps == p.npass - 1;
+                // the first of two passes holds the top diagonals, scaled by 256^-5
+                const int bias = last ? p.exp_bias : -8 * (OZ_PASS_Q + 1);
+                if (!tc::mbar_wait(tmem_full, (uint32_t)(lp & 1), budget)) {
+                    oz_fail(info);
+                    ok = false;
+                    break;
                 }
-                __syncwarp();
-                const int c = col0 + half * 32 + lane;
-                for (int rr = 0; rr < 16; ++rr) {
-                    const int r = row0 + qw * 32 + hh * 16 + rr;
-                    if (r < p.m && c < p.m && c <= r && (p.strip_cols == 0 || c < p.strip_cols))
-                        C[(size_t)r * p.ldc + c] -= stg[rr * OZ_PITCH + lane];
+                tc::fence_after_sync();
+                for (int cc = 0; cc < 2; ++cc) {
+                    const int cb = half * 64 + cc * 32;  // chunk's first column in the tile
+                    double acc[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+                    for (int q = q0; q < q1; ++q) {
+                        uint32_t v[32];
+                        tc::tmem_ld32(tmem_base + ((uint32_t)(qw * 32) << 16) +
+                                          (uint32_t)((q - q0) * OZ_BN + cb), v);
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            acc[j] = fma(acc[j], 256.0, (double)(int)v[j]);
+                    }
+                    if (cc == 1) {
+                        tc::fence_before_sync();
+                        __syncwarp();
+                        if (lane == 0) tc::mbar_arrive(tmem_empty);  // the next pass may start
+                    }
+                    // last pass: (acc 256^-(s+1) + c' (S_r + S_c) + k c'^2) 2^(e_r + e_c + 2);
+                    // first of two: acc 256^-5 2^(e_r + e_c + 2); fixed order, no contraction
+                    const int gcl = col0 + cb + lane;
+                    const int ecl = gcl < p.m ? exps[p.p_row0 + gcl] : 0;
+                    const double scl = gcl < p.m ? rsum[p.p_row0 + gcl] : 0.0;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int ec = __shfl_sync(0xffffffffu, ecl, j);
+                        const double sc = __shfl_sync(0xffffffffu, scl, j);
+                        double core = ldexp(acc[j], bias);
+                        if (last)
+                            core = __dadd_rn(__dadd_rn(core, __dmul_rn(p.zp_c, __dadd_rn(sr, sc))),
+                                             p.zp_kc2);
+                        acc[j] = (er == OZ_NONFINITE || ec == OZ_NONFINITE)
+                                     ? __longlong_as_double(0x7ff8000000000000LL)
+                                     : ldexp(core, er + ec + 2);
+                    }
+#pragma unroll 1
+                    for (int hh = 0; hh < 2; ++hh) {
+                        const int c = col0 + cb + lane;
+                        const int rb = row0 + qw * 32 + hh * 16;
+                        if ((lane >> 4) == hh) {
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) stg[(lane & 15) * OZ_PITCH + j] = acc[j];
+                        }
+                        __syncwarp();
+                        // eight rows' C values are loaded first, all in flight at once
+#pragma unroll
+                        for (int g = 0; g < 16; g += 8) {
+                            double cv[8];
+#pragma unroll
+                            for (int rr = 0; rr < 8; ++rr) {
+                                const int r = rb + g + rr;
+                                const bool in = r < p.m && c < p.m && c <= r &&
+                                                (p.strip_cols == 0 || c < p.strip_cols);
+                                cv[rr] = in ? C[(size_t)r * p.ldc + c] : 0.0;
+                            }
+#pragma unroll
+                            for (int rr = 0; rr < 8; ++rr) {
+                                const int r = rb + g + rr;
+                                if (r < p.m && c < p.m && c <= r &&
+                                    (p.strip_cols == 0 || c < p.strip_cols))
+                                    C[(size_t)r * p.ldc + c] = cv[rr] - stg[(g + rr) * OZ_PITCH + lane];
+                            }
+                        }
+                        __syncwarp();
+                    }
                 }
-                __syncwarp();
             }
         }
     }
@@ -463,9 +511,12 @@ int ozaki_syrk(double *C, long long ldc, int m, const OzakiSlices &s, int p_row0
     FMLB_REQUIRE(s.ns >= 1 && s.ns <= OZAKI_MAX_SLICES, "ozaki: 1..%d slices", OZAKI_MAX_SLICES);
     FMLB_REQUIRE(s.kp % OZ_KB == 0 && s.kp <= 8192, "ozaki: k must be a multiple of 32, <= 8192");
     FMLB_REQUIRE(p_row0 >= 0 && p_row0 + m <= s.rows, "ozaki: rows outside the slice buffer");
-    CUtensorMap mA, mB;
-    FMLB_TRY(make_plane_map(&mA, s.planes, s.rows, s.ldpl, s.kp, s.pstride, s.ns, OZ_BM));
-    FMLB_TRY(make_plane_map(&mB, s.planes, s.rows, s.ldpl, s.kp, s.pstride, s.ns, OZ_BN));
+    // boxes of 128 rows and the planes a pass reads: min(ns, 4) for the first
+    // of two passes, all ns for the last
+    CUtensorMap mLo, mHi;
+    FMLB_TRY(make_plane_map(&mLo, s.planes, s.rows, s.ldpl, s.kp, s.pstride,
+                            std::min(s.ns, OZ_PASS_Q), OZ_BM));
+    FMLB_TRY(make_plane_map(&mHi, s.planes, s.rows, s.ldpl, s.kp, s.pstride, s.ns, OZ_BM));
     OzParams p;
     p.m = m;
     p.p_row0 = p_row0;
@@ -474,7 +525,8 @@ int ozaki_syrk(double *C, long long ldc, int m, const OzakiSlices &s, int p_row0
     p.strip_cols = strip_cols > 0 ? std::min(strip_cols, m) : 0;
     const long long Tr = ceil_div(m, OZ_BM);
     p.strip_tiles = p.strip_cols > 0 ? ceil_div(p.strip_cols, OZ_BN) : 0;
-    p.ntiles = p.strip_tiles ? Tr * p.strip_tiles : Tr * Tr + Tr;
+    p.ntiles = p.strip_tiles ? Tr * p.strip_tiles : Tr * (Tr + 1) / 2;
+    p.npass = s.ns > OZ_PASS_Q ? 2 : 1;
     p.ldc = ldc;
     p.exp_bias = -8 * (s.ns + 1);
     double zc = ldexp(1.0, -8 * s.ns - 1);  // half an ulp of the last digit
@@ -500,7 +552,7 @@ int ozaki_syrk(double *C, long long ldc, int m, const OzakiSlices &s, int p_row0
     // held every SM until the update ended and serialised the lookahead)
     const int grid = (int)std::min<long long>(
         p.ntiles, std::max<long long>(sm_count(), (p.ntiles + 3) / 4));
-    ozaki_syrk_kernel<<<grid, OZ_THREADS, smem, st>>>(mA, mB, s.exps, s.rsum, p, C, info,
+    ozaki_syrk_kernel<<<grid, OZ_THREADS, smem, st>>>(mLo, mHi, s.exps, s.rsum, p, C, info,
                                                        hooks.wait_budget);
     return launch_status("ozaki_syrk_kernel");
 }

@@ -5,8 +5,9 @@ per-row exponent from frexp of the row maximum, base-256 digits by repeated
 flooring (a signed leading digit; lower digits stored with the zero point
 128), the per-row sums of those digits, the exact integer products summed
 per diagonal (float64 holds them exactly), the Horner combination in 256
-with one rounding per step (what the kernel's FMA does), the zero-point
-terms added in the kernel's order, and the power-of-two scaling. The kernel
+with one rounding per step (what the kernel's FMA does) over each pass of
+at most four diagonals, the zero-point terms added in the kernel's order,
+the power-of-two scaling, and one subtraction from C per pass. The kernel
 must match it bit for bit.
 """
 
@@ -41,31 +42,55 @@ def split(P, nslices, kp=None):
     return digits, e, zc, S
 
 
-def product(P, nslices, kp=None):
-    """The emulated P P^T (m, m)."""
+PASS_Q = 4  # diagonals per pass of the kernel (accumulators of 128 TMEM columns)
+
+
+def product_parts(P, nslices, kp=None):
+    """The emulated P P^T as the kernel subtracts it: one (m, m) part per pass.
+
+    Diagonals [0, 4) form the first part and [4, s) the second (s > 4 only);
+    each part is a Horner sum in 256 scaled by 256^-(q1 + 1) for its last
+    diagonal q1 - 1, and the last part carries the zero-point terms."""
     d, e, zc, S = split(P, nslices, kp)
     m, kk = d[0].shape
-    acc = np.zeros((m, m))
-    for q in range(nslices):
-        Dq = np.zeros((m, m))
-        for a in range(q + 1):
-            Dq += d[a] @ d[q - a].T
-        acc = acc * 256.0 + Dq
-    core = (np.ldexp(acc, -8 * (nslices + 1)) + zc * (S[:, None] + S[None, :])) + kk * zc * zc
-    return np.ldexp(core, e[:, None] + e[None, :] + 2)
+    scale = e[:, None] + e[None, :] + 2
+    parts = []
+    for q0 in range(0, nslices, PASS_Q):
+        q1 = min(nslices, q0 + PASS_Q)
+        acc = np.zeros((m, m))
+        for q in range(q0, q1):
+            Dq = np.zeros((m, m))
+            for a in range(q + 1):
+                Dq += d[a] @ d[q - a].T
+            acc = acc * 256.0 + Dq
+        core = np.ldexp(acc, -8 * (q1 + 1))
+        if q1 == nslices:
+            core = (core + zc * (S[:, None] + S[None, :])) + kk * zc * zc
+        parts.append(np.ldexp(core, scale))
+    return parts
+
+
+def product(P, nslices, kp=None):
+    """The emulated P P^T (m, m), the passes' parts summed."""
+    parts = product_parts(P, nslices, kp)
+    V = parts[0]
+    for part in parts[1:]:
+        V = V + part
+    return V
 
 
 def syrk_lower(C, P, nslices, strip_cols=0):
-    """C - P P^T on the lower triangle (first strip_cols columns if > 0); the
-    kernel pads k to a multiple of 32 with zeros."""
+    """C - P P^T on the lower triangle (first strip_cols columns if > 0), one
+    subtraction per pass in the kernel's order; the kernel pads k to a
+    multiple of 32 with zeros."""
     C = np.array(C, dtype=np.float64, copy=True)
     m = C.shape[0]
     kp = -(-P.shape[1] // 32) * 32
-    V = product(P, nslices, kp)
     mask = np.tril(np.ones((m, m), dtype=bool))
     if strip_cols > 0:
         mask[:, strip_cols:] = False
-    C[mask] -= V[mask]
+    for V in product_parts(P, nslices, kp):
+        C[mask] -= V[mask]
     return C
 
 
