@@ -64,15 +64,16 @@ constexpr int OZ_MAX_STAGES = 8;  // the ring depth is set per launch from share
 constexpr int OZ_THREADS = 320;    // 10 warps
 constexpr int OZ_EPI_WARPS = 8;
 constexpr int OZ_TMEM_COLS = 512;
-constexpr int OZ_PITCH = 33;       // doubles per staged row (conflict-free transpose)
+constexpr int OZ_CPITCH = OZ_BN + 1;  // doubles per row of the staged C tile (odd: rows of
+                                      // one column fall in 16 distinct banks per half-warp)
 constexpr int OZ_A_PLANE = OZ_BM * OZ_KB;   // 4096 bytes per A digit plane per stage
 constexpr int OZ_B_PLANE = OZ_BN * OZ_KB;   // 4096
-constexpr int OZ_STAGE_STG = OZ_EPI_WARPS * 16 * OZ_PITCH * (int)sizeof(double);
+constexpr int OZ_CTILE_BYTES = OZ_BM * OZ_CPITCH * (int)sizeof(double);  // 132096
 constexpr int OZ_NONFINITE = 0x7fffffff;    // exponent marking a row with Inf / NaN
 
 constexpr long long kOzDefaultBudget = 4000000000LL;  // clock cycles (~2 s)
 constexpr int OZ_SMEM_LIMIT = 232448 - 64;  // opt-in shared memory per CTA, less static
-constexpr int OZ_BAR_BYTES = (2 * OZ_MAX_STAGES + 3) * 8 + 8;
+constexpr int OZ_BAR_BYTES = (2 * OZ_MAX_STAGES + 4) * 8 + 8;
 
 struct OzParams {
     int m;             // rows (= columns) of C
@@ -92,7 +93,7 @@ struct OzParams {
 };
 
 // Instruction descriptor, kind::i8: signed A and B, int32 accumulator, both
-// K-major, M = 128, N = 64.
+// K-major, M = 128, N = 128.
 constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) |
                               ((uint32_t)(OZ_BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
 __device__ __forceinline__ uint32_t idesc_i8(int, int) { return kIdescI8; }
@@ -127,6 +128,26 @@ __device__ __forceinline__ bool oz_tile(long long t, const OzParams &p, int &row
 
 __device__ __forceinline__ void oz_fail(int *info) { atomicCAS(info, 0, FMLB_ETIMEDOUT); }
 
+// First tile t' >= t of this CTA's sequence (stride gridDim.x) inside C, or ntiles.
+__device__ __forceinline__ long long oz_next_tile(long long t, const OzParams &p, int &row0,
+                                                  int &col0) {
+    for (; t < p.ntiles; t += gridDim.x)
+        if (oz_tile(t, p, row0, col0)) return t;
+    return p.ntiles;
+}
+
+// 8-byte asynchronous global -> shared copies (completion per thread).
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(tc::smem_u32(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 // Pass q0..q1 of the diagonals needs the digit planes 0..q1-1.
 __device__ __forceinline__ void oz_pass(const OzParams &p, int ps, int &q0, int &q1) {
     q0 = ps * OZ_PASS_Q;
@@ -142,12 +163,12 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapLo, const __grid_consta
         (reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~(uintptr_t)1023);
     const int stage_bytes = p.ns * (OZ_A_PLANE + OZ_B_PLANE);  // B planes after ns A planes
     const int nst = p.stages;
-    double *stg_all = reinterpret_cast<double *>(smem + nst * stage_bytes);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + nst * stage_bytes + OZ_STAGE_STG);
+    double *cs = reinterpret_cast<double *>(smem + nst * stage_bytes);  // C tile, 128 x 129
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + nst * stage_bytes + OZ_CTILE_BYTES);
     uint64_t *full = bars, *empty = bars + OZ_MAX_STAGES;
     uint64_t *tmem_full = bars + 2 * OZ_MAX_STAGES, *tmem_empty = tmem_full + 1,
-             *mma_done = tmem_full + 2;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mma_done + 1);
+             *mma_done = tmem_full + 2, *epi_bar = tmem_full + 3;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(epi_bar + 1);
     __shared__ int abort_cta;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -160,6 +181,7 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapLo, const __grid_consta
         tc::mbar_init(tmem_full, 1);
         tc::mbar_init(tmem_empty, OZ_EPI_WARPS);
         tc::mbar_init(mma_done, 1);
+        tc::mbar_init(epi_bar, OZ_EPI_WARPS * 32);
         tc::mbar_fence_init();
     }
     __syncthreads();
@@ -256,24 +278,55 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapLo, const __grid_consta
         }
     } else {
         // --------------------------------------------------------------- epilogue
-        // Two warps per TMEM lane quarter, 64 columns (two chunks of 32) each.
-        // Per pass and chunk: drain the pass's accumulators into FP64 (Horner
-        // in 256), scale, and subtract from C through a shared-memory transpose
-        // (coalesced read-modify-write, the 16 rows' loads in flight at once).
-        // TMEM is released after the second chunk's drain, so the next pass's
-        // MMAs overlap that chunk's read-modify-write.
+        // C's tile is staged in shared memory (cs, rows of 129 doubles) by
+        // cp.async while the tile's first pass runs on the tensor cores, and
+        // written back once after its last pass, both with one coalesced row
+        // segment of 32 columns per warp instruction (element i * 256 + e of
+        // the tile for thread e). Two warps per TMEM lane quarter, 64 columns
+        // (two chunks of 32) each: per pass and chunk, drain the pass's
+        // accumulators into FP64 (Horner in 256), scale, and subtract from
+        // this lane's row of cs. TMEM is released after the second chunk's
+        // drain, so the next pass's MMAs overlap that chunk's arithmetic.
         const int qw = warp & 3;
         const int half = (warp - 2) >> 2;
-        double *stg = stg_all + (warp - 2) * 16 * OZ_PITCH;
+        const int e = threadIdx.x - 64;           // 0 .. 255
+        const int rl = qw * 32 + lane;            // this lane's row of the tile
+        double *csr = cs + rl * OZ_CPITCH;
         int lp = 0;
+        uint32_t nsync = 0;
         bool ok = true;
-        for (long long t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
-            int row0, col0;
-            if (!oz_tile(t, p, row0, col0)) continue;
-            const int grow = row0 + qw * 32 + lane;
+        // every epilogue thread arrives; bounded wait, so a warp that gave up
+        // cannot hold the others
+        auto epi_sync = [&]() -> bool {
+            tc::mbar_arrive(epi_bar);
+            const bool r = tc::mbar_wait(epi_bar, nsync & 1, budget);
+            ++nsync;
+            return r;
+        };
+        auto tile_elem = [&](int i, int r0, int c0, int &r, int &c, size_t &g) -> bool {
+            const int idx = i * (OZ_EPI_WARPS * 32) + e;
+            r = idx >> 7;
+            c = idx & (OZ_BN - 1);
+            const int gr = r0 + r, gc = c0 + c;
+            g = (size_t)gr * p.ldc + gc;
+            return gr < p.m && gc <= gr && (p.strip_cols == 0 || gc < p.strip_cols);
+        };
+        auto prefetch = [&](int r0, int c0) {
+            for (int i = 0; i < OZ_BM * OZ_BN / (OZ_EPI_WARPS * 32); ++i) {
+                int r, c;
+                size_t g;
+                if (tile_elem(i, r0, c0, r, c, g)) cp_async8(cs + r * OZ_CPITCH + c, C + g);
+            }
+            cp_async_commit();
+        };
+        int row0 = 0, col0 = 0;
+        long long t = oz_next_tile(blockIdx.x, p, row0, col0);
+        if (t < p.ntiles) prefetch(row0, col0);
+        while (t < p.ntiles && ok) {
+            const int grow = row0 + rl;
             const int er = grow < p.m ? exps[p.p_row0 + grow] : 0;
             const double sr = grow < p.m ? rsum[p.p_row0 + grow] : 0.0;
-            for (int ps = 0; ps < p.npass; ++ps, ++lp) {
+            for (int ps = 0; ps < p.npass && ok; ++ps, ++lp) {
                 int q0, q1;
                 oz_pass(p, ps, q0, q1);
                 const bool last = ps == p.npass - 1;
@@ -285,6 +338,14 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapLo, const __grid_consta
                     break;
                 }
                 tc::fence_after_sync();
+                if (ps == 0) {  // the tile's C has landed in cs (every thread's copies)
+                    cp_async_wait_all();
+                    if (!epi_sync()) {
+                        oz_fail(info);
+                        ok = false;
+                        break;
+                    }
+                }
                 for (int cc = 0; cc < 2; ++cc) {
                     const int cb = half * 64 + cc * 32;  // chunk's first column in the tile
                     double acc[32];
@@ -316,43 +377,28 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapLo, const __grid_consta
                         if (last)
                             core = __dadd_rn(__dadd_rn(core, __dmul_rn(p.zp_c, __dadd_rn(sr, sc))),
                                              p.zp_kc2);
-                        acc[j] = (er == OZ_NONFINITE || ec == OZ_NONFINITE)
-                                     ? __longlong_as_double(0x7ff8000000000000LL)
-                                     : ldexp(core, er + ec + 2);
-                    }
-#pragma unroll 1
-                    for (int hh = 0; hh < 2; ++hh) {
-                        const int c = col0 + cb + lane;
-                        const int rb = row0 + qw * 32 + hh * 16;
-                        if ((lane >> 4) == hh) {
-#pragma unroll
-                            for (int j = 0; j < 32; ++j) stg[(lane & 15) * OZ_PITCH + j] = acc[j];
-                        }
-                        __syncwarp();
-                        // eight rows' C values are loaded first, all in flight at once
-#pragma unroll
-                        for (int g = 0; g < 16; g += 8) {
-                            double cv[8];
-#pragma unroll
-                            for (int rr = 0; rr < 8; ++rr) {
-                                const int r = rb + g + rr;
-                                const bool in = r < p.m && c < p.m && c <= r &&
-                                                (p.strip_cols == 0 || c < p.strip_cols);
-                                cv[rr] = in ? C[(size_t)r * p.ldc + c] : 0.0;
-                            }
-#pragma unroll
-                            for (int rr = 0; rr < 8; ++rr) {
-                                const int r = rb + g + rr;
-                                if (r < p.m && c < p.m && c <= r &&
-                                    (p.strip_cols == 0 || c < p.strip_cols))
-                                    C[(size_t)r * p.ldc + c] = cv[rr] - stg[(g + rr) * OZ_PITCH + lane];
-                            }
-                        }
-                        __syncwarp();
+                        const double v = (er == OZ_NONFINITE || ec == OZ_NONFINITE)
+                                             ? __longlong_as_double(0x7ff8000000000000LL)
+                                             : ldexp(core, er + ec + 2);
+                        csr[cb + j] = __dsub_rn(csr[cb + j], v);
                     }
                 }
             }
+            if (!ok) break;
+            if (!epi_sync()) {  // every pass's subtraction is in cs
+                oz_fail(info);
+                break;
+            }
+            for (int i = 0; i < OZ_BM * OZ_BN / (OZ_EPI_WARPS * 32); ++i) {
+                int r, c;
+                size_t g;
+                if (tile_elem(i, row0, col0, r, c, g)) C[g] = cs[r * OZ_CPITCH + c];
+            }
+            // the next tile's C into the elements this thread has just written back
+            t = oz_next_tile(t + gridDim.x, p, row0, col0);
+            if (t < p.ntiles) prefetch(row0, col0);
         }
+        cp_async_wait_all();  // no copy lands after the CTA has left
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -474,15 +520,16 @@ int make_plane_map(CUtensorMap *map, const int8_t *base, int rows, long long ldp
 }
 
 // Deepest operand ring (<= OZ_MAX_STAGES) whose shared memory fits a CTA.
+// (two stages at 6 planes, one at 7 or 8 beside the 129 KB C tile).
 int oz_stages(int ns) {
     const int sb = ns * (OZ_A_PLANE + OZ_B_PLANE);
-    const int room = OZ_SMEM_LIMIT - OZ_STAGE_STG - OZ_BAR_BYTES - 1024;
-    return std::max(2, std::min(OZ_MAX_STAGES, room / sb));
+    const int room = OZ_SMEM_LIMIT - OZ_CTILE_BYTES - OZ_BAR_BYTES - 1024;
+    return std::max(1, std::min(OZ_MAX_STAGES, room / sb));
 }
 
 size_t oz_smem_bytes(int ns) {
-    return (size_t)oz_stages(ns) * ns * (OZ_A_PLANE + OZ_B_PLANE) + OZ_STAGE_STG + OZ_BAR_BYTES +
-           1024;
+    return (size_t)oz_stages(ns) * ns * (OZ_A_PLANE + OZ_B_PLANE) + OZ_CTILE_BYTES +
+           OZ_BAR_BYTES + 1024;
 }
 
 thread_local tc::TestHooks t_hooks = {0, 0};
