@@ -49,6 +49,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstring>
 
 #include "common.cuh"
 #include "ozaki.cuh"
@@ -58,7 +59,16 @@ namespace fmlb {
 namespace {
 
 constexpr int OZ_BM = 128, OZ_BN = 128;
-constexpr int OZ_PASS_Q = 4;      // diagonals (accumulators of 128 columns) per pass
+#ifndef OZ_PASS_DIAGONALS
+#define OZ_PASS_DIAGONALS 4
+#endif
+// Diagonals (int32 accumulators of 128 columns) per pass, and the TMEM buffers
+// the 512 columns hold: with two, a pass's MMAs run while the epilogue drains
+// the previous pass.
+constexpr int OZ_PASS_Q = OZ_PASS_DIAGONALS;
+constexpr int OZ_TMEM_BUFS = 4 / OZ_PASS_Q;
+constexpr int OZ_MAX_PASSES = (8 + OZ_PASS_Q - 1) / OZ_PASS_Q;
+static_assert(OZ_PASS_Q == 2 || OZ_PASS_Q == 4, "passes of 2 or 4 diagonals");
 constexpr int OZ_KB = 32;          // int8 k values (bytes) per stage: one MMA K step
 constexpr int OZ_MAX_STAGES = 8;  // the ring depth is set per launch from shared memory
 constexpr int OZ_THREADS = 320;    // 10 warps
@@ -69,11 +79,13 @@ constexpr int OZ_CPITCH = OZ_BN + 1;  // doubles per row of the staged C tile (o
 constexpr int OZ_A_PLANE = OZ_BM * OZ_KB;   // 4096 bytes per A digit plane per stage
 constexpr int OZ_B_PLANE = OZ_BN * OZ_KB;   // 4096
 constexpr int OZ_CTILE_BYTES = OZ_BM * OZ_CPITCH * (int)sizeof(double);  // 132096
+constexpr int OZ_COLF_BYTES = OZ_BN * (int)sizeof(double);
+constexpr int OZ_ALIGN = 256;  // shared-memory base: the 32-byte swizzle atom
 constexpr int OZ_NONFINITE = 0x7fffffff;    // exponent marking a row with Inf / NaN
 
 constexpr long long kOzDefaultBudget = 4000000000LL;  // clock cycles (~2 s)
 constexpr int OZ_SMEM_LIMIT = 232448 - 64;  // opt-in shared memory per CTA, less static
-constexpr int OZ_BAR_BYTES = (2 * OZ_MAX_STAGES + 4) * 8 + 8;
+constexpr int OZ_BAR_BYTES = (2 * OZ_MAX_STAGES + 2 * OZ_TMEM_BUFS + 2) * 8 + 8;
 
 struct OzParams {
     int m;             // rows (= columns) of C
@@ -85,11 +97,16 @@ struct OzParams {
     long long ntiles;
     long long ldc;
     int exp_bias;      // -8 (ns + 1)
-    int npass;         // 1 (ns <= 4) or 2: diagonals [0, 4) then [4, ns)
+    int npass;         // passes: diagonals [0, Q), [Q, 2Q), ... [.., ns)
     double zp_c;       // c' (zero point of the digit planes)
     double zp_kc2;     // kp c'^2
     int skip_loads;    // test hook: the producer issues no copies
     int stages;        // depth of the operand ring
+};
+
+// Tensor maps of the digit planes, one per pass (boxes of that pass's planes).
+struct OzMaps {
+    CUtensorMap m[OZ_MAX_PASSES];
 };
 
 // Instruction descriptor, kind::i8: signed A and B, int32 accumulator, both
@@ -128,6 +145,12 @@ __device__ __forceinline__ bool oz_tile(long long t, const OzParams &p, int &row
 
 __device__ __forceinline__ void oz_fail(int *info) { atomicCAS(info, 0, FMLB_ETIMEDOUT); }
 
+// 2^(e + 1) for a row or column exponent in [-500, 500] (the scaled product
+// core * 2^(e_r+1) * 2^(e_c+1) then equals ldexp(core, e_r + e_c + 2)), else 0.
+__device__ __forceinline__ double oz_pow2_factor(int e) {
+    return (e >= -500 && e <= 500) ? __longlong_as_double((long long)(e + 1 + 1023) << 52) : 0.0;
+}
+
 // First tile t' >= t of this CTA's sequence (stride gridDim.x) inside C, or ntiles.
 __device__ __forceinline__ long long oz_next_tile(long long t, const OzParams &p, int &row0,
                                                   int &col0) {
@@ -155,19 +178,23 @@ __device__ __forceinline__ void oz_pass(const OzParams &p, int ps, int &q0, int 
 }
 
 __global__ void __launch_bounds__(OZ_THREADS, 1)
-ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapLo, const __grid_constant__ CUtensorMap mapHi,
+ozaki_syrk_kernel(const __grid_constant__ OzMaps maps,
                   const int *__restrict__ exps, const double *__restrict__ rsum, OzParams p,
                   double *__restrict__ C, int *__restrict__ info, long long budget) {
     extern __shared__ uint8_t oz_smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
-        (reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~(uintptr_t)1023);
+        (reinterpret_cast<uintptr_t>(oz_smem_raw) + OZ_ALIGN - 1) & ~(uintptr_t)(OZ_ALIGN - 1));
     const int stage_bytes = p.ns * (OZ_A_PLANE + OZ_B_PLANE);  // B planes after ns A planes
     const int nst = p.stages;
-    double *cs = reinterpret_cast<double *>(smem + nst * stage_bytes);  // C tile, 128 x 129
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + nst * stage_bytes + OZ_CTILE_BYTES);
+    // C tile, 128 x 129: column 128 holds the tile's column digit sums S_c
+    double *cs = reinterpret_cast<double *>(smem + nst * stage_bytes);
+    // 2^(e_c + 1) per column of the tile, 0 where the exact scaling needs ldexp
+    double *colf = reinterpret_cast<double *>(smem + nst * stage_bytes + OZ_CTILE_BYTES);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + nst * stage_bytes + OZ_CTILE_BYTES +
+                                                  OZ_COLF_BYTES);
     uint64_t *full = bars, *empty = bars + OZ_MAX_STAGES;
-    uint64_t *tmem_full = bars + 2 * OZ_MAX_STAGES, *tmem_empty = tmem_full + 1,
-             *mma_done = tmem_full + 2, *epi_bar = tmem_full + 3;
+    uint64_t *tmem_full = bars + 2 * OZ_MAX_STAGES, *tmem_empty = tmem_full + OZ_TMEM_BUFS,
+             *mma_done = tmem_empty + OZ_TMEM_BUFS, *epi_bar = mma_done + 1;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(epi_bar + 1);
     __shared__ int abort_cta;
 
@@ -178,8 +205,10 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapLo, const __grid_consta
             tc::mbar_init(&full[s], 1);
             tc::mbar_init(&empty[s], 1);
         }
-        tc::mbar_init(tmem_full, 1);
-        tc::mbar_init(tmem_empty, OZ_EPI_WARPS);
+        for (int b = 0; b < OZ_TMEM_BUFS; ++b) {
+            tc::mbar_init(&tmem_full[b], 1);
+            tc::mbar_init(&tmem_empty[b], OZ_EPI_WARPS);
+        }
         tc::mbar_init(mma_done, 1);
         tc::mbar_init(epi_bar, OZ_EPI_WARPS * 32);
         tc::mbar_fence_init();
@@ -203,7 +232,7 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapLo, const __grid_consta
                 for (int ps = 0; ps < p.npass && ok; ++ps) {
                     int q0, q1;
                     oz_pass(p, ps, q0, q1);
-                    const CUtensorMap *map = q1 == p.ns ? &mapHi : &mapLo;  // q1 planes
+                    const CUtensorMap *map = &maps.m[ps];  // boxes of q1 planes
                     for (int kb = 0; kb < p.nkb && !p.skip_loads; ++kb, ++issued) {
                         const int st = (int)(issued % nst);
                         const uint32_t ph = (uint32_t)((issued / nst) & 1);
@@ -237,7 +266,9 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapLo, const __grid_consta
                 for (int ps = 0; ps < p.npass; ++ps, ++lp) {
                     int q0, q1;
                     oz_pass(p, ps, q0, q1);
-                    if (!tc::mbar_wait(tmem_empty, (uint32_t)((lp & 1) ^ 1), budget)) {
+                    const int buf = lp % OZ_TMEM_BUFS;
+                    if (!tc::mbar_wait(&tmem_empty[buf], (uint32_t)(((lp / OZ_TMEM_BUFS) & 1) ^ 1),
+                                       budget)) {
                         oz_fail(info);
                         ok = false;
                         break;
@@ -257,7 +288,8 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapLo, const __grid_consta
                         const uint64_t da = tc::smem_desc_kmajor(sa, OZ_KB);
                         const uint64_t db = tc::smem_desc_kmajor(sb, OZ_KB);
                         for (int q = q0; q < q1; ++q) {
-                            const uint32_t dacc = tmem_base + (uint32_t)((q - q0) * OZ_BN);
+                            const uint32_t dacc =
+                                tmem_base + (uint32_t)((buf * OZ_PASS_Q + q - q0) * OZ_BN);
                             for (int a = 0; a <= q; ++a) {
                                 const int b = q - a;
                                 // plane offsets in 16-byte units of the descriptor address
@@ -269,7 +301,7 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapLo, const __grid_consta
                         tc::mma_commit(&empty[st]);  // frees the stage once these MMAs finish
                     }
                     if (!ok) break;
-                    tc::mma_commit(tmem_full);
+                    tc::mma_commit(&tmem_full[buf]);
                 }
             }
             // every MMA issued has finished before TMEM is released
@@ -326,13 +358,21 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapLo, const __grid_consta
             const int grow = row0 + rl;
             const int er = grow < p.m ? exps[p.p_row0 + grow] : 0;
             const double sr = grow < p.m ? rsum[p.p_row0 + grow] : 0.0;
+            const double rowf = oz_pow2_factor(er);
+            if (e < OZ_BN) {  // the tile's column data; read after the tile-start barrier
+                const int gc = col0 + e;
+                const int ec = gc < p.m ? exps[p.p_row0 + gc] : 0;
+                colf[e] = oz_pow2_factor(ec);
+                cs[e * OZ_CPITCH + OZ_BN] = gc < p.m ? rsum[p.p_row0 + gc] : 0.0;
+            }
             for (int ps = 0; ps < p.npass && ok; ++ps, ++lp) {
                 int q0, q1;
                 oz_pass(p, ps, q0, q1);
                 const bool last = ps == p.npass - 1;
-                // the first of two passes holds the top diagonals, scaled by 256^-5
-                const int bias = last ? p.exp_bias : -8 * (OZ_PASS_Q + 1);
-                if (!tc::mbar_wait(tmem_full, (uint32_t)(lp & 1), budget)) {
+                // Horner over diagonals q0 .. q1-1 carries 256^(q1-1-q): scale by 256^-(q1+1)
+                const double pbias = __longlong_as_double((long long)(1023 - 8 * (q1 + 1)) << 52);
+                const int buf = lp % OZ_TMEM_BUFS;
+                if (!tc::mbar_wait(&tmem_full[buf], (uint32_t)((lp / OZ_TMEM_BUFS) & 1), budget)) {
                     oz_fail(info);
                     ok = false;
                     break;
@@ -354,7 +394,7 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapLo, const __grid_consta
                     for (int q = q0; q < q1; ++q) {
                         uint32_t v[32];
                         tc::tmem_ld32(tmem_base + ((uint32_t)(qw * 32) << 16) +
-                                          (uint32_t)((q - q0) * OZ_BN + cb), v);
+                                          (uint32_t)((buf * OZ_PASS_Q + q - q0) * OZ_BN + cb), v);
 #pragma unroll
                         for (int j = 0; j < 32; ++j)
                             acc[j] = fma(acc[j], 256.0, (double)(int)v[j]);
@@ -362,24 +402,31 @@ ozaki_syrk_kernel(const __grid_constant__ CUtensorMap mapLo, const __grid_consta
                     if (cc == 1) {
                         tc::fence_before_sync();
                         __syncwarp();
-                        if (lane == 0) tc::mbar_arrive(tmem_empty);  // the next pass may start
+                        if (lane == 0) tc::mbar_arrive(&tmem_empty[buf]);  // the buffer is free
                     }
-                    // last pass: (acc 256^-(s+1) + c' (S_r + S_c) + k c'^2) 2^(e_r + e_c + 2);
-                    // first of two: acc 256^-5 2^(e_r + e_c + 2); fixed order, no contraction
-                    const int gcl = col0 + cb + lane;
-                    const int ecl = gcl < p.m ? exps[p.p_row0 + gcl] : 0;
-                    const double scl = gcl < p.m ? rsum[p.p_row0 + gcl] : 0.0;
+                    // last pass: (acc 256^-(s+1) + c' (S_r + S_c) + k c'^2) 2^(e_r + e_c + 2),
+                    // earlier passes: acc 256^-(q1+1) 2^(e_r + e_c + 2); fixed order, no
+                    // contraction. Both power-of-two scalings are exact multiplications
+                    // (core * 2^(e_r+1) is normal), so the result is ldexp's, rounded once.
 #pragma unroll
                     for (int j = 0; j < 32; ++j) {
-                        const int ec = __shfl_sync(0xffffffffu, ecl, j);
-                        const double sc = __shfl_sync(0xffffffffu, scl, j);
-                        double core = ldexp(acc[j], bias);
+                        const double f = colf[cb + j];
+                        double core = __dmul_rn(acc[j], pbias);
                         if (last)
-                            core = __dadd_rn(__dadd_rn(core, __dmul_rn(p.zp_c, __dadd_rn(sr, sc))),
-                                             p.zp_kc2);
-                        const double v = (er == OZ_NONFINITE || ec == OZ_NONFINITE)
-                                             ? __longlong_as_double(0x7ff8000000000000LL)
-                                             : ldexp(core, er + ec + 2);
+                            core = __dadd_rn(
+                                __dadd_rn(core, __dmul_rn(p.zp_c,
+                                                          __dadd_rn(sr, cs[(cb + j) * OZ_CPITCH + OZ_BN]))),
+                                p.zp_kc2);
+                        double v;
+                        if (rowf != 0.0 && f != 0.0) {
+                            v = __dmul_rn(__dmul_rn(core, rowf), f);
+                        } else {  // a non-finite row or column, or an exponent outside +-500
+                            const int gc = col0 + cb + j;
+                            const int ec = gc < p.m ? exps[p.p_row0 + gc] : 0;
+                            v = (er == OZ_NONFINITE || ec == OZ_NONFINITE)
+                                    ? __longlong_as_double(0x7ff8000000000000LL)
+                                    : ldexp(core, er + ec + 2);
+                        }
                         csr[cb + j] = __dsub_rn(csr[cb + j], v);
                     }
                 }
@@ -523,13 +570,13 @@ int make_plane_map(CUtensorMap *map, const int8_t *base, int rows, long long ldp
 // (two stages at 6 planes, one at 7 or 8 beside the 129 KB C tile).
 int oz_stages(int ns) {
     const int sb = ns * (OZ_A_PLANE + OZ_B_PLANE);
-    const int room = OZ_SMEM_LIMIT - OZ_CTILE_BYTES - OZ_BAR_BYTES - 1024;
+    const int room = OZ_SMEM_LIMIT - OZ_CTILE_BYTES - OZ_COLF_BYTES - OZ_BAR_BYTES - OZ_ALIGN;
     return std::max(1, std::min(OZ_MAX_STAGES, room / sb));
 }
 
 size_t oz_smem_bytes(int ns) {
     return (size_t)oz_stages(ns) * ns * (OZ_A_PLANE + OZ_B_PLANE) + OZ_CTILE_BYTES +
-           OZ_BAR_BYTES + 1024;
+           OZ_COLF_BYTES + OZ_BAR_BYTES + OZ_ALIGN;
 }
 
 thread_local tc::TestHooks t_hooks = {0, 0};
@@ -558,12 +605,14 @@ int ozaki_syrk(double *C, long long ldc, int m, const OzakiSlices &s, int p_row0
     FMLB_REQUIRE(s.ns >= 1 && s.ns <= OZAKI_MAX_SLICES, "ozaki: 1..%d slices", OZAKI_MAX_SLICES);
     FMLB_REQUIRE(s.kp % OZ_KB == 0 && s.kp <= 8192, "ozaki: k must be a multiple of 32, <= 8192");
     FMLB_REQUIRE(p_row0 >= 0 && p_row0 + m <= s.rows, "ozaki: rows outside the slice buffer");
-    // boxes of 128 rows and the planes a pass reads: min(ns, 4) for the first
-    // of two passes, all ns for the last
-    CUtensorMap mLo, mHi;
-    FMLB_TRY(make_plane_map(&mLo, s.planes, s.rows, s.ldpl, s.kp, s.pstride,
-                            std::min(s.ns, OZ_PASS_Q), OZ_BM));
-    FMLB_TRY(make_plane_map(&mHi, s.planes, s.rows, s.ldpl, s.kp, s.pstride, s.ns, OZ_BM));
+    // boxes of 128 rows and the planes each pass reads (planes 0 .. q1-1 for
+    // its last diagonal q1-1)
+    OzMaps maps;
+    memset(&maps, 0, sizeof maps);
+    const int npass = (s.ns + OZ_PASS_Q - 1) / OZ_PASS_Q;
+    for (int ps = 0; ps < npass; ++ps)
+        FMLB_TRY(make_plane_map(&maps.m[ps], s.planes, s.rows, s.ldpl, s.kp, s.pstride,
+                                std::min(s.ns, (ps + 1) * OZ_PASS_Q), OZ_BM));
     OzParams p;
     p.m = m;
     p.p_row0 = p_row0;
@@ -573,7 +622,7 @@ int ozaki_syrk(double *C, long long ldc, int m, const OzakiSlices &s, int p_row0
     const long long Tr = ceil_div(m, OZ_BM);
     p.strip_tiles = p.strip_cols > 0 ? ceil_div(p.strip_cols, OZ_BN) : 0;
     p.ntiles = p.strip_tiles ? Tr * p.strip_tiles : Tr * (Tr + 1) / 2;
-    p.npass = s.ns > OZ_PASS_Q ? 2 : 1;
+    p.npass = npass;
     p.ldc = ldc;
     p.exp_bias = -8 * (s.ns + 1);
     double zc = ldexp(1.0, -8 * s.ns - 1);  // half an ulp of the last digit
@@ -599,7 +648,7 @@ int ozaki_syrk(double *C, long long ldc, int m, const OzakiSlices &s, int p_row0
     // held every SM until the update ended and serialised the lookahead)
     const int grid = (int)std::min<long long>(
         p.ntiles, std::max<long long>(sm_count(), (p.ntiles + 3) / 4));
-    ozaki_syrk_kernel<<<grid, OZ_THREADS, smem, st>>>(mLo, mHi, s.exps, s.rsum, p, C, info,
+    ozaki_syrk_kernel<<<grid, OZ_THREADS, smem, st>>>(maps, s.exps, s.rsum, p, C, info,
                                                        hooks.wait_budget);
     return launch_status("ozaki_syrk_kernel");
 }
