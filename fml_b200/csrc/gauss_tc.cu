@@ -68,12 +68,25 @@ struct TcParams {
     int tma_store;           // K is written by TMA bulk-tensor stores (aligned K)
 };
 
+// L2 policies: the BF16 operands (re-read by every tile of their row / column
+// block) are kept, the K boxes (written once) are evicted first.
+__device__ __forceinline__ uint64_t l2_evict_last() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ uint64_t l2_evict_first() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(pol));
+    return pol;
+}
+
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar,
-                                            int x, int y) {
+                                            int x, int y, uint64_t pol) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%3, %4}], [%2];\n" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        ".L2::cache_hint [%0], [%1, {%3, %4}], [%2], %5;\n" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "l"(pol)
         : "memory");
 }
 
@@ -105,11 +118,11 @@ __device__ __forceinline__ void tile_coords(int t, const TcParams &p, int &ta, i
 
 // 3-D tiled TMA store of a shared-memory box (bulk async-group completion).
 __device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, const void *src, int x, int y,
-                                             int z) {
+                                             int z, uint64_t pol) {
     asm volatile(
-        "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];\n" ::"l"(
-            reinterpret_cast<uint64_t>(map)),
-        "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z)
+        "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group.L2::cache_hint"
+        " [%0, {%2, %3, %4}], [%1], %5;\n" ::"l"(reinterpret_cast<uint64_t>(map)),
+        "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z), "l"(pol)
         : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n"); }
@@ -133,7 +146,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 gauss_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constant__ CUtensorMap mapAlo,
                 const __grid_constant__ CUtensorMap mapBhi, const __grid_constant__ CUtensorMap mapBlo,
                 const __grid_constant__ CUtensorMap mapK, const float *__restrict__ normA,
-                const float *__restrict__ normB, TcParams p, float *__restrict__ K,
+                const float *__restrict__ normB, const __grid_constant__ TcParams p,
+                float *__restrict__ K,
                 int *__restrict__ status) {
     extern __shared__ uint8_t tc_smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -171,6 +185,7 @@ gauss_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constan
     if (warp == 0) {
         // ------------------------------------------------------------ producer
         if (lane == 0) {
+            const uint64_t keep = l2_evict_last();
             long long issued = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok && !p.skip_loads; t += gridDim.x) {
@@ -186,12 +201,13 @@ gauss_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constan
                     }
                     uint8_t *st = smem + stage * TC_STAGE_BYTES;
                     mbar_arrive_expect_tx(&full[stage], TC_STAGE_BYTES);
-                    tma_load_2d(st, &mapAhi, &full[stage], kc * TC_BK, ta * TC_BM);
-                    tma_load_2d(st + TC_TILE_BYTES, &mapAlo, &full[stage], kc * TC_BK, ta * TC_BM);
+                    tma_load_2d(st, &mapAhi, &full[stage], kc * TC_BK, ta * TC_BM, keep);
+                    tma_load_2d(st + TC_TILE_BYTES, &mapAlo, &full[stage], kc * TC_BK, ta * TC_BM,
+                                keep);
                     tma_load_2d(st + 2 * TC_TILE_BYTES, &mapBhi, &full[stage], kc * TC_BK,
-                                tb * TC_BN);
+                                tb * TC_BN, keep);
                     tma_load_2d(st + 3 * TC_TILE_BYTES, &mapBlo, &full[stage], kc * TC_BK,
-                                tb * TC_BN);
+                                tb * TC_BN, keep);
                 }
             }
             // every copy this thread issued has landed before the CTA winds down
@@ -257,6 +273,7 @@ gauss_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constan
         const int half = (warp - 2) >> 2;
         float *stg = stg_all + (warp - 2) * TC_WARP_STG;  // 1024-byte aligned boxes
         float *dbox = stg, *mbox = stg + TC_BOX_FLOATS;
+        const uint64_t stream_out = l2_evict_first();
         int lt = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++lt) {
             int ta, tb;
@@ -322,9 +339,10 @@ gauss_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constan
                         fence_proxy_async();
                         __syncwarp();
                         if (lane == 0) {  // boxes wholly outside K are not issued
-                            if (row0 < p.na && cb < p.nb) tma_store_3d(&mapK, dbox, cb, row0, s);
+                            if (row0 < p.na && cb < p.nb)
+                                tma_store_3d(&mapK, dbox, cb, row0, s, stream_out);
                             if (p.symmetric && row0 < p.nb && cb < p.na)
-                                tma_store_3d(&mapK, mbox, row0, cb, s);
+                                tma_store_3d(&mapK, mbox, row0, cb, s, stream_out);
                             bulk_commit();
                         }
                     } else {
@@ -390,14 +408,27 @@ __global__ void split_center_kernel(const double *__restrict__ X, int n, int ldx
     }
 }
 
-// column means of X (n rows), one thread per column
-__global__ void column_mean_kernel(const double *__restrict__ X, int n, int ldx, int d,
-                                   double *__restrict__ mu) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= d) return;
+// column means of X (n rows): a CTA per 32 columns, 32 row groups of one warp
+// each (row r to group r mod 32, coalesced 32-column segments), the groups'
+// partial sums combined by a fixed shared-memory tree
+constexpr int CM_ROWG = 32;
+__global__ void __launch_bounds__(32 * CM_ROWG)
+column_mean_kernel(const double *__restrict__ X, int n, int ldx, int d, double *__restrict__ mu) {
+    __shared__ double part[CM_ROWG][33];
+    const int c = threadIdx.x, g = threadIdx.y;
+    const int k = blockIdx.x * 32 + c;
     double s = 0.0;
-    for (int i = 0; i < n; ++i) s += X[(size_t)i * ldx + k];
-    mu[k] = n ? s / n : 0.0;
+    if (k < d) {
+#pragma unroll 8
+        for (int i = g; i < n; i += CM_ROWG) s += X[(size_t)i * ldx + k];
+    }
+    part[g][c] = s;
+    __syncthreads();
+    for (int h = CM_ROWG / 2; h > 0; h >>= 1) {
+        if (g < h) part[g][c] += part[g + h][c];
+        __syncthreads();
+    }
+    if (g == 0 && k < d) mu[k] = n ? part[0][c] / n : 0.0;
 }
 
 // ---- host: tensor maps --------------------------------------------------------
@@ -459,7 +490,8 @@ extern "C" int fmlb_column_mean_f64(const double *X, int n, int ldx, int d, doub
                                     void *stream) {
     using namespace fmlb;
     FMLB_REQUIRE(n >= 0 && d >= 1 && ldx >= d && mu, "fmlb_column_mean_f64: bad arguments");
-    column_mean_kernel<<<ceil_div(d, 128), 128, 0, FMLB_STREAM(stream)>>>(X, n, ldx, d, mu);
+    column_mean_kernel<<<ceil_div(d, 32), dim3(32, CM_ROWG), 0, FMLB_STREAM(stream)>>>(X, n, ldx,
+                                                                                  d, mu);
     return launch_status("column_mean_kernel");
 }
 

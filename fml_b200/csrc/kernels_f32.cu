@@ -5,9 +5,11 @@
 //
 // CUDA-core kernel (the L1 distance is not a contraction): 128 x 128 output
 // tile per 256-thread CTA, FP64 descriptors converted to FP32 while staged
-// through shared memory in k-chunks of 32, 8 x 8 outputs per thread (2 FP32
-// instructions per term; operands fetched as float4), every sigma emitted
-// from one pass. The next k-chunk's global loads are issued into registers
+// through shared memory in k-chunks of 32 (the row operand negated), 8 x 8
+// outputs per thread as 8 x 4 column pairs in packed FP32x2 arithmetic
+// (b - a and the abs-add, two terms per instruction; operands fetched as
+// float4), every sigma emitted from one pass. b + (-a) is a - b negated
+// exactly, so the sums equal the scalar |a - b| accumulation bit for bit. The next k-chunk's global loads are issued into registers
 // before the current chunk is computed, so their latency hides under the
 // arithmetic. Symmetric builds compute the tiles on or below the diagonal and
 // write the mirror through a shared-memory transpose.
@@ -29,7 +31,8 @@ struct LapScales {
 
 __global__ void __launch_bounds__(LTPB, 2)
 laplacian_f32_kernel(const double *__restrict__ A, int na, int lda, const double *__restrict__ B,
-                     int nb, int ldb, int d, LapScales sc, int nsig, float *__restrict__ K,
+                     int nb, int ldb, int d, const __grid_constant__ LapScales sc, int nsig,
+                     float *__restrict__ K,
                      long long ldk, long long sstride, int symmetric) {
     extern __shared__ float lap_smem[];
     float(*As)[LB + LPAD] = reinterpret_cast<float(*)[LB + LPAD]>(lap_smem);
@@ -50,11 +53,11 @@ laplacian_f32_kernel(const double *__restrict__ A, int na, int lda, const double
     const int row0 = by * LB, col0 = bx * LB;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
 
-    float acc[8][8];
+    float2 acc[8][4];
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+        for (int j = 0; j < 4; ++j) acc[i][j] = make_float2(0.0f, 0.0f);
 
     // loader: 32 consecutive k of one row per warp, 8 rows per pass; the
     // chunk is held in registers (converted) until the previous one is done
@@ -74,7 +77,7 @@ laplacian_f32_kernel(const double *__restrict__ A, int na, int lda, const double
     for (int k0 = 0; k0 < d; k0 += LK) {
 #pragma unroll
         for (int r = 0; r < LB / 8; ++r) {
-            As[lk][lr + 8 * r] = pa[r];
+            As[lk][lr + 8 * r] = -pa[r];
             Bs[lk][lr + 8 * r] = pb[r];
         }
         __syncthreads();
@@ -85,12 +88,18 @@ laplacian_f32_kernel(const double *__restrict__ A, int na, int lda, const double
             const float4 a1 = *reinterpret_cast<const float4 *>(&As[kk][ty * 8 + 4]);
             const float4 b0 = *reinterpret_cast<const float4 *>(&Bs[kk][tx * 8]);
             const float4 b1 = *reinterpret_cast<const float4 *>(&Bs[kk][tx * 8 + 4]);
-            const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-            const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+            const float na[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};  // -A
+            const float2 b2[4] = {make_float2(b0.x, b0.y), make_float2(b0.z, b0.w),
+                                  make_float2(b1.x, b1.y), make_float2(b1.z, b1.w)};
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
+            for (int i = 0; i < 8; ++i) {
+                const float2 na2 = make_float2(na[i], na[i]);
 #pragma unroll
-                for (int j = 0; j < 8; ++j) acc[i][j] += fabsf(a[i] - b[j]);
+                for (int j = 0; j < 4; ++j) {
+                    const float2 dd = __fadd2_rn(b2[j], na2);
+                    acc[i][j] = __fadd2_rn(acc[i][j], make_float2(fabsf(dd.x), fabsf(dd.y)));
+                }
+            }
         }
         __syncthreads();
     }
@@ -100,7 +109,10 @@ laplacian_f32_kernel(const double *__restrict__ A, int na, int lda, const double
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) T[ty * 8 + i][tx * 8 + j] = acc[i][j];
+        for (int j = 0; j < 4; ++j) {
+            T[ty * 8 + i][tx * 8 + 2 * j] = acc[i][j].x;
+            T[ty * 8 + i][tx * 8 + 2 * j + 1] = acc[i][j].y;
+        }
     __syncthreads();
     const bool mirror = symmetric && by > bx;
     for (int s = 0; s < nsig; ++s) {
