@@ -82,3 +82,55 @@ def test_ozaki_slices_needed_for_fp64_refined_accuracy(oracle_mod, cm_kernel_inp
     assert refined_residual(L6) <= 4 * r64
     L4 = _blocked_cholesky(A, 256, 4)
     assert L4 is None or refined_residual(L4) > 100 * r64
+
+
+def _pcg_iterations(A, L, y, tol=1e-10, cap=3000):
+    """Preconditioned CG on A x = y with M^-1 = (L L^T)^-1, L applied in FP64;
+    iterations until the recurrence residual is below tol * ||y||."""
+    import scipy.linalg as sl
+    x = np.zeros(len(y))
+    r = y.copy()
+    z = sl.cho_solve((L, True), r)
+    p = z.copy()
+    rz = r @ z
+    ny = np.linalg.norm(y)
+    it = 0
+    while np.linalg.norm(r) > tol * ny and it < cap:
+        Ap = A @ p
+        a = rz / (p @ Ap)
+        x += a * p
+        r -= a * Ap
+        z = sl.cho_solve((L, True), r)
+        rz_new = r @ z
+        p = z + (rz_new / rz) * p
+        rz = rz_new
+        it += 1
+    return it
+
+
+@pytest.mark.parametrize("sigma,min_between,min_iters", [(400.0, 100, 150), (1600.0, 300, 500)])
+def test_shifted_fp32_factor_is_a_weak_preconditioner(oracle_mod, cm_kernel_inputs, sigma,
+                                                      min_between, min_iters):
+    """The route around the FP32 breakdown: factor fl32(K + delta I) in FP32
+    with the smallest shift delta = 10^e lambda_max that spotrf accepts, and
+    use that factor to precondition CG on K + lambda I (FP64, lambda = 1e-8).
+    Every eigenvalue of K between lambda and delta is left unpreconditioned,
+    and at N = 1024 there are hundreds of them; PCG then needs hundreds of
+    iterations, each a full pass over K, to reach a 1e-10 residual (measured
+    295 at sigma 400, 1028 at sigma 1600), where the int8-emulated FP64 factor
+    needs two refinement steps."""
+    X = cm_kernel_inputs
+    K = oracle_mod.gaussian_kernel(X.T, X.T, sigma)
+    n, lam = len(K), 1e-8
+    ev = np.linalg.eigvalsh(K)
+    for e in range(-10, 1):
+        delta = 10.0 ** e * ev[-1]
+        L32, info = lapack.spotrf((K + delta * np.eye(n)).astype(np.float32), lower=1)
+        if info == 0:
+            break
+    assert info == 0
+    between = int(np.sum((ev > lam) & (ev < delta)))
+    y = synthetic.generate(1024, nmax=29, seed=2).energies
+    iters = _pcg_iterations(K + lam * np.eye(n), np.tril(L32).astype(np.float64), y)
+    assert between >= min_between
+    assert iters >= min_iters
