@@ -74,7 +74,9 @@ def parse():
     p.add_argument("--stages", nargs="?", const="all", default=None,
                    help="time each hot-path kernel on its own (one JSON line per stage); "
                         "'arad' times only the ARAD kernels, 'build' only the descriptors "
-                        "and kernel-matrix builds, 'factor' only the factorisations")
+                        "and kernel-matrix builds, 'factor' only the factorisations, "
+                        "'update' one int8 and one FP64 trailing update (m = --ntrain, "
+                        "k = 1024) on seeded normal data")
     p.add_argument("--workload", default="krr",
                    choices=["krr", "batched", "serving", "small", "arad"],
                    help="krr: the large-N KRR step (default, the headline line); batched: "
@@ -770,6 +772,8 @@ def run_stages(a):
         return run_arad_stage(a, torch, lib, st, P)
     if a.stages == "factor":
         return run_factor_stages(a, torch, lib, st, P, emit)
+    if a.stages == "update":
+        return run_update_stage(a, torch, lib, st, P, emit)
     # --- descriptors ---------------------------------------------------------
     b = synthetic.generate(40960, nmax=29, seed=2)
     z = torch.from_numpy(b.charges).to(dev)
@@ -901,6 +905,32 @@ def run_stages(a):
     del keep
     out += run_arad_stage(a, torch, lib, st, P)
     return out
+
+
+def run_update_stage(a, torch, lib, st, P, emit):
+    """One trailing update C -= P P^T (lower triangle) of each kind at
+    m = --ntrain, k = 1024, on a seeded normal panel and C: the int8 update
+    (--slices digit planes, the digit split included) and the FP64 one,
+    three launches each (the second is the one a profiler captures)."""
+    from fml_b200 import _lib
+    dev = torch.device("cuda", 0)
+    m, k = a.ntrain, 1024
+    g = torch.Generator(device=dev).manual_seed(a.seed)
+    Pm = torch.randn((m, k), dtype=torch.float64, device=dev, generator=g)
+    C = torch.randn((m, m), dtype=torch.float64, device=dev, generator=g)
+    ws = torch.empty(lib.fmlb_syrk_ozaki_workspace_bytes(m, k, a.slices), dtype=torch.uint8,
+                     device=dev)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    fl = 2.0 * k * m * (m + 1) / 2
+    ms = _time(torch, lambda: _lib.call("fmlb_syrk_lower_ozaki", P(C), m, m, P(Pm), k, k, 0,
+                                        a.slices, P(ws), ws.numel(), P(info), st), reps=2)
+    emit({"stage": "update_ozaki", "config": "m=%d, k=%d, %d digit planes" % (m, k, a.slices),
+          "ms": ms, "fp64_equivalent_tflops": fl / ms / 1e9,
+          "int8_tops": fl * a.slices * (a.slices + 1) / 2 / ms / 1e9, "info": int(info.item())})
+    ms = _time(torch, lambda: _lib.call("fmlb_syrk_lower_f64", P(C), m, m, P(Pm), k, k, 0, None,
+                                        st), reps=2)
+    emit({"stage": "update_fp64", "config": "m=%d, k=%d" % (m, k), "ms": ms,
+          "tflops": fl / ms / 1e9})
 
 
 def run_factor_stages(a, torch, lib, st, P, emit):
