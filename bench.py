@@ -983,6 +983,13 @@ def run_factor_stages(a, torch, lib, st, P, emit):
         emit({"stage": "potrf_" + name, "config": "N=%d, sigma=%g, lambda=%g" % (n, sig, a.lam),
               "ms": ms, "fp64_equivalent_tflops": fl / ms / 1e9, "dgemm_tflops": dgemm,
               "info": int(info.item())})
+    # the triangular solves with the FP64 factor (forward + backward, one right-hand side)
+    build()
+    _lib.call("fmlb_potrf_f64", P(K), n, n, P(w64), P(info), st)
+    x = torch.ones(n, dtype=torch.float64, device=dev)
+    ms = _time(torch, lambda: _lib.call("fmlb_potrs_f64", P(K), n, n, P(w64), P(x), st), reps=3)
+    emit({"stage": "potrs_f64", "config": "N=%d, 1 right-hand side" % n, "ms": ms,
+          "bound": "hbm (the factor is read twice)", "achieved_gbs": n * n * 8.0 / ms / 1e6})
     # one bulk update of each kind: C = K[1024:, 1024:], P = K[1024:, :1024]
     m, k = n - 1024, 1024
     Cv, Pv = K[1024:, 1024:], K[1024:, :1024]

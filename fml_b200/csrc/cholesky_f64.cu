@@ -44,8 +44,8 @@ __device__ __forceinline__ bool failed(const int *info) {
 // with the off-diagonal blocks kept (transposed) in the unused upper triangle.
 constexpr int LDL = NB + 1;
 constexpr int SB = 32, NSB = NB / SB, LDW = SB + 1;
-constexpr size_t kPotf2Smem = ((size_t)NB * LDL + (size_t)NSB * SB * LDW + SB * LDW) *
-                              sizeof(double);
+constexpr size_t kPotf2Smem =
+    ((size_t)NB * LDL + (size_t)NSB * SB * LDW + (size_t)(NSB - 1) * SB * LDW) * sizeof(double);
 
 // One warp factors the 32 x 32 diagonal sub-block at L[b0.., b0..] in place
 // (lane = row) and writes its inverse into W (row-major). Returns the 1-based
@@ -82,7 +82,9 @@ potf2_block_kernel(double *__restrict__ A, long long lda, int k0, int kn,
     extern __shared__ double potf2_smem[];
     double(*L)[LDL] = reinterpret_cast<double(*)[LDL]>(potf2_smem);
     double(*W)[SB][LDW] = reinterpret_cast<double(*)[SB][LDW]>(potf2_smem + NB * LDL);
-    double(*T)[LDW] = reinterpret_cast<double(*)[LDW]>(potf2_smem + NB * LDL + NSB * SB * LDW);
+    // T[J]: sum_{K=J}^{I-1} L_IK inv(L)_KJ for every J < I of one block row I
+    double(*T)[SB][LDW] =
+        reinterpret_cast<double(*)[SB][LDW]>(potf2_smem + NB * LDL + NSB * SB * LDW);
     __shared__ int bad;
     if (failed(info)) return;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -137,31 +139,30 @@ potf2_block_kernel(double *__restrict__ A, long long lda, int k0, int kn,
         const int r = t >> 7, c = t & (NB - 1);
         if (r < kn && c <= r) A[(size_t)(k0 + r) * lda + (k0 + c)] = L[r][c];
     }
-    // block inverse; inv(L)_IJ for I > J is stored transposed at L[b0J + c][b0I + r]
+    // block inverse; inv(L)_IJ for I > J is stored transposed at L[b0J + c][b0I + r].
+    // Block row I needs the rows before it only, so its J < I blocks are formed
+    // together: T[J] for every J, then inv(L)_IJ = -inv(L_II) T[J].
     for (int I = 1; I < NSB; ++I) {
-        for (int J = 0; J < I; ++J) {
-            // T = sum_{K=J}^{I-1} L_IK inv(L)_KJ
-            for (int t = tid; t < SB * SB; t += TPB) {
-                const int r = t >> 5, c = t & 31;
-                double sacc = 0.0;
-                for (int K = J; K < I; ++K) {
-                    for (int q = 0; q < SB; ++q) {
-                        const double lik = L[I * SB + r][K * SB + q];
-                        const double inv = (K == J) ? W[J][q][c] : L[J * SB + c][K * SB + q];
-                        sacc = fma(lik, inv, sacc);
-                    }
+        for (int t = tid; t < I * SB * SB; t += TPB) {
+            const int J = t / (SB * SB), r = (t >> 5) & 31, c = t & 31;
+            double sacc = 0.0;
+            for (int K = J; K < I; ++K) {
+                for (int q = 0; q < SB; ++q) {
+                    const double lik = L[I * SB + r][K * SB + q];
+                    const double inv = (K == J) ? W[J][q][c] : L[J * SB + c][K * SB + q];
+                    sacc = fma(lik, inv, sacc);
                 }
-                T[r][c] = sacc;
             }
-            __syncthreads();
-            for (int t = tid; t < SB * SB; t += TPB) {
-                const int r = t >> 5, c = t & 31;
-                double sacc = 0.0;
-                for (int q = 0; q <= r; ++q) sacc = fma(W[I][r][q], T[q][c], sacc);
-                L[J * SB + c][I * SB + r] = -sacc;
-            }
-            __syncthreads();
+            T[J][r][c] = sacc;
         }
+        __syncthreads();
+        for (int t = tid; t < I * SB * SB; t += TPB) {
+            const int J = t / (SB * SB), r = (t >> 5) & 31, c = t & 31;
+            double sacc = 0.0;
+            for (int q = 0; q <= r; ++q) sacc = fma(W[I][r][q], T[J][q][c], sacc);
+            L[J * SB + c][I * SB + r] = -sacc;
+        }
+        __syncthreads();
     }
     for (int t = tid; t < NB * NB; t += TPB) {
         const int r = t >> 7, c = t & (NB - 1);
