@@ -123,21 +123,33 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
-// Tile t -> (row0, col0): lower triangle of 128 x 128 tiles (row block `by`
-// holds column tiles 0 .. by), or the first strip_tiles column tiles of every
-// row block. False for tiles outside C.
+// Tile t -> (row0, col0) of the lower triangle of 128 x 128 tiles (row block
+// `by` holds column tiles 0 .. by), or of the first strip_tiles column tiles
+// of every row block. Tiles run in bands of OZ_BAND row blocks and, inside a
+// band, in groups of OZ_BAND column tiles (a 1024 x 1024 block of C), so the
+// ~148 tiles in flight at a time share their digit planes through L2. Band
+// b holds b + 1 groups below and on the diagonal. The enumeration covers a
+// superset of C; false for tiles outside C.
+constexpr int OZ_BAND = 8;
+constexpr int OZ_GROUP = OZ_BAND * OZ_BAND;  // tiles of a band x group block
 __device__ __forceinline__ bool oz_tile(long long t, const OzParams &p, int &row0, int &col0) {
     int by, bx;
     if (p.strip_tiles > 0) {
-        by = (int)(t / p.strip_tiles);
-        bx = (int)(t % p.strip_tiles);
-        if (bx > by) return false;
+        const int band = (int)(t / (OZ_BAND * p.strip_tiles));
+        const int w = (int)(t % (OZ_BAND * p.strip_tiles));
+        by = band * OZ_BAND + w / p.strip_tiles;
+        bx = w % p.strip_tiles;
     } else {
-        by = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-        while ((long long)by * (by + 1) / 2 > t) --by;
-        while ((long long)(by + 1) * (by + 2) / 2 <= t) ++by;
-        bx = (int)(t - (long long)by * (by + 1) / 2);
+        // bands before band b: OZ_GROUP b (b + 1) / 2 tiles
+        int b = (int)((sqrt(8.0 * (double)t / OZ_GROUP + 1.0) - 1.0) * 0.5);
+        while ((long long)OZ_GROUP * b * (b + 1) / 2 > t) --b;
+        while ((long long)OZ_GROUP * (b + 1) * (b + 2) / 2 <= t) ++b;
+        const int u = (int)(t - (long long)OZ_GROUP * b * (b + 1) / 2);
+        const int g = u / OZ_GROUP, w = u % OZ_GROUP;
+        by = b * OZ_BAND + w / OZ_BAND;
+        bx = g * OZ_BAND + w % OZ_BAND;
     }
+    if (bx > by) return false;
     row0 = by * OZ_BM;
     col0 = bx * OZ_BN;
     return row0 < p.m && col0 < p.m;
@@ -621,7 +633,9 @@ int ozaki_syrk(double *C, long long ldc, int m, const OzakiSlices &s, int p_row0
     p.strip_cols = strip_cols > 0 ? std::min(strip_cols, m) : 0;
     const long long Tr = ceil_div(m, OZ_BM);
     p.strip_tiles = p.strip_cols > 0 ? ceil_div(p.strip_cols, OZ_BN) : 0;
-    p.ntiles = p.strip_tiles ? Tr * p.strip_tiles : Tr * (Tr + 1) / 2;
+    const long long nband = ceil_div(Tr, OZ_BAND);
+    p.ntiles = p.strip_tiles ? nband * OZ_BAND * p.strip_tiles
+                             : (long long)OZ_GROUP * nband * (nband + 1) / 2;
     p.npass = npass;
     p.ldc = ldc;
     p.exp_bias = -8 * (s.ns + 1);
