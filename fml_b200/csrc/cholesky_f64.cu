@@ -48,35 +48,74 @@ constexpr size_t kPotf2Smem =
     ((size_t)NB * LDL + (size_t)NSB * SB * LDW + (size_t)(NSB - 1) * SB * LDW) * sizeof(double);
 
 // One warp factors the 32 x 32 diagonal sub-block at L[b0.., b0..] in place
-// (lane = row) and writes its inverse into W (row-major). Returns the 1-based
-// failing column or 0 (the same value in every lane).
+// and writes its inverse into W (row-major). Lane r holds row r of the block
+// in registers; the entries other lanes need come by shuffles. The column
+// steps are unrolled by template recursion, so every register index is a
+// constant. The arithmetic (order of the FMAs, reciprocal-multiply scaling,
+// the division in the substitution) is that of right-looking elimination
+// and forward substitution in shared memory, bit for bit.
+template <int J>
+struct WarpFactor32 {
+    __device__ __forceinline__ static void run(double (&a)[SB], int lane, int &fail) {
+        const double piv = __shfl_sync(0xffffffffu, a[J], J);
+        if (!(piv > 0.0) && !fail) fail = J + 1;  // later columns are NaN and not stored
+        const double r = sqrt(piv), inv = 1.0 / r;
+        if (lane == J) a[J] = r;
+        else if (lane > J) a[J] *= inv;
+        const double lij = a[J];
+#pragma unroll
+        for (int c = J + 1; c < SB; ++c) {
+            const double lcj = __shfl_sync(0xffffffffu, a[J], c);  // L[c][J]
+            if (c <= lane) a[c] = fma(-lij, lcj, a[c]);
+        }
+        WarpFactor32<J + 1>::run(a, lane, fail);
+    }
+};
+template <>
+struct WarpFactor32<SB> {
+    __device__ __forceinline__ static void run(double (&)[SB], int, int &) {}
+};
+// Column `lane` of the inverse by forward substitution: w[K] = W[K][lane].
+template <int K>
+struct WarpInverse32 {
+    __device__ __forceinline__ static void run(const double (&a)[SB], double (&w)[SB], int lane) {
+        double sacc = (K == lane) ? 1.0 : 0.0;
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const double lkq = __shfl_sync(0xffffffffu, a[q], K);  // L[K][q]
+            if (q >= lane) sacc = fma(-lkq, w[q], sacc);
+        }
+        const double lkk = __shfl_sync(0xffffffffu, a[K], K);
+        w[K] = (K < lane) ? 0.0 : sacc / lkk;
+        WarpInverse32<K + 1>::run(a, w, lane);
+    }
+};
+template <>
+struct WarpInverse32<SB> {
+    __device__ __forceinline__ static void run(const double (&)[SB], double (&)[SB], int) {}
+};
+
+// Returns the 1-based failing column or 0 (the same value in every lane).
 __device__ __forceinline__ int warp_potrf_inv32(double (*L)[NB + 1], int b0, double (*W)[SB + 1]) {
     const int lane = threadIdx.x & 31;
-    double *row = &L[b0 + lane][b0];
-    for (int j = 0; j < SB; ++j) {
-        const double piv = L[b0 + j][b0 + j];
-        if (!(piv > 0.0)) return j + 1;
-        const double r = sqrt(piv), inv = 1.0 / r;
-        __syncwarp();
-        if (lane == j) row[j] = r;
-        else if (lane > j) row[j] *= inv;
-        __syncwarp();
-        const double lij = row[j];
-        for (int c = j + 1; c <= lane; ++c) row[c] = fma(-lij, L[b0 + c][b0 + j], row[c]);
-        __syncwarp();
-    }
-    // column `lane` of the inverse by forward substitution: W[k][lane]
-    for (int k = 0; k < SB; ++k) {
-        double sacc = (k == lane) ? 1.0 : 0.0;
-        const double *lk = &L[b0 + k][b0];
-        for (int q = lane; q < k; ++q) sacc = fma(-lk[q], W[q][lane], sacc);
-        W[k][lane] = (k < lane) ? 0.0 : sacc / lk[k];
-    }
+    double a[SB];
+#pragma unroll
+    for (int c = 0; c < SB; ++c) a[c] = c <= lane ? L[b0 + lane][b0 + c] : 0.0;
+    int fail = 0;
+    WarpFactor32<0>::run(a, lane, fail);
+    if (fail) return fail;
+#pragma unroll
+    for (int c = 0; c < SB; ++c)
+        if (c <= lane) L[b0 + lane][b0 + c] = a[c];
+    double w[SB];
+    WarpInverse32<0>::run(a, w, lane);
+#pragma unroll
+    for (int k = 0; k < SB; ++k) W[k][lane] = w[k];
     __syncwarp();
     return 0;
 }
 
-__global__ void __launch_bounds__(TPB)
+__global__ void __launch_bounds__(TPB, 1)
 potf2_block_kernel(double *__restrict__ A, long long lda, int k0, int kn,
                    double *__restrict__ Linv, int *__restrict__ info) {
     extern __shared__ double potf2_smem[];
