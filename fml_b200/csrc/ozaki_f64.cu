@@ -66,9 +66,9 @@ constexpr int OZ_BM = 128, OZ_BN = 128;
 // the 512 columns hold: with two, a pass's MMAs run while the epilogue drains
 // the previous pass.
 constexpr int OZ_PASS_Q = OZ_PASS_DIAGONALS;
-constexpr int OZ_TMEM_BUFS = 4 / OZ_PASS_Q;
+constexpr int OZ_TMEM_BUFS = 4 / OZ_PASS_Q;  // 512 columns: 2 buffers of 2, 1 of 3 or 4
 constexpr int OZ_MAX_PASSES = (8 + OZ_PASS_Q - 1) / OZ_PASS_Q;
-static_assert(OZ_PASS_Q == 2 || OZ_PASS_Q == 4, "passes of 2 or 4 diagonals");
+static_assert(OZ_PASS_Q >= 2 && OZ_PASS_Q <= 4, "passes of 2 to 4 diagonals");
 constexpr int OZ_KB = 32;          // int8 k values (bytes) per stage: one MMA K step
 constexpr int OZ_MAX_STAGES = 8;  // the ring depth is set per launch from shared memory
 constexpr int OZ_THREADS = 320;    // 10 warps
