@@ -162,13 +162,21 @@ potf2_block_kernel(double *__restrict__ A, long long lda, int k0, int kn,
             }
         }
         __syncthreads();
-        // update of the rest of the block: L[r][c] -= sum_k X[r][k] X[c][k], r0 <= c <= r
+        // update of the rest of the block: L[r][c] -= sum_k X[r][k] X[c][k], r0 <= c <= r;
+        // two columns per step, so two independent FMA chains share the row loads
         for (int r = r0 + (tid >> 4); r < NB; r += TPB / 16) {
-            for (int c = r0 + (tid & 15); c <= r; c += 16) {
-                double sacc = 0.0;
+            for (int c = r0 + (tid & 15); c <= r; c += 32) {
+                const bool two = c + 16 <= r;
+                const int c2 = two ? c + 16 : c;
+                double s0 = 0.0, s1 = 0.0;
 #pragma unroll 8
-                for (int k = 0; k < SB; ++k) sacc = fma(L[r][b0 + k], L[c][b0 + k], sacc);
-                L[r][c] -= sacc;
+                for (int k = 0; k < SB; ++k) {
+                    const double x = L[r][b0 + k];
+                    s0 = fma(x, L[c][b0 + k], s0);
+                    s1 = fma(x, L[c2][b0 + k], s1);
+                }
+                L[r][c] -= s0;
+                if (two) L[r][c2] -= s1;
             }
         }
         __syncthreads();
@@ -181,25 +189,36 @@ potf2_block_kernel(double *__restrict__ A, long long lda, int k0, int kn,
     // block inverse; inv(L)_IJ for I > J is stored transposed at L[b0J + c][b0I + r].
     // Block row I needs the rows before it only, so its J < I blocks are formed
     // together: T[J] for every J, then inv(L)_IJ = -inv(L_II) T[J].
+    // Thread tid forms, for every J, the four rows r = tid / 32 + 8 i of column
+    // c = tid % 32: the column operand is loaded once for four independent FMA
+    // chains (each entry's sum in the same order as one chain per entry).
+    static_assert(TPB == 8 * SB, "four rows per thread and column block");
+    const int rq = tid >> 5, cq = tid & 31;
     for (int I = 1; I < NSB; ++I) {
-        for (int t = tid; t < I * SB * SB; t += TPB) {
-            const int J = t / (SB * SB), r = (t >> 5) & 31, c = t & 31;
-            double sacc = 0.0;
+        for (int J = 0; J < I; ++J) {
+            double sacc[4] = {0.0, 0.0, 0.0, 0.0};
             for (int K = J; K < I; ++K) {
                 for (int q = 0; q < SB; ++q) {
-                    const double lik = L[I * SB + r][K * SB + q];
-                    const double inv = (K == J) ? W[J][q][c] : L[J * SB + c][K * SB + q];
-                    sacc = fma(lik, inv, sacc);
+                    const double inv = (K == J) ? W[J][q][cq] : L[J * SB + cq][K * SB + q];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        sacc[i] = fma(L[I * SB + rq + 8 * i][K * SB + q], inv, sacc[i]);
                 }
             }
-            T[J][r][c] = sacc;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) T[J][rq + 8 * i][cq] = sacc[i];
         }
         __syncthreads();
-        for (int t = tid; t < I * SB * SB; t += TPB) {
-            const int J = t / (SB * SB), r = (t >> 5) & 31, c = t & 31;
-            double sacc = 0.0;
-            for (int q = 0; q <= r; ++q) sacc = fma(W[I][r][q], T[J][q][c], sacc);
-            L[J * SB + c][I * SB + r] = -sacc;
+        for (int J = 0; J < I; ++J) {
+            double sacc[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int q = 0; q <= rq + 24; ++q) {
+                const double tq = T[J][q][cq];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (q <= rq + 8 * i) sacc[i] = fma(W[I][rq + 8 * i][q], tq, sacc[i]);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) L[J * SB + cq][I * SB + rq + 8 * i] = -sacc[i];
         }
         __syncthreads();
     }
