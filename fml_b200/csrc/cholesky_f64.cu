@@ -75,19 +75,22 @@ template <>
 struct WarpFactor32<SB> {
     __device__ __forceinline__ static void run(double (&)[SB], int, int &) {}
 };
-// Column `lane` of the inverse by forward substitution: w[K] = W[K][lane].
+// Column `lane` of the inverse by forward substitution, right-looking: once
+// w[K] = W[K][lane] is final it is subtracted from every later row's sum, so
+// the serial chain per step is one division and one FMA. Each row's sum takes
+// its terms in ascending column order, as the left-looking loop does; v[K]
+// holds that sum until step K turns it into w[K].
 template <int K>
 struct WarpInverse32 {
-    __device__ __forceinline__ static void run(const double (&a)[SB], double (&w)[SB], int lane) {
-        double sacc = (K == lane) ? 1.0 : 0.0;
-#pragma unroll
-        for (int q = 0; q < K; ++q) {
-            const double lkq = __shfl_sync(0xffffffffu, a[q], K);  // L[K][q]
-            if (q >= lane) sacc = fma(-lkq, w[q], sacc);
-        }
+    __device__ __forceinline__ static void run(const double (&a)[SB], double (&v)[SB], int lane) {
         const double lkk = __shfl_sync(0xffffffffu, a[K], K);
-        w[K] = (K < lane) ? 0.0 : sacc / lkk;
-        WarpInverse32<K + 1>::run(a, w, lane);
+        v[K] = (K < lane) ? 0.0 : v[K] / lkk;
+#pragma unroll
+        for (int r = K + 1; r < SB; ++r) {
+            const double lrk = __shfl_sync(0xffffffffu, a[K], r);  // L[r][K]
+            if (K >= lane) v[r] = fma(-lrk, v[K], v[r]);
+        }
+        WarpInverse32<K + 1>::run(a, v, lane);
     }
 };
 template <>
@@ -108,6 +111,8 @@ __device__ __forceinline__ int warp_potrf_inv32(double (*L)[NB + 1], int b0, dou
     for (int c = 0; c < SB; ++c)
         if (c <= lane) L[b0 + lane][b0 + c] = a[c];
     double w[SB];
+#pragma unroll
+    for (int k = 0; k < SB; ++k) w[k] = (k == lane) ? 1.0 : 0.0;
     WarpInverse32<0>::run(a, w, lane);
 #pragma unroll
     for (int k = 0; k < SB; ++k) W[k][lane] = w[k];
