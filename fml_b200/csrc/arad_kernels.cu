@@ -540,67 +540,16 @@ __device__ __forceinline__ float set_lt(float a, float b) {  // 1.0f if a < b, e
     return r;
 }
 
-// Paired work item over molecule I in radius bands: lane = one record of I
-// (records sorted by r, 32 per pass), loop over the record pairs of atom j1
-// of J, two records per step with packed FP32x2 arithmetic. Every term is
-// computed with the same operations as in fast_item. Records of j1 that lie
-// outside the (8w)^2 window of every lane of the pass (j1's records are
-// sorted by r) are skipped: their terms are exactly zero. The lane's sum is
+// Paired work item over molecule I in radius bands: lane = one record of
+// pass p and one of pass p + 1 (records of I sorted by r, 32 per pass),
+// against the record pairs of atom j1 of J, two records per step with packed
+// FP32x2 arithmetic; each J record pair is loaded once for four
+// neighbour-pair evaluations. Every term is computed with the same operations
+// as in fast_item. Records of j1 outside the (8w)^2 window of every lane of
+// the two passes (j1's records are sorted by r) are skipped, and terms outside
+// a record's own window are masked: both are exactly zero. The lane's sums are
 // added to S(i1, j1) in 2^-32 fixed point, so the result does not depend on
 // the order of the additions.
-__device__ __forceinline__ void fast_item_band(FastSmem &sm, int p, int j1, float maxg2s,
-                                               float wd) {
-    const int lane = threadIdx.x & 31;
-    const float4 u = sm.recI[p * 32 + lane];
-    const int meta = sm.metaI[p * 32 + lane];
-    const float2 *ptrow = sm.pt + ((meta >> 16) & 0xff) * FC_PTS;
-    const float2 nux = make_float2(-u.x, -u.x), uy = make_float2(u.y, u.y),
-                 uz = make_float2(u.z, u.z), uw = make_float2(u.w, u.w);
-    const int beg = sm.offJ[j1], end = sm.offJ[j1 + 1];
-    // window sub-range: pairs whose records are all <= lo, and pairs from the
-    // first one whose first record is >= hi (at most 16 pairs: one per lane)
-    const float lo = sm.passLo[p] - wd, hi = sm.passHi[p] + wd;
-    bool below = false, before = false;
-    if (beg + lane < end) {
-        const float4 A = sm.J.p.a[beg + lane];
-        below = !(A.y > lo);
-        before = A.x < hi;
-    }
-    const int mb = beg + __popc(__ballot_sync(0xffffffffu, below));
-    const int me = beg + __popc(__ballot_sync(0xffffffffu, before));
-    float2 acc = make_float2(0.0f, 0.0f);
-#pragma unroll 4
-    for (int m = mb; m < me; ++m) {
-        const float4 A = sm.J.p.a[m];
-        const float4 B = sm.J.p.b[m];
-        const float2 st = ptrow[sm.J.p.k[m]];
-        const float2 dr = __fadd2_rn(make_float2(A.x, A.y), nux);
-        const float2 t = __fmul2_rn(dr, dr);
-        float e0, e1;
-        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e0) : "f"(-t.x));
-        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e1) : "f"(-t.y));
-        const float2 g = __ffma2_rn(make_float2(B.z, B.w), uw,
-                                    __ffma2_rn(make_float2(B.x, B.y), uz,
-                                               __fmul2_rn(make_float2(A.z, A.w), uy)));
-        const float2 win = make_float2(set_lt(t.x, maxg2s), set_lt(t.y, maxg2s));
-        const float2 eg = __fmul2_rn(__fmul2_rn(make_float2(e0, e1), st), win);
-        acc = __ffma2_rn(eg, g, acc);
-    }
-    if ((meta >> 24) & 1) {
-        const long long f = __float2ll_rn((acc.x + acc.y) * 4294967296.0f);
-        if (f)
-            atomicAdd(reinterpret_cast<unsigned long long *>(&sm.S.q[(meta & 0xff) * FC_SS + j1]),
-                      (unsigned long long)f);
-    }
-}
-
-// Two passes per work item: lane = one record of pass p and one of pass
-// p + 1 (the next 32 records in r order), against the record pairs of atom j1
-// of J in the union of the two passes' windows. Each J record pair is loaded
-// once for four neighbour-pair evaluations, and the item set-up is shared by
-// two passes. Terms outside a record's own window are masked to exactly zero,
-// so every lane sums the same non-zero terms in the same order as
-// fast_item_band and the fixed-point sums are unchanged.
 __device__ __forceinline__ void fast_item_band2(FastSmem &sm, int p, int j1, float maxg2s,
                                                 float wd) {
     const int lane = threadIdx.x & 31;
