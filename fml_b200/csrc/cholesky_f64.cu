@@ -496,6 +496,16 @@ int launch_syrk(double *C, long long ldc, int m, const double *P, long long ldp,
 // block's stored inverse, so the next launch starts from a finished
 // sub-vector. All reductions run in a fixed order (deterministic).
 constexpr int SOLVE_WARPS = TPB / 32;
+
+// Programmatic dependent launch: the solve's step kernels are launched with
+// programmatic stream serialization, so the next step's CTAs are scheduled
+// (and read their rows of the factor, which no step writes) while this step
+// finishes; griddepcontrol.wait then orders every read of x and y after the
+// previous step's grid has completed and its writes are visible.
+__device__ __forceinline__ void pdl_launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 constexpr int FWD_ROWS = 32;   // rows per thread block past the next diagonal block
 constexpr int BWD_COLS = 32;   // columns per thread block before the previous one
 
@@ -561,6 +571,8 @@ __global__ void __launch_bounds__(TPB)
 solve_first_backward_kernel(const double *__restrict__ Linvk, const double *__restrict__ y,
                             double *__restrict__ x, int kn) {
     __shared__ double red[TPB];
+    pdl_launch_dependents();
+    pdl_wait();
     tri_upper_apply(Linvk, y, x, kn, red);
 }
 
@@ -583,13 +595,10 @@ forward_step_kernel(const double *__restrict__ L, long long lda, int n, int k0, 
     __shared__ double xn[NB];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool owner = blockIdx.x == 0;
+    pdl_launch_dependents();
     if (owner && LinvNext != nullptr) prefetch_block_l2(LinvNext);
     double ykr[NB / 32];
-#pragma unroll
-    for (int i = 0; i < NB / 32; ++i) {
-        const int c = lane + 32 * i;
-        ykr[i] = c < kn ? y[k0 + c] : 0.0;
-    }
+    bool waited = false;
     const int nb0 = k0 + kn;
     int rb, re;
     if (owner) {
@@ -601,18 +610,37 @@ forward_step_kernel(const double *__restrict__ L, long long lda, int n, int k0, 
     }
     constexpr int G = 8;  // rows per warp in flight
     for (int r0 = rb + warp; r0 < re; r0 += G * SOLVE_WARPS) {
-        double s[G], xr[G];
+        double s[G], xr[G], lv[G][NB / 32];
+#pragma unroll
+        for (int q = 0; q < G; ++q) {  // the factor's rows: not written by any step
+            const int r = r0 + q * SOLVE_WARPS;
+            const bool ok = r < re;
+            const double *row = L + (size_t)min(r, n - 1) * lda + k0;
+#pragma unroll
+            for (int i = 0; i < NB / 32; ++i) {
+                const int c = lane + 32 * i;
+                lv[q][i] = (ok && c < kn) ? row[c] : 0.0;
+            }
+        }
+        if (!waited) {
+            pdl_wait();
+            waited = true;
+#pragma unroll
+            for (int i = 0; i < NB / 32; ++i) {
+                const int c = lane + 32 * i;
+                ykr[i] = c < kn ? y[k0 + c] : 0.0;
+            }
+        }
 #pragma unroll
         for (int q = 0; q < G; ++q) {
             const int r = r0 + q * SOLVE_WARPS;
             const bool ok = r < re;
-            const double *row = L + (size_t)min(r, n - 1) * lda + k0;
             s[q] = 0.0;
             xr[q] = (ok && lane == 0) ? x[r] : 0.0;
 #pragma unroll
             for (int i = 0; i < NB / 32; ++i) {
                 const int c = lane + 32 * i;
-                if (ok && c < kn) s[q] = fma(row[c], ykr[i], s[q]);
+                if (ok && c < kn) s[q] = fma(lv[q][i], ykr[i], s[q]);
             }
         }
 #pragma unroll
@@ -626,6 +654,7 @@ forward_step_kernel(const double *__restrict__ L, long long lda, int n, int k0, 
             }
         }
     }
+    if (!waited) pdl_wait();
     if (owner && LinvNext != nullptr) {
         __syncthreads();
         tri_lower_apply(LinvNext, xn, y + nb0, re - rb);
@@ -646,7 +675,9 @@ backward_step_kernel(const double *__restrict__ L, long long lda, int k0, int kn
     __shared__ double red[TPB];
     const int tid = threadIdx.x;
     const bool owner = blockIdx.x == 0;
+    pdl_launch_dependents();
     if (owner) prefetch_block_l2(LinvPrev);
+    pdl_wait();
     if (tid < NB) xk[tid] = tid < kn ? x[k0 + tid] : 0.0;
     __syncthreads();
     const int pb = k0 - NB;  // first column of the previous diagonal block (k0 >= NB here)
@@ -1055,6 +1086,25 @@ extern "C" int fmlb_potrf_ozaki_f64(double *A, long long lda, int n, int nslices
     return potrf_blocked(A, lda, n, work, info, st, &oz);
 }
 
+// Launch with programmatic stream serialization (the kernel orders its
+// dependent reads with griddepcontrol.wait).
+template <typename... KArgs, typename... Args>
+static int launch_pdl(void (*kernel)(KArgs...), int grid, cudaStream_t st, const char *name,
+                      Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(fmlb::TPB);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    FMLB_TRY(fmlb::cuda_status(cudaLaunchKernelEx(&cfg, kernel, args...), name));
+    return fmlb::launch_status(name);
+}
+
 extern "C" int fmlb_potrs_f64(const double *L, long long lda, int n, const void *work, double *x,
                               void *stream) {
     using namespace fmlb;
@@ -1071,22 +1121,20 @@ extern "C" int fmlb_potrs_f64(const double *L, long long lda, int n, const void 
     for (int k0 = 0, kb = 0; k0 + NB < n; k0 += NB, ++kb) {
         const int rest = n - k0 - NB;  // rows past this block column
         const int grid = 1 + ceil_div(std::max(0, rest - NB), FWD_ROWS);
-        forward_step_kernel<<<grid, TPB, 0, st>>>(L, lda, n, k0, NB,
-                                                  Linv + (size_t)(kb + 1) * NB * NB, x, y);
-        FMLB_TRY(launch_status("forward_step_kernel"));
+        FMLB_TRY(launch_pdl(forward_step_kernel, grid, st, "forward_step_kernel", L, lda, n, k0,
+                            (int)NB, (const double *)(Linv + (size_t)(kb + 1) * NB * NB), x, y));
     }
     {
         const int kb = (int)nblk - 1, k0 = kb * NB;
-        solve_first_backward_kernel<<<1, TPB, 0, st>>>(Linv + (size_t)kb * NB * NB, y + k0,
-                                                       x + k0, n - k0);
-        FMLB_TRY(launch_status("solve_first_backward_kernel"));
+        FMLB_TRY(launch_pdl(solve_first_backward_kernel, 1, st, "solve_first_backward_kernel",
+                            (const double *)(Linv + (size_t)kb * NB * NB), (const double *)(y + k0),
+                            x + k0, n - k0));
     }
     for (int kb = (int)nblk - 1; kb >= 1; --kb) {
         const int k0 = kb * NB, kn = std::min(NB, n - k0);
         const int grid = 1 + ceil_div(k0 - NB, BWD_COLS);
-        backward_step_kernel<<<grid, TPB, 0, st>>>(L, lda, k0, kn,
-                                                   Linv + (size_t)(kb - 1) * NB * NB, y, x);
-        FMLB_TRY(launch_status("backward_step_kernel"));
+        FMLB_TRY(launch_pdl(backward_step_kernel, grid, st, "backward_step_kernel", L, lda, k0, kn,
+                            (const double *)(Linv + (size_t)(kb - 1) * NB * NB), y, x));
     }
     return FMLB_OK;
 }
