@@ -35,6 +35,20 @@ __device__ __forceinline__ bool failed(const int *info) {
     return info && *(volatile const int *)info != 0;
 }
 
+// Programmatic dependent launch (kernels launched with programmatic stream
+// serialization; in a kernel launched without it both are no-ops).
+// griddepcontrol.wait returns once the previous kernel of the stream has
+// completed and its writes are visible, so every read of data that kernel
+// may write comes after it. The panel chain (diagonal block, panel solve,
+// update inside the outer panel) signals its dependent only at its end, so
+// the next kernel's CTAs do not sit on SMs the concurrent bulk update needs;
+// the solve's step kernels signal at their start and read their rows of the
+// factor, which no step writes, before waiting.
+__device__ __forceinline__ void pdl_launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ---- 1. diagonal block ----------------------------------------------------
 // The 128 x 128 block is factored in four 32-column steps. In step J one warp
 // factors (and inverts) the 32 x 32 diagonal sub-block in registers with warp
@@ -130,6 +144,7 @@ potf2_block_kernel(double *__restrict__ A, long long lda, int k0, int kn,
     double(*T)[SB][LDW] =
         reinterpret_cast<double(*)[SB][LDW]>(potf2_smem + NB * LDL + NSB * SB * LDW);
     __shared__ int bad;
+    pdl_wait();
     if (failed(info)) return;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     for (int t = tid; t < NB * NB; t += TPB) {
@@ -235,6 +250,7 @@ potf2_block_kernel(double *__restrict__ A, long long lda, int k0, int kn,
         else if (I > J) v = L[c][r];
         Linv[t] = v;
     }
+    pdl_launch_dependents();
 }
 
 // ---- 2. panel solve: rows [r0, n) of columns [k0, k0+kn): X <- X Linv^T ----
@@ -275,8 +291,10 @@ __global__ void __launch_bounds__(TPB)
 panel_trsm_kernel(double *__restrict__ A, long long lda, int n, int k0, int kn,
                   const double *__restrict__ Linv, const int *__restrict__ info) {
     extern __shared__ double trsm_smem[];
+    pdl_wait();
     if (failed(info)) return;
     trsm_rows(A, lda, k0 + kn + blockIdx.x * TRSM_ROWS, n, k0, kn, Linv, trsm_smem);
+    pdl_launch_dependents();
 }
 
 // Rows [0, rend) of columns [k0, k0 + kn): X <- X Linv^T (the inverse's
@@ -356,6 +374,7 @@ __global__ void __launch_bounds__(SY_TPB, 2)
 syrk_dmma_kernel(double *__restrict__ C, long long ldc, int m, const double *__restrict__ P,
                  long long ldp, int k, int strip_tiles, const int *__restrict__ info) {
     extern __shared__ __align__(16) double sy_smem[];
+    pdl_wait();
     if (failed(info)) return;
     const long long t = blockIdx.x;
     int by, bx;
@@ -456,11 +475,31 @@ syrk_dmma_kernel(double *__restrict__ C, long long ldc, int m, const double *__r
         if (gc < m && gc <= gr) dst[0] = Cs[r * SY_CLD + c];
         if (gc + 1 < m && gc + 1 <= gr) dst[1] = Cs[r * SY_CLD + c + 1];
     }
+    pdl_launch_dependents();
+}
+
+// Launch with programmatic stream serialization when `pdl` is set (the kernel
+// orders its dependent reads with griddepcontrol.wait).
+template <typename... KArgs, typename... Args>
+int launch_maybe_pdl(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                     cudaStream_t st, const char *name, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    FMLB_TRY(cuda_status(cudaLaunchKernelEx(&cfg, kernel, args...), name));
+    return launch_status(name);
 }
 
 template <bool kAligned16>
 int launch_syrk_impl(double *C, long long ldc, int m, const double *P, long long ldp, int k,
-                     int strip_cols, const int *info, cudaStream_t st) {
+                     int strip_cols, const int *info, cudaStream_t st, bool pdl) {
     static int attr_dev = -1;
     int dev = 0;
     FMLB_TRY(cuda_status(cudaGetDevice(&dev), "syrk: cudaGetDevice"));
@@ -474,19 +513,19 @@ int launch_syrk_impl(double *C, long long ldc, int m, const double *P, long long
     const int strip_tiles = strip_cols > 0 ? ceil_div(std::min(strip_cols, m), SY_TN) : 0;
     // full: row block by holds 2 by + 2 column tiles; strip: strip_tiles per row block
     const long long ntiles = strip_tiles ? Tr * strip_tiles : Tr * Tr + Tr;
-    syrk_dmma_kernel<kAligned16><<<(unsigned)ntiles, SY_TPB, kSyrkSmem, st>>>(
-        C, ldc, m, P, ldp, k, strip_tiles, info);
-    return launch_status("syrk_dmma_kernel");
+    return launch_maybe_pdl(pdl, syrk_dmma_kernel<kAligned16>, dim3((unsigned)ntiles),
+                            dim3(SY_TPB), kSyrkSmem, st, "syrk_dmma_kernel", C, ldc, m, P, ldp, k,
+                            strip_tiles, info);
 }
 
 // strip_cols = 0: lower triangle of the m x m block; > 0: only its first
 // strip_cols columns (the lower part of that column strip).
 int launch_syrk(double *C, long long ldc, int m, const double *P, long long ldp, int k,
-                const int *info, cudaStream_t st, int strip_cols = 0) {
+                const int *info, cudaStream_t st, int strip_cols = 0, bool pdl = false) {
     if (m <= 0 || k <= 0) return FMLB_OK;
     if (((uintptr_t)P % 16 == 0) && (ldp % 2 == 0))
-        return launch_syrk_impl<true>(C, ldc, m, P, ldp, k, strip_cols, info, st);
-    return launch_syrk_impl<false>(C, ldc, m, P, ldp, k, strip_cols, info, st);
+        return launch_syrk_impl<true>(C, ldc, m, P, ldp, k, strip_cols, info, st, pdl);
+    return launch_syrk_impl<false>(C, ldc, m, P, ldp, k, strip_cols, info, st, pdl);
 }
 
 // ---- 4. triangular solves with the factor (potrs) ---------------------------
@@ -497,15 +536,6 @@ int launch_syrk(double *C, long long ldc, int m, const double *P, long long ldp,
 // sub-vector. All reductions run in a fixed order (deterministic).
 constexpr int SOLVE_WARPS = TPB / 32;
 
-// Programmatic dependent launch: the solve's step kernels are launched with
-// programmatic stream serialization, so the next step's CTAs are scheduled
-// (and read their rows of the factor, which no step writes) while this step
-// finishes; griddepcontrol.wait then orders every read of x and y after the
-// previous step's grid has completed and its writes are visible.
-__device__ __forceinline__ void pdl_launch_dependents() {
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 constexpr int FWD_ROWS = 32;   // rows per thread block past the next diagonal block
 constexpr int BWD_COLS = 32;   // columns per thread block before the previous one
 
@@ -954,14 +984,15 @@ static int panel_factor(double *A, long long lda, int n, int k0, double *Li, int
                         cudaStream_t st) {
     using namespace fmlb;
     const int kn = std::min(NB, n - k0);
-    potf2_block_kernel<<<1, TPB, kPotf2Smem, st>>>(A, lda, k0, kn, Li, info);
-    FMLB_TRY(launch_status("potf2_block_kernel"));
+    // the chain of one outer panel: each kernel follows the previous one of
+    // the stream with a programmatic dependency
+    FMLB_TRY(launch_maybe_pdl(true, potf2_block_kernel, dim3(1), dim3(TPB), kPotf2Smem, st,
+                              "potf2_block_kernel", A, lda, k0, kn, Li, info));
     const int rest = n - k0 - kn;
-    if (rest > 0) {
-        panel_trsm_kernel<<<ceil_div(rest, TRSM_ROWS), TPB, kTrsmSmem, st>>>(A, lda, n, k0, kn, Li,
-                                                                            info);
-        FMLB_TRY(launch_status("panel_trsm_kernel"));
-    }
+    if (rest > 0)
+        FMLB_TRY(launch_maybe_pdl(true, panel_trsm_kernel, dim3(ceil_div(rest, TRSM_ROWS)),
+                                  dim3(TPB), kTrsmSmem, st, "panel_trsm_kernel", A, lda, n, k0, kn,
+                                  (const double *)Li, (const int *)info));
     return FMLB_OK;
 }
 
@@ -978,7 +1009,7 @@ static int factor_outer_panel(double *A, long long lda, int n, int K0, int width
         const int rem = end - (int)b;
         if (rem > 0)
             FMLB_TRY(launch_syrk(A + b * lda + b, lda, n - (int)b, A + b * lda + k0, lda, NB, info,
-                                 st, rem));
+                                 st, rem, true));
     }
     return FMLB_OK;
 }
@@ -1086,25 +1117,6 @@ extern "C" int fmlb_potrf_ozaki_f64(double *A, long long lda, int n, int nslices
     return potrf_blocked(A, lda, n, work, info, st, &oz);
 }
 
-// Launch with programmatic stream serialization (the kernel orders its
-// dependent reads with griddepcontrol.wait).
-template <typename... KArgs, typename... Args>
-static int launch_pdl(void (*kernel)(KArgs...), int grid, cudaStream_t st, const char *name,
-                      Args... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(fmlb::TPB);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    FMLB_TRY(fmlb::cuda_status(cudaLaunchKernelEx(&cfg, kernel, args...), name));
-    return fmlb::launch_status(name);
-}
-
 extern "C" int fmlb_potrs_f64(const double *L, long long lda, int n, const void *work, double *x,
                               void *stream) {
     using namespace fmlb;
@@ -1121,20 +1133,23 @@ extern "C" int fmlb_potrs_f64(const double *L, long long lda, int n, const void 
     for (int k0 = 0, kb = 0; k0 + NB < n; k0 += NB, ++kb) {
         const int rest = n - k0 - NB;  // rows past this block column
         const int grid = 1 + ceil_div(std::max(0, rest - NB), FWD_ROWS);
-        FMLB_TRY(launch_pdl(forward_step_kernel, grid, st, "forward_step_kernel", L, lda, n, k0,
-                            (int)NB, (const double *)(Linv + (size_t)(kb + 1) * NB * NB), x, y));
+        FMLB_TRY(launch_maybe_pdl(true, forward_step_kernel, dim3(grid), dim3(TPB), 0, st,
+                                  "forward_step_kernel", L, lda, n, k0, (int)NB,
+                                  (const double *)(Linv + (size_t)(kb + 1) * NB * NB), x, y));
     }
     {
         const int kb = (int)nblk - 1, k0 = kb * NB;
-        FMLB_TRY(launch_pdl(solve_first_backward_kernel, 1, st, "solve_first_backward_kernel",
-                            (const double *)(Linv + (size_t)kb * NB * NB), (const double *)(y + k0),
-                            x + k0, n - k0));
+        FMLB_TRY(launch_maybe_pdl(true, solve_first_backward_kernel, dim3(1), dim3(TPB), 0, st,
+                                  "solve_first_backward_kernel",
+                                  (const double *)(Linv + (size_t)kb * NB * NB),
+                                  (const double *)(y + k0), x + k0, n - k0));
     }
     for (int kb = (int)nblk - 1; kb >= 1; --kb) {
         const int k0 = kb * NB, kn = std::min(NB, n - k0);
         const int grid = 1 + ceil_div(k0 - NB, BWD_COLS);
-        FMLB_TRY(launch_pdl(backward_step_kernel, grid, st, "backward_step_kernel", L, lda, k0, kn,
-                            (const double *)(Linv + (size_t)(kb - 1) * NB * NB), y, x));
+        FMLB_TRY(launch_maybe_pdl(true, backward_step_kernel, dim3(grid), dim3(TPB), 0, st,
+                                  "backward_step_kernel", L, lda, k0, kn,
+                                  (const double *)(Linv + (size_t)(kb - 1) * NB * NB), y, x));
     }
     return FMLB_OK;
 }
