@@ -981,12 +981,14 @@ static int lookahead_for(cudaStream_t caller, Lookahead **out) {
 }
 
 static int panel_factor(double *A, long long lda, int n, int k0, double *Li, int *info,
-                        cudaStream_t st) {
+                        cudaStream_t st, bool after_kernel) {
     using namespace fmlb;
     const int kn = std::min(NB, n - k0);
     // the chain of one outer panel: each kernel follows the previous one of
-    // the stream with a programmatic dependency
-    FMLB_TRY(launch_maybe_pdl(true, potf2_block_kernel, dim3(1), dim3(TPB), kPotf2Smem, st,
+    // the stream with a programmatic dependency; the first block of an outer
+    // panel is launched normally, as what precedes it may be a memset or an
+    // event wait rather than a kernel of the chain
+    FMLB_TRY(launch_maybe_pdl(after_kernel, potf2_block_kernel, dim3(1), dim3(TPB), kPotf2Smem, st,
                               "potf2_block_kernel", A, lda, k0, kn, Li, info));
     const int rest = n - k0 - kn;
     if (rest > 0)
@@ -1004,7 +1006,8 @@ static int factor_outer_panel(double *A, long long lda, int n, int K0, int width
     using namespace fmlb;
     const int end = std::min(K0 + width, n);
     for (int k0 = K0; k0 < end; k0 += NB) {
-        FMLB_TRY(panel_factor(A, lda, n, k0, Linv + (size_t)(k0 / NB) * NB * NB, info, st));
+        FMLB_TRY(panel_factor(A, lda, n, k0, Linv + (size_t)(k0 / NB) * NB * NB, info, st,
+                              k0 > K0));
         const size_t b = (size_t)(k0 + NB);
         const int rem = end - (int)b;
         if (rem > 0)
