@@ -39,7 +39,7 @@ import torch
 from . import _lib
 from .cho_solve import CholeskyWarning, potrf
 from ._tensors import device, is_torch, to_device, to_output, workspace
-from .data import ptp_of
+from .data import PTP_COL, PTP_ROW
 
 PRECISIONS = {"fp64": 0, "fp32": 1}
 
@@ -151,16 +151,29 @@ def laplacian_kernel(A, B, sigma, precision="fp64"):
 # ARAD
 # ---------------------------------------------------------------------------
 def _ptp_arrays(Z, amax):
-    """kernels.py:261-292: PTP (nm, amax, 2) float64 and atom counts N (nm,) int32."""
+    """kernels.py:261-292: PTP (nm, amax, 2) float64 and atom counts N (nm,) int32.
+
+    One table lookup over the concatenated charges and one scatter into the
+    padded rows. A charge the table does not hold raises KeyError with the
+    first such charge in molecule and atom order, as the reference's dict
+    lookup does (kernels.py:276)."""
     nm = len(Z)
-    N = np.array([len(z) for z in Z], dtype=np.int32)
+    zs = [np.asarray(z).reshape(-1) for z in Z]
+    N = np.array([len(z) for z in zs], dtype=np.int32)
     if nm and N.max() > amax:
         raise ValueError("a molecule has more atoms (%d) than the descriptor size %d"
                          % (int(N.max()), amax))
     Zp = np.zeros((nm, amax, 2))
-    for i, z in enumerate(Z):
-        if len(z):
-            Zp[i, :len(z)] = ptp_of(z)
+    if nm and N.sum():
+        zi = np.concatenate(zs).astype(np.int64)
+        bad = (zi < 0) | (zi > 127)
+        bad |= PTP_ROW[np.clip(zi, 0, 127)] < 0
+        if bad.any():
+            raise KeyError(int(zi[np.argmax(bad)]))
+        mol = np.repeat(np.arange(nm), N)
+        slot = np.arange(len(zi)) - np.repeat(np.cumsum(N) - N, N)
+        Zp[mol, slot, 0] = PTP_ROW[zi]
+        Zp[mol, slot, 1] = PTP_COL[zi]
     return Zp, N
 
 
