@@ -46,11 +46,13 @@ constexpr int TC_TMEM_COLS = 2 * TC_BN;
 constexpr int TC_MAXSIG = 8;
 constexpr int TC_PITCH = 33;                               // floats per transposed row
 constexpr int TC_BOX_FLOATS = 32 * 32;                     // one 32 x 32 FP32 store box
-constexpr int TC_WARP_STG = 2 * TC_BOX_FLOATS;             // direct + mirrored box per warp
+constexpr int TC_RING = 3;                                 // store boxes per epilogue warp
+constexpr int TC_WARP_STG = TC_RING * TC_BOX_FLOATS;
 static_assert(32 * TC_PITCH <= TC_WARP_STG, "the transposed fallback tile fits the boxes");
 constexpr int TC_STG_BYTES = TC_EPI_WARPS * TC_WARP_STG * 4;
 constexpr size_t kTcSmem =
     (size_t)TC_STAGES * TC_STAGE_BYTES + TC_STG_BYTES + 1024 /* align */ + 256;
+static_assert(kTcSmem <= 232448, "dynamic shared memory of one CTA");
 
 enum TcStatus { TC_OK = 0, TC_TIMEOUT_FULL = 1, TC_TIMEOUT_EMPTY = 2, TC_TIMEOUT_TMEM = 3,
                 TC_TIMEOUT_DRAIN = 4 };
@@ -128,6 +130,12 @@ __device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, const void 
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n"); }
 __device__ __forceinline__ void bulk_wait_read() {
     asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+}
+// the box a ring slot held is free once at most TC_RING - 1 newer groups are
+// still reading (every slot use is its own commit group)
+__device__ __forceinline__ void bulk_wait_ring_slot() {
+    static_assert(TC_RING == 3, "the wait count below is TC_RING - 1");
+    asm volatile("cp.async.bulk.wait_group.read 2;\n" ::: "memory");
 }
 __device__ __forceinline__ void bulk_wait_all() {
     asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
@@ -266,13 +274,16 @@ gauss_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constan
         // --------------------------------------------------------------- epilogue
         // Two warps per TMEM lane quarter, 64 columns each. Both 32-column
         // chunks are drained into registers first and TMEM is released, then
-        // every sigma is written: the mirrored tile straight from registers
-        // (lanes hold consecutive rows: coalesced), the direct tile through a
-        // shared-memory transpose (one coalesced row of 32 floats per store).
+        // every sigma is written through a ring of TC_RING 32 x 32 boxes per
+        // warp (direct and mirrored box of each chunk in consecutive slots,
+        // one TMA store and commit group per slot use), so a box is refilled
+        // while the stores of the two before it are still being read.
+        // Diagonal tiles (and K without TMA alignment) take per-element
+        // stores through a shared-memory transpose.
         const int q = warp & 3;
         const int half = (warp - 2) >> 2;
         float *stg = stg_all + (warp - 2) * TC_WARP_STG;  // 1024-byte aligned boxes
-        float *dbox = stg, *mbox = stg + TC_BOX_FLOATS;
+        int slot = 0;
         const uint64_t stream_out = l2_evict_first();
         int lt = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++lt) {
@@ -297,11 +308,22 @@ gauss_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constan
                 uint32_t v[32];
                 tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) +
                               (uint32_t)(acc * TC_BN + half * 64 + c * 32), v);
+                // the norms are padded to whole tiles (zero past nb) and
+                // 16-byte aligned at every 32-column chunk
+                float ncol[32];
+                const float4 *nb4 = reinterpret_cast<const float4 *>(normB + gcol0 + c * 32);
+#pragma unroll
+                for (int j4 = 0; j4 < 8; ++j4) {
+                    const float4 t4 = __ldg(nb4 + j4);
+                    ncol[4 * j4] = t4.x;
+                    ncol[4 * j4 + 1] = t4.y;
+                    ncol[4 * j4 + 2] = t4.z;
+                    ncol[4 * j4 + 3] = t4.w;
+                }
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     const int gcol = gcol0 + c * 32 + j;
-                    const float nc = gcol < p.nb ? __ldg(normB + gcol) : 0.0f;
-                    float x = fmaxf(nr + nc - 2.0f * __uint_as_float(v[j]), 0.0f);
+                    float x = fmaxf(nr + ncol[j] - 2.0f * __uint_as_float(v[j]), 0.0f);
                     if (diag_tile && gcol == grow) x = 0.0f;  // exact zero distance
                     d2[c * 32 + j] = x;
                 }
@@ -319,33 +341,46 @@ gauss_tc_kernel(const __grid_constant__ CUtensorMap mapAhi, const __grid_constan
                     float kv[32];
 #pragma unroll
                     for (int j = 0; j < 32; ++j) kv[j] = fast_exp2(d2[c * 32 + j] * sc);
-                    // the boxes are free once the previous stores have read them
-                    if (lane == 0) bulk_wait_read();
-                    __syncwarp();
                     if (tma) {
                         // direct box K[row0 + r][cb + j], row r = lane, 128-byte
                         // swizzle: 16-byte chunk j4 of row r at chunk j4 ^ (r & 7)
+                        if (lane == 0) bulk_wait_ring_slot();
+                        __syncwarp();
+                        float *dbox = stg + slot * TC_BOX_FLOATS;
 #pragma unroll
                         for (int j4 = 0; j4 < 8; ++j4)
                             *reinterpret_cast<float4 *>(dbox + lane * 32 + ((j4 ^ (lane & 7)) << 2)) =
                                 make_float4(kv[4 * j4], kv[4 * j4 + 1], kv[4 * j4 + 2],
                                             kv[4 * j4 + 3]);
-                        // mirrored box K[cb + j][row0 + lane]: row j, column lane
-                        if (p.symmetric) {
-#pragma unroll
-                            for (int j = 0; j < 32; ++j)
-                                mbox[j * 32 + (((lane >> 2) ^ (j & 7)) << 2) + (lane & 3)] = kv[j];
-                        }
                         fence_proxy_async();
                         __syncwarp();
                         if (lane == 0) {  // boxes wholly outside K are not issued
                             if (row0 < p.na && cb < p.nb)
                                 tma_store_3d(&mapK, dbox, cb, row0, s, stream_out);
-                            if (p.symmetric && row0 < p.nb && cb < p.na)
-                                tma_store_3d(&mapK, mbox, row0, cb, s, stream_out);
                             bulk_commit();
                         }
+                        slot = slot == TC_RING - 1 ? 0 : slot + 1;
+                        // mirrored box K[cb + j][row0 + lane]: row j, column lane
+                        if (p.symmetric) {
+                            if (lane == 0) bulk_wait_ring_slot();
+                            __syncwarp();
+                            float *mbox = stg + slot * TC_BOX_FLOATS;
+#pragma unroll
+                            for (int j = 0; j < 32; ++j)
+                                mbox[j * 32 + (((lane >> 2) ^ (j & 7)) << 2) + (lane & 3)] = kv[j];
+                            fence_proxy_async();
+                            __syncwarp();
+                            if (lane == 0) {
+                                if (row0 < p.nb && cb < p.na)
+                                    tma_store_3d(&mapK, mbox, row0, cb, s, stream_out);
+                                bulk_commit();
+                            }
+                            slot = slot == TC_RING - 1 ? 0 : slot + 1;
+                        }
                     } else {
+                        // the whole ring is free once every earlier store has read it
+                        if (lane == 0) bulk_wait_read();
+                        __syncwarp();
                         // mirrored tile K[col][row]: lanes write 32 consecutive rows
                         if (p.symmetric && row_ok) {
 #pragma unroll
