@@ -61,3 +61,51 @@ def test_argument_errors_need_no_gpu(lib):
     assert rc == -22  # lda < d
     lib.fmlb_last_error_string.restype = ctypes.c_char_p
     assert b"leading dimension" in lib.fmlb_last_error_string()
+
+
+def _rc_and_message(lib, fn, *args):
+    f = getattr(lib, fn)
+    f.restype = ctypes.c_int
+    rc = f(*args)
+    lib.fmlb_last_error_string.restype = ctypes.c_char_p
+    return rc, lib.fmlb_last_error_string()
+
+
+def test_tensor_core_and_refinement_argument_errors_need_no_gpu(lib):
+    """The int8 factorisation, the int8 trailing update and the double-double
+    refinement reject bad sizes on the host, before any CUDA call."""
+    info = ctypes.c_int(0)
+    ll = ctypes.c_longlong
+    # n < 0
+    rc, msg = _rc_and_message(lib, "fmlb_potrf_ozaki_f64", None, ll(4), -1, 6, None,
+                              ctypes.c_size_t(0), ctypes.byref(info), None)
+    assert rc == -22 and b"fmlb_potrf_ozaki_f64: bad n" in msg
+    # digit planes outside 1..max
+    for s in (0, 99):
+        rc, msg = _rc_and_message(lib, "fmlb_potrf_ozaki_f64", None, ll(4), 4, s, None,
+                                  ctypes.c_size_t(0), ctypes.byref(info), None)
+        assert rc == -22 and b"nslices" in msg
+    # int8 update: k above the int32-exact bound of 8192
+    rc, msg = _rc_and_message(lib, "fmlb_syrk_lower_ozaki", None, ll(16), 16, None,
+                              ll(16384), 16384, 0, 6, None, ctypes.c_size_t(0),
+                              ctypes.byref(info), None)
+    assert rc == -22 and b"8192" in msg
+    # double-double refinement: negative iteration count
+    rc, msg = _rc_and_message(lib, "fmlb_krr_refine_dd", None, ll(4), 4, None, None, None,
+                              None, None, -1, None, None, None)
+    assert rc == -22 and b"fmlb_krr_refine_dd: bad sizes" in msg
+
+
+def test_noalloc_prediction_limits_need_no_gpu(lib):
+    """The allocation-free prediction checks its kind and its fixed scratch
+    limit, ceil(nt/1024) * nsigma * nq <= 2^20 doubles, before it touches a
+    device."""
+    sig = (ctypes.c_double * 8)(*([100.0] * 8))
+    ll = ctypes.c_longlong
+    rc, msg = _rc_and_message(lib, "fmlb_kernel_predict_f64_noalloc", 2, None, 1, 4, None, 1,
+                              4, 4, sig, 1, None, ll(1), None, ll(1), None)
+    assert rc == -22 and b"kind" in msg
+    nq = (1 << 20) // 8 + 1  # 8 sigmas, one 1024-row split: one row above the limit
+    rc, msg = _rc_and_message(lib, "fmlb_kernel_predict_f64_noalloc", 0, None, nq, 4, None,
+                              1024, 4, 4, sig, 8, None, ll(1024), None, ll(nq), None)
+    assert rc == -22 and b"exceeds the fixed scratch" in msg
