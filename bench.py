@@ -149,22 +149,37 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-        rows = []
-        for line in open(self.path):
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
+        with open(self.path) as fh:
+            lines = fh.readlines()
         os.unlink(self.path)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4)
-                          if r[5 + i].lower().startswith("active")})
-        loaded = [v for v in sm if v > 0.5 * smax] or sm
-        return {"sm_mhz": float(np.median(loaded)), "sm_max_mhz": smax, "reasons": reasons,
+        return clock_summary(lines)
+
+
+def clock_summary(lines):
+    """Median SM clock under load, the maximum SM clock and the throttle
+    reasons seen, from `nvidia-smi --query-gpu=<ClockSampler.FIELDS>
+    --format=csv,noheader,nounits` lines. Samples below half the maximum
+    clock (idle moments) are left out of the median; fields that are not
+    numbers ("[N/A]") are skipped."""
+    def num(x):
+        try:
+            return float(x)
+        except ValueError:
+            return None
+
+    rows = [p for p in ([x.strip() for x in line.split(",")] for line in lines) if len(p) >= 9]
+    sm = [v for v in (num(r[1]) for r in rows) if v is not None]
+    smaxes = [v for v in (num(r[2]) for r in rows) if v is not None]
+    if not rows or not sm or not smaxes:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"],
                 "samples": len(rows)}
+    smax = max(smaxes)
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    reasons = sorted({names[i] for r in rows for i in range(4)
+                      if r[5 + i].lower().startswith("active")})
+    loaded = [v for v in sm if v > 0.5 * smax] or sm
+    return {"sm_mhz": float(np.median(loaded)), "sm_max_mhz": smax, "reasons": reasons,
+            "samples": len(rows)}
 
 
 # ---------------------------------------------------------------------------

@@ -1,0 +1,49 @@
+"""Host-side pieces of bench.py that need no GPU: the clock-record summary
+that decides whether a timed run saw throttling, and the workload arithmetic."""
+
+import importlib.util
+import os
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def bench():
+    spec = importlib.util.spec_from_file_location("bench_under_test", os.path.join(ROOT, "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _line(sm, smax=1965, power=700.0, active="0x0", hw="Not Active", hwt="Not Active",
+          swt="Not Active", cap="Not Active"):
+    return "0, %s, %s, %s, %s, %s, %s, %s, %s\n" % (sm, smax, power, active, hw, hwt, swt, cap)
+
+
+def test_clock_summary_median_under_load_and_no_reason(bench):
+    lines = [_line(345)] + [_line(1965)] * 5 + [_line(1950)] * 2
+    s = bench.clock_summary(lines)
+    assert s["sm_mhz"] == 1965.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == [] and s["samples"] == 8
+
+
+def test_clock_summary_reports_throttle_reasons(bench):
+    lines = [_line(1965)] * 3 + [_line(1300, cap="Active")] + [_line(1100, hwt="Active")]
+    s = bench.clock_summary(lines)
+    assert s["reasons"] == ["hw_thermal_slowdown", "sw_power_cap"]
+    assert s["sm_mhz"] == 1965.0
+
+
+def test_clock_summary_skips_unavailable_fields(bench):
+    lines = [_line("[N/A]", "[N/A]")] + [_line(1900)] * 3 + ["garbage\n"]
+    s = bench.clock_summary(lines)
+    assert s["sm_mhz"] == 1900.0 and s["samples"] == 4
+    assert bench.clock_summary([_line("[N/A]", "[N/A]")])["reasons"] == ["no samples"]
+    assert bench.clock_summary([])["sm_mhz"] is None
+
+
+def test_entries_per_step(bench):
+    # (N_train^2 + N_test * N_train) kernel entries per sigma
+    assert bench.entries_per_step(32768, 8192, 3) == (32768 ** 2 + 8192 * 32768) * 3
