@@ -47,3 +47,19 @@ def test_clock_summary_skips_unavailable_fields(bench):
 def test_entries_per_step(bench):
     # (N_train^2 + N_test * N_train) kernel entries per sigma
     assert bench.entries_per_step(32768, 8192, 3) == (32768 ** 2 + 8192 * 32768) * 3
+
+
+def test_clock_sampler_end_to_end_with_a_stand_in_nvidia_smi(bench, tmp_path, monkeypatch):
+    """start()/stop() around a stand-in `nvidia-smi` that prints one sample
+    per 20 ms: the samples are read back and summarised."""
+    import time
+    exe = tmp_path / "nvidia-smi"
+    exe.write_text("#!/bin/sh\nwhile true; do echo '%s'; sleep 0.02; done\n"
+                   % _line(1965, cap="Active").strip())
+    exe.chmod(0o755)
+    monkeypatch.setenv("PATH", str(tmp_path) + os.pathsep + os.environ["PATH"])
+    cs = bench.ClockSampler(0)
+    cs.start()
+    time.sleep(0.3)
+    s = cs.stop()
+    assert s["sm_mhz"] == 1965.0 and s["reasons"] == ["sw_power_cap"] and s["samples"] >= 2
