@@ -63,3 +63,29 @@ def test_clock_sampler_end_to_end_with_a_stand_in_nvidia_smi(bench, tmp_path, mo
     time.sleep(0.3)
     s = cs.stop()
     assert s["sm_mhz"] == 1965.0 and s["reasons"] == ["sw_power_cap"] and s["samples"] >= 2
+
+
+def test_reference_arm_reports_our_arms_config(bench, monkeypatch):
+    """`bench.py --impl reference` (CPU only) prints one JSON line on the same
+    config, metric, unit and direction as our arm at its defaults, with its
+    bounded sample stated in cpu_baseline and no host<->device bytes."""
+    import json
+    import subprocess
+    import sys
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                          "--steps", "1", "--warmup", "0", "--cpu-ntrain", "256",
+                          "--cpu-ntest", "64"], capture_output=True, text=True, timeout=600,
+                         env=dict(os.environ, OMP_NUM_THREADS="2", OPENBLAS_NUM_THREADS="2"))
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    monkeypatch.setattr(sys, "argv", ["bench.py"])
+    a = bench.parse()  # our arm's defaults
+    ours = bench.headline_config(a, [float(s) for s in a.sigmas.split(",")], 1)
+    assert line["impl"] == "reference"
+    assert line["config"] == ours and ours["n_train"] == 32768 and ours["n_test"] == 8192
+    assert line["metric"] == bench.METRIC and line["unit"] == bench.UNIT
+    assert line["higher_is_better"] is True
+    assert line["cpu_baseline"]["value"] == line["value"]
+    assert line["cpu_baseline"]["kind"] == "port"
+    assert "N_train=256" in line["cpu_baseline"]["sample"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
