@@ -109,3 +109,26 @@ def test_noalloc_prediction_limits_need_no_gpu(lib):
     rc, msg = _rc_and_message(lib, "fmlb_kernel_predict_f64_noalloc", 0, None, nq, 4, None,
                               1024, 4, 4, sig, 8, None, ll(1024), None, ll(nq), None)
     assert rc == -22 and b"exceeds the fixed scratch" in msg
+
+
+def test_integration_stubs_match_the_abi():
+    """The ctypes stubs shown to maintainers declare the argument and result
+    types the library's own binding table (checked against the header above)
+    uses for the same functions."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    blocks = re.findall(r"```python\n(.*?)```", text, flags=re.S)
+    ns = {"ctypes": ctypes, "_vp": ctypes.c_void_p, "_i": ctypes.c_int,
+          "_ll": ctypes.c_longlong}
+    seen = set()
+    for block in blocks:
+        for name, kind, expr in re.findall(r"_lib\.(fmlb_\w+)\.(argtypes|restype)\s*=\s*"
+                                           r"(\[.*?\]|[\w.]+)", block, flags=re.S):
+            value = eval(expr, ns)  # the stub's own expression
+            restype, argtypes = _lib.SIGNATURES[name]
+            if kind == "argtypes":
+                assert value == argtypes, name
+                seen.add(name)
+            else:
+                assert value == restype, name
+    assert {"fmlb_gaussian_kernel_f64", "fmlb_potrf_f64", "fmlb_potrs_f64",
+            "fmlb_potri_f64"} <= seen
