@@ -11,6 +11,13 @@
 //     fewer than 4 tokens ends the atom list; otherwise token 1 is the element
 //     symbol (looked up in the caller's charge table, NUCLEAR_CHARGE of
 //     fml/data.py) and tokens 2-4 are x, y, z (float()).
+// Whitespace and number syntax follow Python's str.split(), int() and float()
+// for ASCII text: tokens split on space, \t, \v, \f and \x1c-\x1f; int()
+// strips space, \t, \v and \f around the count; numbers are an optional
+// sign and decimal digits with single underscores between digits (PEP 515),
+// for float() also a fraction, an exponent, or inf / infinity / nan in any
+// case. Non-ASCII digits and whitespace, which Python also accepts, are
+// rejected, and so are declared counts outside the int32 range.
 // The atom list length, not the declared count, sizes the molecule, as in
 // the reference (natoms is only stored).
 #include <ctype.h>
@@ -63,7 +70,10 @@ void split_lines(const std::string &s, std::vector<std::pair<size_t, size_t>> &l
     if (b < n) lines.emplace_back(b, n);
 }
 
-bool is_ws(char c) { return c == ' ' || c == '\t' || c == '\v' || c == '\f'; }
+// ASCII whitespace of Python's str.split() (newlines never occur inside a line)
+bool is_ws(char c) {
+    return c == ' ' || c == '\t' || c == '\v' || c == '\f' || (c >= '\x1c' && c <= '\x1f');
+}
 
 // Whitespace tokens of s[b, e), at most 4 (the rest are ignored).
 int tokens(const std::string &s, size_t b, size_t e, std::string tok[4]) {
@@ -80,26 +90,83 @@ int tokens(const std::string &s, size_t b, size_t e, std::string tok[4]) {
     return k;
 }
 
-bool parse_double(const std::string &t, double &v) {
-    if (t.empty()) return false;
-    char *end = nullptr;
-    errno = 0;
-    v = strtod(t.c_str(), &end);
-    // Python float() rejects hexadecimal forms, which strtod accepts
-    for (char c : t)
-        if (c == 'x' || c == 'X') return false;
-    return end == t.c_str() + t.size();
+bool is_digit(char c) { return c >= '0' && c <= '9'; }
+
+// Removes the digit-group underscores of a PEP 515 literal into `out`; false
+// when an underscore does not sit between two digits.
+bool strip_underscores(const std::string &t, std::string &out) {
+    out.clear();
+    for (size_t i = 0; i < t.size(); ++i) {
+        if (t[i] != '_') {
+            out.push_back(t[i]);
+            continue;
+        }
+        if (i == 0 || i + 1 == t.size() || !is_digit(t[i - 1]) || !is_digit(t[i + 1]))
+            return false;
+    }
+    return true;
 }
 
+bool equals_nocase(const char *a, size_t n, const char *word) {
+    if (strlen(word) != n) return false;
+    for (size_t i = 0; i < n; ++i)
+        if (tolower((unsigned char)a[i]) != word[i]) return false;
+    return true;
+}
+
+// float() of one token (no surrounding whitespace): [sign] then inf, infinity
+// or nan in any case, or digits [. digits] / . digits with an optional
+// exponent e[sign]digits. The value comes from strtod on the validated text
+// (correctly rounded, like Python's own conversion).
+bool parse_double(const std::string &tok, double &v) {
+    std::string t;
+    if (tok.empty() || !strip_underscores(tok, t)) return false;
+    const char *p = t.c_str();
+    size_t i = (t[0] == '+' || t[0] == '-') ? 1 : 0;
+    const size_t rest = t.size() - i;
+    if (equals_nocase(p + i, rest, "inf") || equals_nocase(p + i, rest, "infinity") ||
+        equals_nocase(p + i, rest, "nan")) {
+        v = strtod(p, nullptr);
+        return true;
+    }
+    size_t digits = 0;
+    while (i < t.size() && is_digit(t[i])) ++i, ++digits;
+    if (i < t.size() && t[i] == '.') {
+        ++i;
+        while (i < t.size() && is_digit(t[i])) ++i, ++digits;
+    }
+    if (digits == 0) return false;
+    if (i < t.size() && (t[i] == 'e' || t[i] == 'E')) {
+        ++i;
+        if (i < t.size() && (t[i] == '+' || t[i] == '-')) ++i;
+        size_t exp_digits = 0;
+        while (i < t.size() && is_digit(t[i])) ++i, ++exp_digits;
+        if (exp_digits == 0) return false;
+    }
+    if (i != t.size()) return false;
+    v = strtod(p, nullptr);
+    return true;
+}
+
+// The whitespace int() strips around its argument: C isspace, narrower than
+// str.split()'s (\x1c-\x1f are not stripped)
+bool is_strip_ws(char c) { return c == ' ' || c == '\t' || c == '\v' || c == '\f'; }
+
+// int() of s[b, e): surrounding whitespace, [sign] digits with PEP 515
+// underscores; values outside the int32 range are rejected.
 bool parse_int(const std::string &s, size_t b, size_t e, int &v) {
-    while (b < e && (is_ws(s[b]))) ++b;
-    while (e > b && (is_ws(s[e - 1]))) --e;
+    while (b < e && is_strip_ws(s[b])) ++b;
+    while (e > b && is_strip_ws(s[e - 1])) --e;
     if (b == e) return false;
-    const std::string t = s.substr(b, e - b);
-    char *end = nullptr;
+    std::string t;
+    if (!strip_underscores(s.substr(b, e - b), t)) return false;
+    size_t i = (t[0] == '+' || t[0] == '-') ? 1 : 0;
+    if (i == t.size()) return false;
+    for (size_t k = i; k < t.size(); ++k)
+        if (!is_digit(t[k])) return false;
     errno = 0;
-    const long x = strtol(t.c_str(), &end, 10);
-    if (end != t.c_str() + t.size() || errno || x < -2147483647L || x > 2147483647L) return false;
+    const long long x = strtoll(t.c_str(), nullptr, 10);
+    if (errno || x < -2147483647LL || x > 2147483647LL) return false;
     v = (int)x;
     return true;
 }
@@ -215,9 +282,19 @@ extern "C" int fmlb_xyz_parse(const char *const *paths, int nfiles, const int *o
                               const char *const *table_symbols, const double *table_charges,
                               int ntable, double *charges, double *coords, int *symbol_index,
                               int nthreads) {
-    if (nfiles < 0 || ntable < 0 ||
-        (nfiles > 0 && (!paths || !offsets || !charges || !coords)) ||
+    if (nfiles < 0 || ntable < 0 || (nfiles > 0 && (!paths || !offsets)) ||
         (ntable > 0 && (!table_symbols || !table_charges))) {
+        fmlb::set_error("fmlb_xyz_parse: bad arguments");
+        return FMLB_EINVAL;
+    }
+    // a batch without atoms (every file an empty molecule) needs no output
+    // buffers; its files are still parsed, into a dummy of capacity zero
+    double dummy[3] = {0.0, 0.0, 0.0};
+    if (nfiles > 0 && offsets[nfiles] == 0) {
+        if (!charges) charges = dummy;
+        if (!coords) coords = dummy;
+    }
+    if (nfiles > 0 && (!charges || !coords)) {
         fmlb::set_error("fmlb_xyz_parse: bad arguments");
         return FMLB_EINVAL;
     }

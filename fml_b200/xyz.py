@@ -54,10 +54,11 @@ def read_xyz_batch(paths, nthreads=0, to_device=False):
 
     Raises KeyError for an element missing from NUCLEAR_CHARGE (the
     reference's dict lookup) and ValueError for an unreadable file, a bad
-    atom count or a coordinate that is not a decimal number. Coordinates are
-    read with C strtod: decimal and exponent forms, inf and nan as Python's
-    float() reads them; Python's digit-group underscores ("1_0.5") are
-    rejected.
+    atom count or a coordinate that is not a decimal number. The count and
+    the coordinates are read as Python's int() and float() read ASCII text
+    (signs, fractions, exponents, inf / infinity / nan in any case, digit-group
+    underscores such as "1_0.5"); non-ASCII digits and declared counts outside
+    the int32 range raise ValueError.
     """
     enc = [os.fsencode(os.fspath(p)) for p in paths]
     n = len(enc)

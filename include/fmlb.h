@@ -103,7 +103,11 @@ int fmlb_exp_weighted_colsum_f64(const double *M, long long ldm, int rows, int c
  *   charges (A,), coords (A, 3) and, when not NULL, symbol_index (A,) (index
  *   of the element in the caller's table: table_symbols / table_charges,
  *   the reference's NUCLEAR_CHARGE). Pass page-locked buffers to follow with
- *   one asynchronous copy per array.
+ *   one asynchronous copy per array. charges and coords may be NULL when
+ *   offsets[nfiles] == 0 (no atoms in the batch).
+ * Numbers follow Python's int() and float() for ASCII text (signs, fractions,
+ * exponents, inf / infinity / nan in any case, PEP 515 digit-group
+ * underscores); tokens split on str.split()'s ASCII whitespace.
  * Errors: FMLB_EINVAL with the file and line in the error string (unreadable
  * file, bad atom count, unknown element, a coordinate that is not a number).
  * ---------------------------------------------------------------------- */
