@@ -154,26 +154,34 @@ def _ptp_arrays(Z, amax):
     """kernels.py:261-292: PTP (nm, amax, 2) float64 and atom counts N (nm,) int32.
 
     One table lookup over the concatenated charges and one scatter into the
-    padded rows. A charge the table does not hold raises KeyError with the
-    first such charge in molecule and atom order, as the reference's dict
-    lookup does (kernels.py:276)."""
+    padded rows, with the reference's errors in its order: charges are
+    truncated toward zero as int(q) does (a non-finite charge raises
+    ValueError or OverflowError as int() does); a charge the table does not
+    hold raises KeyError with the first such charge in molecule and atom order
+    (the dict lookup of kernels.py:276, done for every molecule before any
+    row is filled); then a molecule with more atoms than the descriptor size
+    raises IndexError (the row fill of kernels.py:281)."""
     nm = len(Z)
-    zs = [np.asarray(z).reshape(-1) for z in Z]
+    zs = [np.asarray(z, dtype=np.float64).reshape(-1) for z in Z]
     N = np.array([len(z) for z in zs], dtype=np.int32)
-    if nm and N.max() > amax:
-        raise ValueError("a molecule has more atoms (%d) than the descriptor size %d"
-                         % (int(N.max()), amax))
     Zp = np.zeros((nm, amax, 2))
-    if nm and N.sum():
-        zi = np.concatenate(zs).astype(np.int64)
-        bad = (zi < 0) | (zi > 127)
-        bad |= PTP_ROW[np.clip(zi, 0, 127)] < 0
-        if bad.any():
-            raise KeyError(int(zi[np.argmax(bad)]))
-        mol = np.repeat(np.arange(nm), N)
-        slot = np.arange(len(zi)) - np.repeat(np.cumsum(N) - N, N)
-        Zp[mol, slot, 0] = PTP_ROW[zi]
-        Zp[mol, slot, 1] = PTP_COL[zi]
+    if not (nm and N.sum()):
+        return Zp, N
+    zf = np.concatenate(zs)
+    fin = np.isfinite(zf)
+    zi = np.trunc(np.clip(np.where(fin, zf, 0.0), -1.0, 128.0)).astype(np.int64)
+    bad = ~fin | (zi < 0) | (zi > 127)
+    bad |= PTP_ROW[np.clip(zi, 0, 127)] < 0
+    if bad.any():
+        # int() of the first offending charge raises for NaN / inf as the
+        # reference's int(q) does; otherwise the dict lookup's KeyError
+        raise KeyError(int(zf[int(np.argmax(bad))]))
+    if N.max() > amax:
+        raise IndexError("index %d is out of bounds for axis 1 with size %d" % (amax, amax))
+    mol = np.repeat(np.arange(nm), N)
+    slot = np.arange(len(zi)) - np.repeat(np.cumsum(N) - N, N)
+    Zp[mol, slot, 0] = PTP_ROW[zi]
+    Zp[mol, slot, 1] = PTP_COL[zi]
     return Zp, N
 
 

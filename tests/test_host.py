@@ -127,3 +127,46 @@ def test_vector_kernel_dropin_checks_sizes():
     with pytest.raises(ValueError):
         fml_b200.fget_vector_kernels_gaussian(np.zeros((3, 2, 4)), np.zeros((3, 2, 5)),
                                               [1] * 4, [1] * 5, [1.0], 4, 4, 1)
+
+
+def _reference_ptp_marshalling(Z, amax):
+    """The loops of kernels.py:261-292 (get_atomic_kernels_arad), restated
+    with the reference's PTP dict, for comparison with the vectorised form."""
+    from fml_b200.data import PTP
+    N = np.array([len(z) for z in Z], dtype=np.int32)
+    c = [np.array([PTP[int(q)] for q in z], dtype=np.int32) for z in Z]
+    out = np.zeros((len(Z), amax, 2))
+    for i in range(len(Z)):
+        for j, p in enumerate(c[i]):
+            out[i, j] = p
+    return out, N
+
+
+def _outcome(fn, *args):
+    try:
+        return fn(*args)
+    except (KeyError, IndexError, ValueError, OverflowError) as e:
+        return type(e), e.args[:1] if isinstance(e, KeyError) else ()
+
+
+from hypothesis import given, settings  # noqa: E402
+from hypothesis import strategies as hst  # noqa: E402
+
+_CHARGE = hst.one_of(hst.sampled_from([1.0, 6.0, 7.0, 8.0, 16.0, 9.0, 17.0, 35.0, 53.0]),
+                     hst.floats(-3.0, 130.0), hst.sampled_from([0.0, -0.5, 118.0, 6.99,
+                                                                float("nan"), float("inf")]))
+
+
+@settings(max_examples=300, deadline=None)
+@given(hst.lists(hst.lists(_CHARGE, max_size=7), max_size=5), hst.integers(1, 6))
+def test_ptp_marshalling_matches_reference_loops(Z, amax):
+    """Same arrays, or the same exception (type and KeyError key) in the same
+    order of checks, as the reference's per-molecule loops."""
+    from fml_b200.kernels import _ptp_arrays
+    got = _outcome(_ptp_arrays, Z, amax)
+    ref = _outcome(_reference_ptp_marshalling, Z, amax)
+    if isinstance(ref, tuple) and isinstance(ref[0], type):
+        assert got == ref, (Z, amax, got, ref)
+        return
+    np.testing.assert_array_equal(got[0], ref[0])
+    np.testing.assert_array_equal(got[1], ref[1])
