@@ -626,8 +626,8 @@ class KRRServer:
             t_adm = time.perf_counter()
             self.phase_max["completions"] = max(self.phase_max["completions"], t_adm - t_ph)
             # admission of prediction batches: the model with the oldest waiting
-            # request first; CM batches prefer the high-priority slots, ARAD
-            # batches use the others
+            # request first; CM batches take only the high-priority slots, ARAD
+            # batches only the others
             for _, mid in sorted((q[0].arrival, mid) for mid, q in queues.items() if q):
                 m = self.models[mid]
                 q = queues[mid]
